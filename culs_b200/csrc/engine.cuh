@@ -1,0 +1,102 @@
+// Batch engine: many AIGs resident on one GPU, rewritten (`rw`) and strashed
+// (`st`) together by the same kernels.
+//
+// At rest a batch stores its graphs one after another ("graph-major"): graph
+// g owns positions base_g .. base_g + nObjs_g - 1 and keeps the AIGMan arrays
+// of CULS (src/aig_manager.h:51-58) with graph-local literals: F0/F1 hold
+// 2*localId + complement with literal 0 = constant TRUE (-1 for the constant
+// and the PIs), POs hold local literals.  A single graph is a batch of one.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "prim.cuh"
+#include "rw_core.cuh"
+
+namespace culs {
+
+struct DevGraph {
+    int nPIs, nPOs, nAnds, nLevels;
+    int base;   // first position of this graph in graph-major arrays
+    int poOff;  // first PO of this graph in the PO array
+    int cpos;   // position of the constant node in the current working layout
+    int pad;
+};
+
+// Counters reported by the choice loop (CULS src/algorithms/rewrite.cu:849-897)
+struct RwStats {
+    long long replaced, replacedPos, replacedZero, reverted, compromised, preEval, smallCut, newIdx, expected,
+        newNodes, candidates;
+};
+
+struct Batch {
+    int G = 0;
+    int64_t nObj = 0, nPO = 0;
+    std::vector<DevGraph> hg;  // host copy of the graph table
+    DevGraph *dg = nullptr;
+    int *F0 = nullptr, *F1 = nullptr, *PO = nullptr;  // graph-local literals
+    int64_t capObj = 0, capPO = 0;
+    int capG = 0;
+    ~Batch();
+    void release();
+};
+
+// Per-node dumps of the last rw (for parity checks); indexed by the graph's
+// reordered local id (the numbering rw::CPUSolver::Reorder produces).
+struct RwDump {
+    bool enabled = false;
+    // for graph 0 of the batch only
+    std::vector<int> reorderF0, reorderF1, reorderOut;  // AIGER convention, local ids
+    std::vector<int> cuts;                              // (n+1)*8*9
+    std::vector<int> selected;                          // (n+1)*10
+    std::vector<int> replace, newF0, newF1;             // local ids, rebuilt numbering
+    std::vector<int> choice;                            // per node outcome code
+};
+
+class Engine {
+  public:
+    Engine();
+    ~Engine();
+    int init(size_t hbmBudget);  // loads the library, creates the stream
+    const std::string &error() const { return err_; }
+
+    int upload(Batch &b, int count, const int32_t *const *f0, const int32_t *const *f1, const int32_t *const *outs,
+               const int32_t *nPIs, const int32_t *nPOs, const int32_t *nAnds);
+    int download(const Batch &b, int g, int32_t *f0, int32_t *f1, int32_t *outs);
+    int rw(Batch &b, bool useZeros, bool gpuDedup, RwStats *stats, RwDump *dump);
+    int st(Batch &b, bool cpuOrder);
+    int sync();
+
+    cudaStream_t stream() const { return s_; }
+    size_t budget() const { return budget_; }
+    size_t arenaHighWater() const { return ar_.high_water(); }
+    int kernelLaunches() const { return launches_; }
+    void resetLaunchCount() { launches_ = 0; }
+
+  private:
+    int fail(int code, const std::string &msg);
+    int check(cudaError_t e, const char *what);
+    int check_status(const char *what);
+    int ensure_arena(size_t bytes);
+
+    // stage helpers
+    int strash_core(Batch &b, int64_t nNodes, const int *lit0, const int *lit1, const int *gidArr, const int *po,
+                    bool cpuOrder, bool removeDangling, bool foldTrivial);
+
+    std::string err_;
+    cudaStream_t s_ = nullptr;
+    RwLib *lib_ = nullptr;
+    int *status_ = nullptr;     // device status word
+    int *counters_ = nullptr;   // device scratch counters
+    int *hostSmall_ = nullptr;  // pinned host scratch
+    size_t budget_ = 0;
+    Arena ar_;
+    int launches_ = 0;
+    int sms_ = 148;
+};
+
+}  // namespace culs

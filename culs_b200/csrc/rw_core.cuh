@@ -1,0 +1,330 @@
+// Per-item logic of the rewriting pass, written as __host__ __device__
+// functions over plain arrays.  The engine's kernels (engine.cu) call these;
+// each function names the reference code whose semantics it reproduces
+// (paths relative to the CULS source tree).
+//
+// Node addressing: every object of a batch has a storage position; literals
+// are 2*position + complement.  Within one graph, storage order equals id
+// order, so comparisons of positions reproduce the reference's comparisons of
+// node ids.  Per graph, `cpos` is the position of the constant node.
+#pragma once
+
+#include "common.cuh"
+
+namespace culs {
+
+// ----------------------------------------------------------- library
+// The 4-input rewriting library (same values as CULS
+// src/algorithms/rewrite_library.inc, decoded as rw::CPUSolver::ReadLibrary
+// does, src/algorithms/rewrite.cu:1281-1307), repacked for single loads.
+constexpr int kNumClasses = 222;
+constexpr int kMaxLibNodes = 56;  // <= 50 internal nodes + 4 inputs fit in 54
+struct RwLib {
+    // per truth table: phase (bits 0-4) | perm index (bits 8-12) | class (bits 16-23)
+    uint32_t npn[1 << 16];
+    uint8_t perm4[24][4];
+    uint8_t nNodes[kNumClasses], nRoots[kNumClasses];
+    // per class and internal node j (library index j+4):
+    // fanin0 (bits 0-7) | fanin1 (bits 8-15) | compl0 (bit 16) | compl1 (bit 17)
+    uint32_t node[kNumClasses][kMaxLibNodes];
+    uint8_t roots[kNumClasses][16];
+};
+
+CULS_HD int npn_phase(uint32_t w) { return (int)(w & 31u); }
+CULS_HD int npn_perm(uint32_t w) { return (int)((w >> 8) & 31u); }
+CULS_HD int npn_class(uint32_t w) { return (int)((w >> 16) & 255u); }
+CULS_HD int ln_f0(uint32_t w) { return (int)(w & 255u); }
+CULS_HD int ln_f1(uint32_t w) { return (int)((w >> 8) & 255u); }
+CULS_HD int ln_c0(uint32_t w) { return (int)((w >> 16) & 1u); }
+CULS_HD int ln_c1(uint32_t w) { return (int)((w >> 17) & 1u); }
+
+// --------------------------------------------------------------- cuts
+// A cut slot (rw::Cut, src/algorithms/rewrite.h:10-16).  In device memory a
+// slot is an int4 of leaves plus an int2 {sign, packed}, packed =
+// tt (bits 0-15) | value (bits 16-26) | nLeaves (bits 27-29) | used (bit 30).
+struct Cut {
+    int leaves[4];
+    uint32_t sign;
+    uint32_t tt;
+    uint32_t value;
+    uint32_t nLeaves;
+    uint32_t used;
+};
+
+CULS_HD uint32_t cut_pack(const Cut &c) {
+    return (c.tt & 0xFFFFu) | ((c.value & 0x7FFu) << 16) | ((c.nLeaves & 7u) << 27) | ((c.used & 1u) << 30);
+}
+CULS_HD void cut_unpack(uint32_t w, Cut &c) {
+    c.tt = w & 0xFFFFu;
+    c.value = (w >> 16) & 0x7FFu;
+    c.nLeaves = (w >> 27) & 7u;
+    c.used = (w >> 30) & 1u;
+}
+CULS_HD uint32_t packed_used(uint32_t w) { return (w >> 30) & 1u; }
+CULS_HD uint32_t packed_nleaves(uint32_t w) { return (w >> 27) & 7u; }
+
+CULS_HD int popc32(uint32_t x) {
+#if defined(__CUDA_ARCH__)
+    return __popc(x);
+#else
+    return __builtin_popcount(x);
+#endif
+}
+CULS_HD int popc64(uint64_t x) {
+#if defined(__CUDA_ARCH__)
+    return __popcll(x);
+#else
+    return __builtin_popcountll(x);
+#endif
+}
+
+// CutFindValue, src/algorithms/rewrite.cu:49-61
+CULS_HD uint32_t cut_value(const Cut &c, const int *ref) {
+    int value = 0, nOnes = 0;
+    for (uint32_t i = 0; i < c.nLeaves; i++) {
+        int r = ref[c.leaves[i]];
+        value += r;
+        nOnes += (r == 1);
+    }
+    if (c.nLeaves < 2) return 1001u;
+    if (value > 1000) value = 1000;
+    if (nOnes > 3) value = 5 - nOnes;
+    return (uint32_t)value & 0x7FFu;
+}
+
+// FindCut, src/algorithms/rewrite.cu:84-109: first unused slot, else the
+// lowest-value slot among >2-leaf cuts, then 2-leaf, then smaller cuts; the
+// chosen slot is marked unused before any merge is tried.
+CULS_HD int find_slot(Cut *s) {
+    for (int i = 0; i < 8; i++)
+        if (s[i].used == 0) return i;
+    int ans = -1;
+    for (int i = 0; i < 8; i++)
+        if (s[i].nLeaves > 2 && (ans == -1 || s[i].value < s[ans].value)) ans = i;
+    if (ans == -1)
+        for (int i = 0; i < 8; i++)
+            if (s[i].nLeaves == 2 && (ans == -1 || s[i].value < s[ans].value)) ans = i;
+    if (ans == -1)
+        for (int i = 0; i < 8; i++)
+            if (s[i].nLeaves < 2 && (ans == -1 || s[i].value < s[ans].value)) ans = i;
+    s[ans].used = 0;
+    return ans;
+}
+
+// MergeCutOrdered / MergeCut, src/algorithms/rewrite.cu:112-164.  Merges
+// the sorted leaf lists of a and b into out (at most 4 leaves).  Returns 0
+// when the union exceeds 4 leaves; out's leaves may be partly written then.
+CULS_HD int merge_cuts(const Cut &a0, const Cut &b0, Cut *out) {
+    const Cut &a = (a0.nLeaves >= b0.nLeaves) ? a0 : b0;
+    const Cut &b = (a0.nLeaves >= b0.nLeaves) ? b0 : a0;
+    int c = 0, i = 0, k = 0;
+    const int na = (int)a.nLeaves, nb = (int)b.nLeaves;
+    for (c = 0; c < 4; c++) {
+        if (k == nb) {
+            if (i == na) {
+                out->nLeaves = (uint32_t)c;
+                out->sign = a0.sign | b0.sign;
+                out->used = 1;
+                return 1;
+            }
+            out->leaves[c] = a.leaves[i++];
+            continue;
+        }
+        if (i == na) {
+            out->leaves[c] = b.leaves[k++];
+            continue;
+        }
+        if (a.leaves[i] < b.leaves[k]) {
+            out->leaves[c] = a.leaves[i++];
+            continue;
+        }
+        if (a.leaves[i] > b.leaves[k]) {
+            out->leaves[c] = b.leaves[k++];
+            continue;
+        }
+        out->leaves[c] = a.leaves[i++];
+        k++;
+    }
+    if (i < na || k < nb) return 0;
+    out->nLeaves = (uint32_t)c;
+    out->sign = a0.sign | b0.sign;
+    out->used = 1;
+    return 1;
+}
+
+// CutDominance, src/algorithms/rewrite.cu:167-175: leaves(a) subset of leaves(b)
+CULS_HD int cut_subset(const Cut &a, const Cut &b) {
+    for (uint32_t i = 0; i < a.nLeaves; i++) {
+        int ok = 0;
+        for (uint32_t j = 0; j < b.nLeaves; j++)
+            if (b.leaves[j] == a.leaves[i]) ok = 1;
+        if (!ok) return 0;
+    }
+    return 1;
+}
+
+// CutFilter, src/algorithms/rewrite.cu:178-193
+CULS_HD int cut_filter(Cut *s, int id) {
+    for (int i = 0; i < 8; i++) {
+        if (i == id || !s[i].used) continue;
+        if (s[i].nLeaves > s[id].nLeaves) {
+            if ((s[i].sign & s[id].sign) != s[id].sign) continue;
+            if (cut_subset(s[id], s[i])) s[i].used = 0;
+        } else {
+            if ((s[i].sign & s[id].sign) != s[i].sign) continue;
+            if (cut_subset(s[i], s[id])) {
+                s[id].used = 0;
+                return 1;
+            }
+        }
+    }
+    return 0;
+}
+
+// CutTruthSwapAdjacentVars, src/algorithms/rewrite.cu:203-211, on 16 bits.
+CULS_HD uint32_t tt_swap_adj(uint32_t t, int v) {
+    if (v == 0) return (t & 0x9999u) | ((t & 0x2222u) << 1) | ((t & 0x4444u) >> 1);
+    if (v == 1) return (t & 0xC3C3u) | ((t & 0x0C0Cu) << 2) | ((t & 0x3030u) >> 2);
+    if (v == 2) return (t & 0xF00Fu) | ((t & 0x00F0u) << 4) | ((t & 0x0F00u) >> 4);
+    return 0;
+}
+
+// CutTruthPhase, src/algorithms/rewrite.cu:195-201
+CULS_HD int tt_phase(const Cut &x, const Cut &cut) {
+    int ph = 0;
+    for (uint32_t i = 0; i < cut.nLeaves; i++)
+        for (uint32_t j = 0; j < x.nLeaves; j++)
+            if (x.leaves[j] == cut.leaves[i]) ph |= 1 << i;
+    return ph;
+}
+
+// CutTruthStretch, src/algorithms/rewrite.cu:213-221
+CULS_HD uint32_t tt_stretch(uint32_t t, int nVar, int ph) {
+    int var = nVar - 1;
+    for (int i = 3; i >= 0; i--)
+        if (ph >> i & 1) {
+            for (int k = var; k < i; k++) t = tt_swap_adj(t, k);
+            var--;
+        }
+    return t;
+}
+
+// CutTruthtable, src/algorithms/rewrite.cu:223-229
+CULS_HD uint32_t cut_truth(const Cut &cut, const Cut &a, const Cut &b, int ca, int cb) {
+    uint32_t t0 = ca ? (~a.tt & 0xFFFFu) : a.tt;
+    uint32_t t1 = cb ? (~b.tt & 0xFFFFu) : b.tt;
+    t0 = tt_stretch(t0, (int)a.nLeaves, tt_phase(a, cut));
+    t1 = tt_stretch(t1, (int)b.nLeaves, tt_phase(b, cut));
+    return (t0 & t1) & 0xFFFFu;
+}
+
+// CutTruthShrink, src/algorithms/rewrite.cu:231-241
+CULS_HD uint32_t tt_shrink(uint32_t t, int ph) {
+    int var = 0;
+    for (int i = 0; i < 4; i++)
+        if (ph & (1 << i)) {
+            for (int k = i - 1; k >= var; k--) t = tt_swap_adj(t, k);
+            var++;
+        }
+    return t;
+}
+
+// MinimizeCutSupport, src/algorithms/rewrite.cu:243-266.  `lsb` holds
+// (local id & 31) of each leaf position so that the recomputed sign uses
+// graph-local ids; it is read through lidLow[leaf].
+CULS_HD int cut_minimize(Cut *c, const uint8_t *lidLow) {
+    const uint32_t m0[4] = {0x5555u, 0x3333u, 0x0F0Fu, 0x00FFu};
+    const uint32_t m1[4] = {0xAAAAu, 0xCCCCu, 0xF0F0u, 0xFF00u};
+    int ph = 0;
+    uint32_t t = c->tt & 0xFFFFu;
+    int nl = (int)c->nLeaves;
+    for (uint32_t i = 0; i < c->nLeaves; i++) {
+        if ((t & m0[i]) == ((t & m1[i]) >> (1 << i)))
+            nl--;
+        else
+            ph |= 1 << i;
+    }
+    if (nl == (int)c->nLeaves) return 0;
+    t = tt_shrink(t, ph);
+    c->tt = t & 0xFFFFu;
+    c->sign = 0;
+    for (uint32_t i = 0, k = 0; i < c->nLeaves; i++)
+        if (ph >> i & 1) {
+            c->leaves[k++] = c->leaves[i];
+            c->sign |= 1u << (lidLow[c->leaves[i]] & 31u);
+        }
+    c->nLeaves = (uint32_t)nl;
+    return 1;
+}
+
+// The CutEnumerate body for one pair (src/algorithms/rewrite.cu:282-291).
+// Returns 1 when enumeration of this node must stop (a cut with fewer than
+// two leaves was produced).
+CULS_HD int enum_pair(Cut *s, const Cut &a, const Cut &b, int ca, int cb, const int *ref, const uint8_t *lidLow) {
+    if (popc32(a.sign | b.sign) > 4) return 0;
+    int id = find_slot(s);
+    if (!merge_cuts(a, b, &s[id])) return 0;
+    if (cut_filter(s, id)) return 0;
+    s[id].tt = cut_truth(s[id], a, b, ca, cb);
+    if (cut_minimize(&s[id], lidLow)) cut_filter(s, id);
+    s[id].value = cut_value(s[id], ref);
+    return s[id].nLeaves < 2 ? 1 : 0;
+}
+
+// ------------------------------------------------------ existence table
+// Open-addressing table of AND nodes keyed by (fanin0 id, fanin1 id,
+// compl0, compl1): the role of BuildHashTable/TableLookup
+// (src/algorithms/rewrite.cu:328-367,450-471).  Duplicate keys keep the
+// smallest position.
+CULS_HD unsigned long long and_key(int in0, int in1, int c0, int c1) {
+    return ((unsigned long long)(uint32_t)in0 << 32) | ((unsigned long long)(uint32_t)in1 << 2) |
+           ((unsigned long long)c0 << 1) | (unsigned long long)c1;
+}
+
+struct AndTable {
+    unsigned long long *keys;
+    int *vals;
+    uint32_t mask;  // capacity - 1 (capacity is a power of two)
+};
+
+CULS_HD int table_insert(const AndTable &t, unsigned long long key, int val, int *status) {
+    uint32_t h = (uint32_t)mix64(key) & t.mask;
+    for (uint32_t probe = 0; probe <= t.mask; probe++) {
+        unsigned long long prev = at_cas(&t.keys[h], kEmptyKey, key);
+        if (prev == kEmptyKey || prev == key) {
+            at_min(&t.vals[h], val);
+            return (int)h;
+        }
+        h = (h + 1) & t.mask;
+    }
+    set_status(status, kDevTableFull);
+    return -1;
+}
+
+// Returns the value stored for key, or -1 when absent.
+CULS_HD int table_find(const AndTable &t, unsigned long long key, int *status) {
+    uint32_t h = (uint32_t)mix64(key) & t.mask;
+    for (uint32_t probe = 0; probe <= t.mask; probe++) {
+        unsigned long long k = t.keys[h];
+        if (k == key) return t.vals[h];
+        if (k == kEmptyKey) return -1;
+        h = (h + 1) & t.mask;
+    }
+    set_status(status, kDevTableFull);
+    return -1;
+}
+
+// TableLookup, src/algorithms/rewrite.cu:346-367 (ids swapped, not literals)
+CULS_HD int and_lookup(const AndTable &t, int in0, int in1, int c0, int c1, int *status) {
+    if (in0 > in1) {
+        int x = in0;
+        in0 = in1;
+        in1 = x;
+        x = c0;
+        c0 = c1;
+        c1 = x;
+    }
+    return table_find(t, and_key(in0, in1, c0, c1), status);
+}
+
+}  // namespace culs

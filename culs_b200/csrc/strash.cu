@@ -1,0 +1,513 @@
+// Structural hashing with dangling-node removal (`st`, and the
+// deduplication that ends `rw`): a B200 restatement of Aig::strash (CULS
+// src/aig/strash.cu:190-314) and of the CPU variants (src/aig/strash.cu:
+// 322-466, src/aig_manager.cu:454-522).
+//
+// Reference semantics kept:
+//  * dangling AND nodes are those outside the transitive fanin of the POs
+//    (the fix-point of markDanglingNodesIter, strash.cu:175-188);
+//  * nodes are hashed frontier by frontier, where a node's frontier is its
+//    ASAP level among the remaining nodes, and inside a frontier in id order
+//    (strash.cu:247-277);
+//  * fanins are mapped to new literals, sorted, folded by
+//    checkTrivialAndCases (src/hash_table/hash_table.h:435-449), then hashed
+//    on the 64-bit key (lit0 << 32 | lit1) (hash_table.h:427-433);
+//  * survivors are renumbered consecutively in (frontier, id) order and the
+//    frontier count becomes the AIG level (strash.cu:279-300,483).
+// Deterministic choice: among equal keys the earliest node in (frontier, id)
+// order wins (the reference keeps whichever insertion lands first).
+//
+// B200 design: no per-frontier host loop.  Liveness is a reverse Kahn
+// worklist, levels a forward Kahn worklist over a fanout CSR, and hashing a
+// single in-order dataflow pass whose dependency waits are per-level
+// completion counters (bounded spins).
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "kernels.cuh"
+
+namespace culs {
+
+namespace {
+
+__device__ __forceinline__ bool is_and(const int *L0, int v) { return L0[v] >= 0; }
+
+__global__ void k_fanout_count(int64_t M, const int *L0, const int *L1, const int *po, int64_t nPO, int *cnt) {
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < M; v += stride) {
+        int a = L0[v];
+        if (a < 0) continue;
+        atomicAdd(&cnt[a >> 1], 1);
+        atomicAdd(&cnt[L1[v] >> 1], 1);
+    }
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < nPO; k += stride) atomicAdd(&cnt[po[k] >> 1], 1);
+}
+
+__global__ void k_dead_seed_flags(int64_t M, const int *L0, const int *cnt, uint8_t *flags) {
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < M; v += stride)
+        flags[v] = (L0[v] >= 0 && cnt[v] == 0) ? 1 : 0;
+}
+
+// Reverse Kahn: a node whose fanout count reaches zero is dangling.
+__global__ void __launch_bounds__(kBlock) k_dead_queue(WorkQueue q, const int *L0, const int *L1, int *cnt,
+                                                        uint8_t *dead, int *status) {
+    const int lane = threadIdx.x & 31;
+    while (true) {
+        int base = 0;
+        if (lane == 0) base = atomicAdd(q.head, 32);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        int v = queue_pop_wait(q, base + lane, status);
+        if (v >= 0) {
+            dead[v] = 1;
+            int u0 = L0[v] >> 1, u1 = L1[v] >> 1;
+            if (L0[u0] >= 0 && atomicSub(&cnt[u0], 1) == 1) queue_push(q, u0);
+            if (L0[u1] >= 0 && atomicSub(&cnt[u1], 1) == 1) queue_push(q, u1);
+            __threadfence();
+            atomicAdd(q.done, 1);
+        }
+        if (__all_sync(0xffffffffu, v < 0)) break;
+    }
+}
+
+// pending[v] = AND fanins of a live AND node; outdeg[u] = live AND fanouts.
+__global__ void k_live_degrees(int64_t M, const int *L0, const int *L1, const uint8_t *dead, int *pending, int *outdeg,
+                               uint8_t *liveFlag, uint8_t *seedFlag) {
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < M; v += stride) {
+        int a = L0[v];
+        bool live = a >= 0 && !dead[v];
+        liveFlag[v] = live;
+        int pend = 0;
+        if (live) {
+            int u0 = a >> 1, u1 = L1[v] >> 1;
+            if (L0[u0] >= 0) {
+                pend++;
+                atomicAdd(&outdeg[u0], 1);
+            }
+            if (L0[u1] >= 0) {
+                pend++;
+                atomicAdd(&outdeg[u1], 1);
+            }
+        }
+        pending[v] = pend;
+        seedFlag[v] = live && pend == 0;
+    }
+}
+
+__global__ void k_csr_fill(int64_t M, const int *L0, const int *L1, const uint8_t *liveFlag, int *cursor, int *adj) {
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < M; v += stride) {
+        if (!liveFlag[v]) continue;
+        int u0 = L0[v] >> 1, u1 = L1[v] >> 1;
+        if (L0[u0] >= 0) adj[atomicAdd(&cursor[u0], 1)] = (int)v;
+        if (L0[u1] >= 0) adj[atomicAdd(&cursor[u1], 1)] = (int)v;
+    }
+}
+
+// Forward Kahn: ASAP level of every live AND node (PIs and constant: 0).
+__global__ void __launch_bounds__(kBlock) k_level_queue(WorkQueue q, const int *L0, const int *L1, const int *off,
+                                                         const int *adj, int *pending, int *level, const int *gid,
+                                                         int *graphLevels, int *maxLevel, int *status) {
+    const int lane = threadIdx.x & 31;
+    while (true) {
+        int base = 0;
+        if (lane == 0) base = atomicAdd(q.head, 32);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        int v = queue_pop_wait(q, base + lane, status);
+        if (v >= 0) {
+            int u0 = L0[v] >> 1, u1 = L1[v] >> 1;
+            int l0 = L0[u0] >= 0 ? __ldcg(&level[u0]) : 0;
+            int l1 = L0[u1] >= 0 ? __ldcg(&level[u1]) : 0;
+            int lv = 1 + (l0 > l1 ? l0 : l1);
+            __stcg(&level[v], lv);
+            atomicMax(&graphLevels[gid[v]], lv);
+            atomicMax(maxLevel, lv);
+            __threadfence();
+            int e = off[v + 1];
+            for (int k = off[v]; k < e; k++) {
+                int w = adj[k];
+                if (atomicSub(&pending[w], 1) == 1) queue_push(q, w);
+            }
+            __threadfence();
+            atomicAdd(q.done, 1);
+        }
+        if (__all_sync(0xffffffffu, v < 0)) break;
+    }
+}
+
+__global__ void k_gather_levels(int64_t n, const int *idx, const int *level, uint32_t *keys, int *lvlCnt) {
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        int l = level[idx[i]];
+        keys[i] = (uint32_t)l;
+        atomicAdd(&lvlCnt[l], 1);
+    }
+}
+
+__global__ void k_inverse(int64_t n, const int *srt, int *tOf) {
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += stride) tOf[srt[t]] = (int)t;
+}
+
+struct DedupArgs {
+    int64_t nLive;
+    const int *srt;     // live AND positions in processing order
+    const int *rankOf;  // per position: tentative rank (min wins)
+    const int *L0, *L1;
+    const int *level;
+    const int *lvlCnt;
+    int *lvlDone;
+    const int *gid;
+    const DevGraph *dg;
+    AndTable tab;
+    int *mapEnc;  // per position: mapped literal (>= 0) or -(slot+1)
+    int *kl0, *kl1;
+    int foldTrivial;
+    int *counter;
+    int *status;
+};
+
+__device__ __forceinline__ int resolve_map(const DedupArgs &A, int u) {
+    int e = __ldcg(&A.mapEnc[u]);
+    if (e >= 0) return e;
+    int t = __ldcg(&A.tab.vals[-e - 1]);
+    return 2 * A.srt[t];
+}
+
+// In-order dataflow over the processing order: each node waits until every
+// node of its fanins' levels has been hashed, then maps, folds and hashes.
+__global__ void __launch_bounds__(kBlock) k_dedup(DedupArgs A) {
+    __shared__ int s_chunk;
+    while (true) {
+        if (threadIdx.x == 0) s_chunk = atomicAdd(A.counter, 1);
+        __syncthreads();
+        int64_t t = (int64_t)s_chunk * kBlock + threadIdx.x;
+        __syncthreads();
+        if ((int64_t)s_chunk * kBlock >= A.nLive) break;
+        if (t >= A.nLive) continue;
+        int v = A.srt[t];
+        int lits[2] = {A.L0[v], A.L1[v]};
+        bool ok = true;
+        for (int k = 0; k < 2; k++) {
+            int u = lits[k] >> 1;
+            if (A.L0[u] < 0) continue;  // PI or constant keeps its literal
+            int lu = A.level[u];
+            if (!wait_ge(&A.lvlDone[lu], A.lvlCnt[lu], A.status)) {
+                ok = false;
+                break;
+            }
+            lits[k] = resolve_map(A, u) ^ (lits[k] & 1);
+        }
+        int lv = A.level[v];
+        if (ok) {
+            int l0 = lits[0], l1 = lits[1];
+            if (l0 > l1) {
+                int x = l0;
+                l0 = l1;
+                l1 = x;
+            }
+            const int T = 2 * A.dg[A.gid[v]].cpos;  // AIGMan: constant TRUE
+            const int F = T + 1;
+            int triv = -1;
+            if (A.foldTrivial) {
+                if (l0 == l1)
+                    triv = l0;
+                else if (l0 == (l1 ^ 1))
+                    triv = F;
+                else if (l0 == T)
+                    triv = l1;
+                else if (l1 == T)
+                    triv = l0;
+                else if (l0 == F || l1 == F)
+                    triv = F;
+            }
+            if (triv >= 0) {
+                A.mapEnc[v] = triv;
+            } else {
+                unsigned long long key = ((unsigned long long)(uint32_t)l0 << 32) | (uint32_t)l1;
+                int slot = table_insert(A.tab, key, A.rankOf[v], A.status);
+                A.kl0[t] = l0;
+                A.kl1[t] = l1;
+                A.mapEnc[v] = slot >= 0 ? -(slot + 1) : 0;
+            }
+        }
+        __threadfence();
+        atomicAdd(&A.lvlDone[lv], 1);
+    }
+}
+
+__global__ void k_winner_flags(int64_t n, const int *srt, const int *rankOf, const int *mapEnc, const int *vals,
+                               uint8_t *flags) {
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += stride) {
+        int v = srt[t];
+        int e = mapEnc[v];
+        flags[t] = (e < 0 && vals[-e - 1] == rankOf[v]) ? 1 : 0;
+    }
+}
+
+// Winners of each graph in output order: key = gid, stable.
+__global__ void k_winner_keys(int64_t n, const int *wl, const int *srt, const int *gid, uint32_t *keys, int *cntG) {
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        int g = gid[srt[wl[i]]];
+        keys[i] = (uint32_t)g;
+        atomicAdd(&cntG[g], 1);
+    }
+}
+
+__global__ void k_winner_local(int64_t n, const int *wlByG, const int *srt, const int *gid, const int *gStart,
+                               const DevGraph *dg, int *newLocalT) {
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        int t = wlByG[i];
+        int g = gid[srt[t]];
+        newLocalT[t] = dg[g].nPIs + 1 + (int)(i - gStart[g]);
+    }
+}
+
+struct OutArgs {
+    const int *srt, *tOf, *gid, *lidIn, *L0, *kl0, *kl1, *newLocalT, *mapEnc, *vals, *po;
+    const DevGraph *dgNew;
+    int *F0, *F1, *PO;
+    int64_t nPO;
+    int G;
+};
+
+__device__ __forceinline__ int local_lit(const OutArgs &A, int lit) {
+    int u = lit >> 1;
+    if (A.L0[u] < 0) return 2 * A.lidIn[u] + (lit & 1);
+    return 2 * A.newLocalT[A.tOf[u]] + (lit & 1);
+}
+
+__global__ void k_strash_out(int64_t nW, const int *wl, OutArgs A) {
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nW; i += stride) {
+        int t = wl[i];
+        int v = A.srt[t];
+        int g = A.gid[v];
+        int p = A.dgNew[g].base + A.newLocalT[t];
+        A.F0[p] = local_lit(A, A.kl0[t]);
+        A.F1[p] = local_lit(A, A.kl1[t]);
+    }
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < A.nPO; k += stride) {
+        int lit = A.po[k];
+        int u = lit >> 1;
+        int m = lit;
+        if (A.L0[u] >= 0) {
+            int e = A.mapEnc[u];
+            int base = e >= 0 ? e : 2 * A.srt[A.vals[-e - 1]];
+            m = base ^ (lit & 1);
+        }
+        A.PO[k] = local_lit(A, m);
+    }
+}
+
+}  // namespace
+
+int Engine::strash_core(Batch &b, int64_t M, const int *L0, const int *L1, const int *gidA, const int *lidIn,
+                        const int *po, bool idOrder, bool removeDangling, bool foldTrivial) {
+    const int G = b.G;
+    const int64_t nPO = b.nPO;
+    cudaStream_t s = s_;
+    size_t mark = ar_.used();
+    int *cnt = ar_.get<int>(M + 1);
+    uint8_t *dead = ar_.get<uint8_t>(M + 1);
+    uint8_t *flags = ar_.get<uint8_t>(M + 1);
+    uint8_t *liveFlag = ar_.get<uint8_t>(M + 1);
+    int *items = ar_.get<int>(M + 1);
+    int *level = ar_.get<int>(M + 1);
+    int *pending = ar_.get<int>(M + 1);
+    int *off = ar_.get<int>(M + 2);
+    int *graphLevels = ar_.get<int>(G + 1);
+    if (!cnt || !dead || !flags || !liveFlag || !items || !level || !pending || !off || !graphLevels)
+        return fail(CULS_E_OOM, "strash: scratch arena exhausted");
+    int *qc = counters_;  // [0]=head [1]=tail [2]=done [3]=count [4]=maxLevel [5]=counter
+    const unsigned gridM = grid_1d(std::max<int64_t>(M, nPO), kBlock, sms_ * 16);
+    const unsigned gridQ = (unsigned)(sms_ * 8);
+
+    // 1. liveness
+    check(cudaMemsetAsync(dead, 0, (size_t)M + 1, s), "memset");
+    if (removeDangling) {
+        check(cudaMemsetAsync(cnt, 0, sizeof(int) * (M + 1), s), "memset");
+        k_fanout_count<<<gridM, kBlock, 0, s>>>(M, L0, L1, po, nPO, cnt);
+        k_dead_seed_flags<<<gridM, kBlock, 0, s>>>(M, L0, cnt, flags);
+        check(fill_i32(items, -1, M + 1, s), "fill");
+        check(cudaMemsetAsync(qc, 0, sizeof(int) * 8, s), "memset");
+        check(compact_flags(flags, M, items, qc + 1, ar_, s), "compact");
+        k_dead_queue<<<gridQ, kBlock, 0, s>>>(WorkQueue{items, qc + 0, qc + 1, qc + 2, (int)(M + 1)}, L0, L1, cnt,
+                                              dead, status_);
+        launches_ += 4;
+    }
+    // 2. levels of live AND nodes
+    check(cudaMemsetAsync(off, 0, sizeof(int) * (M + 2), s), "memset");
+    k_live_degrees<<<gridM, kBlock, 0, s>>>(M, L0, L1, dead, pending, off, liveFlag, flags);
+    check(scan_exclusive(off, off, M + 1, nullptr, ar_, s), "scan");
+    int *cursor = cnt;  // reuse
+    check(cudaMemcpyAsync(cursor, off, sizeof(int) * (M + 1), cudaMemcpyDeviceToDevice, s), "copy");
+    // number of live edges = off[M]
+    check(cudaMemcpyAsync(hostSmall_, off + M, sizeof(int), cudaMemcpyDeviceToHost, s), "d2h");
+    if (sync()) return -1;
+    int64_t nEdges = hostSmall_[0];
+    int *adj = ar_.get<int>(nEdges + 1);
+    if (!adj) return fail(CULS_E_OOM, "strash: scratch arena exhausted");
+    k_csr_fill<<<gridM, kBlock, 0, s>>>(M, L0, L1, liveFlag, cursor, adj);
+    check(fill_i32(items, -1, M + 1, s), "fill");
+    check(cudaMemsetAsync(qc, 0, sizeof(int) * 8, s), "memset");
+    check(cudaMemsetAsync(graphLevels, 0, sizeof(int) * (G + 1), s), "memset");
+    check(cudaMemsetAsync(level, 0, sizeof(int) * (M + 1), s), "memset");
+    check(compact_flags(flags, M, items, qc + 1, ar_, s), "compact");
+    k_level_queue<<<gridQ, kBlock, 0, s>>>(WorkQueue{items, qc + 0, qc + 1, qc + 2, (int)(M + 1)}, L0, L1, off, adj,
+                                           pending, level, gidA, graphLevels, qc + 4, status_);
+    launches_ += 4;
+    // 3. live list, processing order (level, position) and tentative ranks
+    int *liveIdx = items;  // reuse: queue finished
+    check(compact_flags(liveFlag, M, liveIdx, qc + 3, ar_, s), "compact");
+    check(cudaMemcpyAsync(hostSmall_, qc, sizeof(int) * 8, cudaMemcpyDeviceToHost, s), "d2h");
+    if (sync()) return -1;
+    if (check_status("strash levels")) return -1;
+    int64_t nLive = hostSmall_[3];
+    int maxLevel = hostSmall_[4];
+    if (hostSmall_[2] != nLive) return fail(CULS_E_INVALID, "strash: the AIG has a cycle");
+    int *srt = ar_.get<int>(nLive + 1);
+    uint32_t *keys = ar_.get<uint32_t>(nLive + 1);
+    uint32_t *keys2 = ar_.get<uint32_t>(nLive + 1);
+    int *vals2 = ar_.get<int>(nLive + 1);
+    int *lvlCnt = ar_.get<int>(maxLevel + 2);
+    int *lvlDone = ar_.get<int>(maxLevel + 2);
+    int *tOf = pending;  // reuse
+    int *rankOf = off;   // reuse (only needs M entries)
+    if (!srt || !keys || !keys2 || !vals2 || !lvlCnt || !lvlDone) return fail(CULS_E_OOM, "strash: arena exhausted");
+    check(cudaMemsetAsync(lvlCnt, 0, sizeof(int) * (maxLevel + 2), s), "memset");
+    check(cudaMemsetAsync(lvlDone, 0, sizeof(int) * (maxLevel + 2), s), "memset");
+    if (nLive > 0) {
+        unsigned gl = grid_1d(nLive, kBlock, sms_ * 16);
+        k_gather_levels<<<gl, kBlock, 0, s>>>(nLive, liveIdx, level, keys, lvlCnt);
+        int bits = 1;
+        while ((1ll << bits) <= maxLevel) bits++;
+        check(cudaMemcpyAsync(vals2, liveIdx, sizeof(int) * nLive, cudaMemcpyDeviceToDevice, s), "copy");
+        check(radix_sort_pairs(keys, vals2, keys2, srt, nLive, bits, ar_, s), "sort");
+        k_inverse<<<gl, kBlock, 0, s>>>(nLive, srt, tOf);
+        // tentative rank: processing order, or id order for the CPU variants
+        k_inverse<<<gl, kBlock, 0, s>>>(nLive, idOrder ? liveIdx : srt, rankOf);
+        launches_ += 3;
+    }
+    // 4. hash in dataflow order
+    uint32_t cap = 1024;
+    while (cap < (uint32_t)std::min<int64_t>(nLive * 2, 1ll << 31)) cap <<= 1;
+    unsigned long long *tk = ar_.get<unsigned long long>(cap);
+    int *tv = ar_.get<int>(cap);
+    int *mapEnc = level == nullptr ? nullptr : ar_.get<int>(M + 1);
+    int *kl0 = ar_.get<int>(nLive + 1), *kl1 = ar_.get<int>(nLive + 1);
+    uint8_t *wflags = ar_.get<uint8_t>(nLive + 1);
+    int *wl = ar_.get<int>(nLive + 1);
+    if (!tk || !tv || !mapEnc || !kl0 || !kl1 || !wflags || !wl) return fail(CULS_E_OOM, "strash: arena exhausted");
+    check(cudaMemsetAsync(tk, 0xFF, sizeof(unsigned long long) * cap, s), "memset");
+    check(cudaMemsetAsync(tv, 0x7F, sizeof(int) * cap, s), "memset");
+    check(cudaMemsetAsync(qc + 5, 0, sizeof(int), s), "memset");
+    if (nLive > 0) {
+        DedupArgs A{nLive, srt,     rankOf, L0,     L1,     level,      lvlCnt,         lvlDone,  gidA,
+                    b.dg,  AndTable{tk, tv, cap - 1}, mapEnc, kl0, kl1, foldTrivial ? 1 : 0, qc + 5, status_};
+        k_dedup<<<(unsigned)(sms_ * 8), kBlock, 0, s>>>(A);
+        k_winner_flags<<<grid_1d(nLive, kBlock, sms_ * 16), kBlock, 0, s>>>(nLive, srt, rankOf, mapEnc, tv, wflags);
+        launches_ += 2;
+    }
+    check(compact_flags(wflags, nLive, wl, qc + 6, ar_, s), "compact");
+    // In id order (CPU variants) the winners are ranked by position, not by
+    // processing order: sort the winner list by rank.
+    check(cudaMemcpyAsync(hostSmall_, qc, sizeof(int) * 8, cudaMemcpyDeviceToHost, s), "d2h");
+    if (sync()) return -1;
+    if (check_status("strash hashing")) return -1;
+    int64_t nW = hostSmall_[6];
+    int *newLocalT = ar_.get<int>(nLive + 1);
+    int *cntG = ar_.get<int>(G + 1);
+    int *gStart = ar_.get<int>(G + 1);
+    int *wlByG = ar_.get<int>(nW + 1);
+    uint32_t *wk = ar_.get<uint32_t>(nW + 1), *wk2 = ar_.get<uint32_t>(nW + 1);
+    int *wv = ar_.get<int>(nW + 1);
+    if (!newLocalT || !cntG || !gStart || !wlByG || !wk || !wk2 || !wv) return fail(CULS_E_OOM, "strash: arena");
+    if (idOrder && nW > 0) {
+        // re-order winners by id order: key = rank (position order)
+        // (ranks fit in 31 bits)
+        int bits = 1;
+        while ((1ll << bits) <= nLive) bits++;
+        k_gather_rank<<<grid_1d(nW, kBlock, sms_ * 16), kBlock, 0, s>>>(nW, wl, srt, rankOf, wk);
+        check(cudaMemcpyAsync(wv, wl, sizeof(int) * nW, cudaMemcpyDeviceToDevice, s), "copy");
+        check(radix_sort_pairs(wk, wv, wk2, wl, nW, bits, ar_, s), "sort");
+        launches_ += 1;
+    }
+    check(cudaMemsetAsync(cntG, 0, sizeof(int) * (G + 1), s), "memset");
+    if (nW > 0) {
+        unsigned gw = grid_1d(nW, kBlock, sms_ * 16);
+        k_winner_keys<<<gw, kBlock, 0, s>>>(nW, wl, srt, gidA, wk, cntG);
+        launches_ += 1;
+        if (G > 1) {
+            int bits = 1;
+            while ((1ll << bits) < G) bits++;
+            check(cudaMemcpyAsync(wv, wl, sizeof(int) * nW, cudaMemcpyDeviceToDevice, s), "copy");
+            check(radix_sort_pairs(wk, wv, wk2, wlByG, nW, bits, ar_, s), "sort");
+        } else {
+            check(cudaMemcpyAsync(wlByG, wl, sizeof(int) * nW, cudaMemcpyDeviceToDevice, s), "copy");
+        }
+    }
+    check(scan_exclusive(cntG, gStart, G, nullptr, ar_, s), "scan");
+    std::vector<int> hCnt(G), hLev(G);
+    check(cudaMemcpyAsync(hCnt.data(), cntG, sizeof(int) * G, cudaMemcpyDeviceToHost, s), "d2h");
+    check(cudaMemcpyAsync(hLev.data(), graphLevels, sizeof(int) * G, cudaMemcpyDeviceToHost, s), "d2h");
+    if (sync()) return -1;
+    // new graph table
+    std::vector<DevGraph> ng = b.hg;
+    int64_t base = 0;
+    for (int g = 0; g < G; g++) {
+        ng[g].nAnds = hCnt[g];
+        ng[g].nLevels = hLev[g];
+        ng[g].base = (int)base;
+        base += 1 + ng[g].nPIs + hCnt[g];
+    }
+    int64_t nObjNew = base;
+    DevGraph *dgNew = reinterpret_cast<DevGraph *>(ar_.get<char>(sizeof(DevGraph) * (G + 1)));
+    int *F0n = nullptr, *F1n = nullptr, *POn = nullptr;
+    if (!dgNew) return fail(CULS_E_OOM, "strash: arena");
+    if (check(cudaMalloc(&F0n, sizeof(int) * (nObjNew + 1)), "cudaMalloc") ||
+        check(cudaMalloc(&F1n, sizeof(int) * (nObjNew + 1)), "cudaMalloc") ||
+        check(cudaMalloc(&POn, sizeof(int) * (nPO + 1)), "cudaMalloc")) {
+        cudaFree(F0n);
+        cudaFree(F1n);
+        cudaFree(POn);
+        return -1;
+    }
+    check(cudaMemcpyAsync(dgNew, ng.data(), sizeof(DevGraph) * G, cudaMemcpyHostToDevice, s), "h2d");
+    check(fill_i32(F0n, -1, nObjNew, s), "fill");
+    check(fill_i32(F1n, -1, nObjNew, s), "fill");
+    if (nW > 0) {
+        unsigned gw = grid_1d(nW, kBlock, sms_ * 16);
+        k_winner_local<<<gw, kBlock, 0, s>>>(nW, wlByG, srt, gidA, gStart, b.dg, newLocalT);
+        launches_ += 1;
+    }
+    OutArgs O{srt, tOf, gidA, lidIn, L0, kl0, kl1, newLocalT, mapEnc, tv, po, dgNew, F0n, F1n, POn, nPO, G};
+    k_strash_out<<<grid_1d(std::max<int64_t>(std::max<int64_t>(nW, nPO), 1), kBlock, sms_ * 16), kBlock, 0, s>>>(nW, wl,
+                                                                                                             O);
+    launches_ += 1;
+    check(cudaMemcpyAsync(b.dg, ng.data(), sizeof(DevGraph) * G, cudaMemcpyHostToDevice, s), "h2d");
+    if (sync()) {
+        cudaFree(F0n);
+        cudaFree(F1n);
+        cudaFree(POn);
+        return -1;
+    }
+    cudaFree(b.F0);
+    cudaFree(b.F1);
+    cudaFree(b.PO);
+    b.F0 = F0n;
+    b.F1 = F1n;
+    b.PO = POn;
+    b.hg = ng;
+    b.nObj = nObjNew;
+    ar_.reset();
+    (void)mark;
+    return check_status("strash output");
+}
+
+}  // namespace culs
