@@ -1,0 +1,281 @@
+"""culs_b200 -- B200 implementation of CULS's `rw` (AIG rewriting) and `st`
+(structural hashing with dangling-node removal).
+
+Python mirror of the reference's AIG manager surface (CULS
+src/aig_manager.h:13-26: readFile / saveFile / rewrite / strash /
+printStats) over the C ABI in include/culs_b200.h.  The compute path is the
+in-tree libculs_b200.so; importing this package fails if it is missing.
+"""
+import ctypes
+from dataclasses import dataclass
+from pathlib import Path
+
+import numpy as np
+
+_HERE = Path(__file__).resolve().parent
+LIB_PATH = _HERE / "libculs_b200.so"
+
+if not LIB_PATH.exists():
+    raise ImportError(f"{LIB_PATH} is missing: build it with `python -m culs_b200.build`")
+
+_lib = ctypes.CDLL(str(LIB_PATH))
+
+CULS_OK = 0
+ERRORS = {-1: "CULS_E_INVALID", -2: "CULS_E_OOM", -3: "CULS_E_BUDGET", -4: "CULS_E_PROBE", -5: "CULS_E_DEVICE",
+          -6: "CULS_E_IO", -7: "CULS_E_BUSY", -8: "CULS_E_NOTFOUND"}
+RW_ZEROS, RW_GPU_DEDUP, RW_DUMP = 1, 2, 4
+ST_CPU = 1
+STAT_NAMES = ["replaced", "replaced_pos", "replaced_zero", "reverted", "compromised", "pre_eval", "small_cut",
+              "new_idx", "expected", "new_nodes", "candidates"]
+DUMPS = ["reorder_f0", "reorder_f1", "reorder_out", "cuts", "selected", "replace", "new_f0", "new_f1", "choice"]
+
+
+class CulsError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class _HostGraph(ctypes.Structure):
+    _fields_ = [("nPIs", ctypes.c_int32), ("nPOs", ctypes.c_int32), ("nAnds", ctypes.c_int32),
+                ("fanin0", ctypes.POINTER(ctypes.c_int32)), ("fanin1", ctypes.POINTER(ctypes.c_int32)),
+                ("outs", ctypes.POINTER(ctypes.c_int32))]
+
+
+_vp = ctypes.c_void_p
+_ip = ctypes.POINTER(ctypes.c_int32)
+_lib.culs_create.restype = _vp
+_lib.culs_create.argtypes = [ctypes.c_size_t]
+_lib.culs_destroy.argtypes = [_vp]
+_lib.culs_last_error.restype = ctypes.c_char_p
+_lib.culs_last_error.argtypes = [_vp]
+_lib.culs_sync.argtypes = [_vp]
+_lib.culs_graph_upload.argtypes = [_vp, _ip, _ip, _ip, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                   ctypes.POINTER(_vp)]
+_lib.culs_batch_upload.argtypes = [_vp, ctypes.c_int, ctypes.POINTER(_HostGraph), ctypes.POINTER(_vp)]
+_lib.culs_graph_free.argtypes = [_vp]
+_lib.culs_graph_count.argtypes = [_vp]
+_lib.culs_graph_stats.argtypes = [_vp, ctypes.c_int, _ip, _ip, _ip, _ip]
+_lib.culs_graph_download.argtypes = [_vp, _vp, ctypes.c_int, _ip, _ip, _ip]
+_lib.culs_rw.argtypes = [_vp, _vp, ctypes.c_uint32]
+_lib.culs_st.argtypes = [_vp, _vp, ctypes.c_uint32]
+_lib.culs_rw_st.argtypes = [_vp, _vp, ctypes.c_uint32, ctypes.c_uint32]
+_lib.culs_rw_stats.argtypes = [_vp, ctypes.POINTER(ctypes.c_int64), ctypes.c_int]
+_lib.culs_dump_size.restype = ctypes.c_int64
+_lib.culs_dump_size.argtypes = [_vp, ctypes.c_int]
+_lib.culs_dump_copy.argtypes = [_vp, ctypes.c_int, _ip]
+_lib.culs_kernel_launches.restype = ctypes.c_int64
+_lib.culs_kernel_launches.argtypes = [_vp]
+_lib.culs_aiger_read.argtypes = [ctypes.c_char_p, ctypes.POINTER(_HostGraph)]
+_lib.culs_aiger_write.argtypes = [ctypes.c_char_p, ctypes.POINTER(_HostGraph)]
+_lib.culs_gen_layered.argtypes = [ctypes.c_uint64, ctypes.c_int, ctypes.c_int, ctypes.c_int64, ctypes.c_int,
+                                  ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.POINTER(_HostGraph)]
+_lib.culs_gen_multiplier.argtypes = [ctypes.c_int, ctypes.POINTER(_HostGraph)]
+_lib.culs_gen_batch.argtypes = [ctypes.c_uint64, ctypes.c_int, ctypes.c_int, ctypes.c_int64, ctypes.c_int64,
+                                ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(_HostGraph)]
+_lib.culs_host_graph_free.argtypes = [ctypes.POINTER(_HostGraph)]
+
+
+def _p(a):
+    return a.ctypes.data_as(_ip)
+
+
+@dataclass
+class Aig:
+    """AIG in the AIGMan layout: fanin arrays over objects 0..nObjs-1
+    (entries 0..nPIs are -1), literal 0 = constant TRUE."""
+    nPIs: int
+    fanin0: np.ndarray
+    fanin1: np.ndarray
+    outs: np.ndarray
+    nLevels: int = -1
+
+    @property
+    def nObjs(self):
+        return len(self.fanin0)
+
+    @property
+    def nAnds(self):
+        return self.nObjs - 1 - self.nPIs
+
+    @property
+    def nPOs(self):
+        return len(self.outs)
+
+    def host(self):
+        """A culs_host_graph view (keeps references to the arrays)."""
+        self.fanin0 = np.ascontiguousarray(self.fanin0, dtype=np.int32)
+        self.fanin1 = np.ascontiguousarray(self.fanin1, dtype=np.int32)
+        self.outs = np.ascontiguousarray(self.outs, dtype=np.int32)
+        return _HostGraph(self.nPIs, self.nPOs, self.nAnds, _p(self.fanin0), _p(self.fanin1), _p(self.outs))
+
+
+def _take(h: _HostGraph) -> Aig:
+    n = 1 + h.nPIs + h.nAnds
+    f0 = np.ctypeslib.as_array(h.fanin0, (n,)).copy()
+    f1 = np.ctypeslib.as_array(h.fanin1, (n,)).copy()
+    outs = np.ctypeslib.as_array(h.outs, (max(h.nPOs, 1),))[:h.nPOs].copy()
+    _lib.culs_host_graph_free(ctypes.byref(h))
+    return Aig(h.nPIs, f0, f1, outs)
+
+
+def _check(rc, what=""):
+    if rc != CULS_OK:
+        raise CulsError(rc, what)
+
+
+def read_aiger(path) -> Aig:
+    h = _HostGraph()
+    _check(_lib.culs_aiger_read(str(path).encode(), ctypes.byref(h)), f"read {path}")
+    return _take(h)
+
+
+def write_aiger(path, g: Aig):
+    hg = g.host()
+    _check(_lib.culs_aiger_write(str(path).encode(), ctypes.byref(hg)), f"write {path}")
+
+
+def gen_layered(seed, nPIs, nPOs, nAnds, nLayers, window, pFar=0.0, withPIs=True) -> Aig:
+    h = _HostGraph()
+    _check(_lib.culs_gen_layered(seed, nPIs, nPOs, nAnds, nLayers, window, pFar, int(withPIs), ctypes.byref(h)),
+           "gen_layered")
+    return _take(h)
+
+
+def gen_multiplier(n) -> Aig:
+    h = _HostGraph()
+    _check(_lib.culs_gen_multiplier(n, ctypes.byref(h)), "gen_multiplier")
+    return _take(h)
+
+
+def gen_batch(tag, first, count, minAnds, maxAnds, minPIs, maxPIs, threads=8):
+    arr = (_HostGraph * count)()
+    _check(_lib.culs_gen_batch(tag, first, count, minAnds, maxAnds, minPIs, maxPIs, threads, arr), "gen_batch")
+    return [_take(arr[i]) for i in range(count)]
+
+
+class Context:
+    """One GPU context (stream, rewriting library, scratch arena)."""
+
+    def __init__(self, hbm_budget=0):
+        self.h = _lib.culs_create(hbm_budget)
+        if not self.h:
+            raise CulsError(-5, _lib.culs_last_error(None).decode())
+
+    def close(self):
+        if getattr(self, "h", None):
+            _lib.culs_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def _err(self, rc, what):
+        if rc != CULS_OK:
+            raise CulsError(rc, f"{what}: {_lib.culs_last_error(self.h).decode()}")
+
+    def upload(self, g: Aig) -> "DeviceGraphs":
+        out = _vp()
+        hg = g.host()
+        self._err(_lib.culs_graph_upload(self.h, hg.fanin0, hg.fanin1, hg.outs, g.nPIs, g.nPOs, g.nAnds,
+                                         ctypes.byref(out)), "upload")
+        return DeviceGraphs(self, out)
+
+    def upload_batch(self, graphs) -> "DeviceGraphs":
+        arr = (_HostGraph * len(graphs))(*[g.host() for g in graphs])
+        out = _vp()
+        self._err(_lib.culs_batch_upload(self.h, len(graphs), arr, ctypes.byref(out)), "batch upload")
+        return DeviceGraphs(self, out)
+
+    def rw(self, d, zeros=False, gpu_dedup=True, dump=False):
+        f = (RW_ZEROS if zeros else 0) | (RW_GPU_DEDUP if gpu_dedup else 0) | (RW_DUMP if dump else 0)
+        self._err(_lib.culs_rw(self.h, d.h, f), "rw")
+
+    def st(self, d, cpu=False):
+        self._err(_lib.culs_st(self.h, d.h, ST_CPU if cpu else 0), "st")
+
+    def rw_st(self, d, zeros=False, gpu_dedup=True, cpu_st=False):
+        f = (RW_ZEROS if zeros else 0) | (RW_GPU_DEDUP if gpu_dedup else 0)
+        self._err(_lib.culs_rw_st(self.h, d.h, f, ST_CPU if cpu_st else 0), "rw;st")
+
+    def rw_stats(self):
+        out = (ctypes.c_int64 * 11)()
+        _lib.culs_rw_stats(self.h, out, 11)
+        return dict(zip(STAT_NAMES, list(out)))
+
+    def dump(self):
+        res = {}
+        for i, name in enumerate(DUMPS):
+            n = _lib.culs_dump_size(self.h, i)
+            a = np.empty(max(n, 1), np.int32)
+            _lib.culs_dump_copy(self.h, i, _p(a))
+            res[name] = a[:n]
+        return res
+
+    def kernel_launches(self):
+        return _lib.culs_kernel_launches(self.h)
+
+    def sync(self):
+        self._err(_lib.culs_sync(self.h), "sync")
+
+
+class DeviceGraphs:
+    """Handle of one or more AIGs resident in device memory."""
+
+    def __init__(self, ctx: Context, h):
+        self.ctx = ctx
+        self.h = h
+
+    def free(self):
+        if getattr(self, "h", None):
+            _lib.culs_graph_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.free()
+
+    def __len__(self):
+        return _lib.culs_graph_count(self.h)
+
+    def stats(self, i=0):
+        v = [ctypes.c_int32() for _ in range(4)]
+        _check(_lib.culs_graph_stats(self.h, i, *[ctypes.byref(x) for x in v]), "stats")
+        return dict(zip(["nPIs", "nPOs", "nAnds", "nLevels"], [x.value for x in v]))
+
+    def download(self, i=0) -> Aig:
+        s = self.stats(i)
+        n = 1 + s["nPIs"] + s["nAnds"]
+        f0 = np.empty(n, np.int32)
+        f1 = np.empty(n, np.int32)
+        outs = np.empty(max(s["nPOs"], 1), np.int32)
+        self.ctx._err(_lib.culs_graph_download(self.ctx.h, self.h, i, _p(f0), _p(f1), _p(outs)), "download")
+        return Aig(s["nPIs"], f0, f1, outs[:s["nPOs"]], s["nLevels"])
+
+
+class AIGMan:
+    """Mirror of CULS's AIGMan command surface for one graph
+    (src/aig_manager.h:13-26)."""
+
+    def __init__(self, ctx: Context = None):
+        self.ctx = ctx or Context()
+        self.dev = None
+
+    def readFile(self, path):
+        self.dev = self.ctx.upload(read_aiger(path))
+        return 1
+
+    def load(self, g: Aig):
+        self.dev = self.ctx.upload(g)
+
+    def saveFile(self, path):
+        write_aiger(path, self.dev.download())
+
+    def rewrite(self, fUseZeros=False, fGPUDeduplicate=True):
+        self.ctx.rw(self.dev, zeros=fUseZeros, gpu_dedup=fGPUDeduplicate)
+
+    def strash(self, fCPU=False):
+        self.ctx.st(self.dev, cpu=fCPU)
+
+    def printStats(self):
+        s = self.dev.stats()
+        return f"AIG stats: i/o = {s['nPIs']}/{s['nPOs']} and = {s['nAnds']} level = {s['nLevels']}"

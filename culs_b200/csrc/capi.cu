@@ -1,0 +1,185 @@
+// C ABI (include/culs_b200.h) over the batch engine.
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "culs_b200.h"
+#include "engine.cuh"
+
+struct culs_ctx {
+    culs::Engine eng;
+    std::mutex mu;  // the engine owns one stream; calls on a context serialise
+    culs::RwStats last{};
+    culs::RwDump dump;
+    std::string err;
+};
+
+struct culs_graph {
+    culs::Batch b;
+    culs_ctx *owner = nullptr;
+};
+
+namespace {
+thread_local std::string g_err;
+
+int set_err(culs_ctx *c, int rc) {
+    if (rc != CULS_OK && c) c->err = c->eng.error();
+    return rc;
+}
+}  // namespace
+
+extern "C" {
+
+culs_ctx *culs_create(size_t hbm_budget) {
+    culs_ctx *c = new culs_ctx();
+    int rc = c->eng.init(hbm_budget);
+    if (rc != CULS_OK) {
+        g_err = c->eng.error();
+        delete c;
+        return nullptr;
+    }
+    return c;
+}
+
+void culs_destroy(culs_ctx *ctx) { delete ctx; }
+
+const char *culs_last_error(culs_ctx *ctx) { return ctx ? ctx->err.c_str() : g_err.c_str(); }
+
+int culs_graph_upload(culs_ctx *ctx, const int32_t *fanin0, const int32_t *fanin1, const int32_t *outs, int32_t nPIs,
+                      int32_t nPOs, int32_t nAnds, culs_graph **g) {
+    if (!ctx || !g || (!fanin0 && nAnds) || (!fanin1 && nAnds) || (!outs && nPOs)) return CULS_E_INVALID;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    culs_graph *h = new culs_graph();
+    h->owner = ctx;
+    int32_t zero = 0;
+    const int32_t *p0 = fanin0 ? fanin0 : &zero, *p1 = fanin1 ? fanin1 : &zero, *po = outs ? outs : &zero;
+    int rc = ctx->eng.upload(h->b, 1, &p0, &p1, &po, &nPIs, &nPOs, &nAnds);
+    if (rc != CULS_OK) {
+        delete h;
+        return set_err(ctx, rc);
+    }
+    *g = h;
+    return CULS_OK;
+}
+
+int culs_batch_upload(culs_ctx *ctx, int count, const culs_host_graph *graphs, culs_graph **g) {
+    if (!ctx || !g || !graphs || count < 1) return CULS_E_INVALID;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    std::vector<const int32_t *> p0(count), p1(count), po(count);
+    std::vector<int32_t> nPI(count), nPO(count), nA(count);
+    int32_t zero = 0;
+    for (int i = 0; i < count; i++) {
+        p0[i] = graphs[i].fanin0 ? graphs[i].fanin0 : &zero;
+        p1[i] = graphs[i].fanin1 ? graphs[i].fanin1 : &zero;
+        po[i] = graphs[i].outs ? graphs[i].outs : &zero;
+        nPI[i] = graphs[i].nPIs;
+        nPO[i] = graphs[i].nPOs;
+        nA[i] = graphs[i].nAnds;
+    }
+    culs_graph *h = new culs_graph();
+    h->owner = ctx;
+    int rc = ctx->eng.upload(h->b, count, p0.data(), p1.data(), po.data(), nPI.data(), nPO.data(), nA.data());
+    if (rc != CULS_OK) {
+        delete h;
+        return set_err(ctx, rc);
+    }
+    *g = h;
+    return CULS_OK;
+}
+
+void culs_graph_free(culs_graph *g) { delete g; }
+
+int culs_graph_count(const culs_graph *g) { return g ? g->b.G : 0; }
+
+int culs_graph_stats(const culs_graph *g, int index, int32_t *nPIs, int32_t *nPOs, int32_t *nAnds, int32_t *nLevels) {
+    if (!g || index < 0 || index >= g->b.G) return CULS_E_INVALID;
+    const culs::DevGraph &d = g->b.hg[index];
+    if (nPIs) *nPIs = d.nPIs;
+    if (nPOs) *nPOs = d.nPOs;
+    if (nAnds) *nAnds = d.nAnds;
+    if (nLevels) *nLevels = d.nLevels;
+    return CULS_OK;
+}
+
+int culs_graph_download(culs_ctx *ctx, const culs_graph *g, int index, int32_t *fanin0, int32_t *fanin1,
+                        int32_t *outs) {
+    if (!ctx || !g) return CULS_E_INVALID;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    return set_err(ctx, ctx->eng.download(g->b, index, fanin0, fanin1, outs));
+}
+
+int culs_rw(culs_ctx *ctx, culs_graph *g, uint32_t flags) {
+    if (!ctx || !g) return CULS_E_INVALID;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->dump.enabled = (flags & CULS_RW_DUMP) != 0;
+    int rc = ctx->eng.rw(g->b, (flags & CULS_RW_ZEROS) != 0, (flags & CULS_RW_GPU_DEDUP) != 0, &ctx->last, &ctx->dump);
+    return set_err(ctx, rc);
+}
+
+int culs_st(culs_ctx *ctx, culs_graph *g, uint32_t flags) {
+    if (!ctx || !g) return CULS_E_INVALID;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    return set_err(ctx, ctx->eng.st(g->b, (flags & CULS_ST_CPU) != 0));
+}
+
+int culs_rw_st(culs_ctx *ctx, culs_graph *g, uint32_t rwFlags, uint32_t stFlags) {
+    int rc = culs_rw(ctx, g, rwFlags);
+    if (rc != CULS_OK) return rc;
+    return culs_st(ctx, g, stFlags);
+}
+
+int culs_rw_stats(culs_ctx *ctx, int64_t *out, int n) {
+    if (!ctx || !out) return CULS_E_INVALID;
+    const culs::RwStats &s = ctx->last;
+    int64_t v[11] = {s.replaced, s.replacedPos, s.replacedZero, s.reverted, s.compromised, s.preEval,
+                     s.smallCut, s.newIdx,      s.expected,     s.newNodes, s.candidates};
+    for (int i = 0; i < n && i < 11; i++) out[i] = v[i];
+    return CULS_OK;
+}
+
+int64_t culs_dump_size(culs_ctx *ctx, int which) {
+    if (!ctx) return -1;
+    const culs::RwDump &d = ctx->dump;
+    switch (which) {
+        case CULS_DUMP_REORDER_F0: return (int64_t)d.reorderF0.size();
+        case CULS_DUMP_REORDER_F1: return (int64_t)d.reorderF1.size();
+        case CULS_DUMP_REORDER_OUT: return (int64_t)d.reorderOut.size();
+        case CULS_DUMP_CUTS: return (int64_t)d.cuts.size();
+        case CULS_DUMP_SELECTED: return (int64_t)d.selected.size();
+        case CULS_DUMP_REPLACE: return (int64_t)d.replace.size();
+        case CULS_DUMP_NEW_F0: return (int64_t)d.newF0.size();
+        case CULS_DUMP_NEW_F1: return (int64_t)d.newF1.size();
+        case CULS_DUMP_CHOICE: return (int64_t)d.choice.size();
+        default: return -1;
+    }
+}
+
+int culs_dump_copy(culs_ctx *ctx, int which, int32_t *out) {
+    if (!ctx || !out) return CULS_E_INVALID;
+    const culs::RwDump &d = ctx->dump;
+    const std::vector<int> *v = nullptr;
+    switch (which) {
+        case CULS_DUMP_REORDER_F0: v = &d.reorderF0; break;
+        case CULS_DUMP_REORDER_F1: v = &d.reorderF1; break;
+        case CULS_DUMP_REORDER_OUT: v = &d.reorderOut; break;
+        case CULS_DUMP_CUTS: v = &d.cuts; break;
+        case CULS_DUMP_SELECTED: v = &d.selected; break;
+        case CULS_DUMP_REPLACE: v = &d.replace; break;
+        case CULS_DUMP_NEW_F0: v = &d.newF0; break;
+        case CULS_DUMP_NEW_F1: v = &d.newF1; break;
+        case CULS_DUMP_CHOICE: v = &d.choice; break;
+        default: return CULS_E_INVALID;
+    }
+    if (!v->empty()) memcpy(out, v->data(), sizeof(int32_t) * v->size());
+    return CULS_OK;
+}
+
+int64_t culs_kernel_launches(culs_ctx *ctx) { return ctx ? ctx->eng.kernelLaunches() : 0; }
+
+int culs_sync(culs_ctx *ctx) {
+    if (!ctx) return CULS_E_INVALID;
+    return set_err(ctx, ctx->eng.sync());
+}
+
+}  // extern "C"

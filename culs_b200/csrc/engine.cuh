@@ -14,10 +14,13 @@
 #include <string>
 #include <vector>
 
+#include "culs_b200.h"
 #include "prim.cuh"
 #include "rw_core.cuh"
 
 namespace culs {
+
+struct ExecCtx;
 
 struct DevGraph {
     int nPIs, nPOs, nAnds, nLevels;
@@ -82,10 +85,16 @@ class Engine {
     int check(cudaError_t e, const char *what);
     int check_status(const char *what);
     int ensure_arena(size_t bytes);
+    ExecCtx ctx();
 
     // stage helpers
-    int strash_core(Batch &b, int64_t nNodes, const int *lit0, const int *lit1, const int *gidArr, const int *po,
-                    bool cpuOrder, bool removeDangling, bool foldTrivial);
+    // Strash over M positions: L0/L1 are AIGMan-convention literals over
+    // positions (L0 < 0 marks the constant and PIs), gid/lid give each
+    // position's graph and local id (lid is read for the constant and PIs
+    // only), po the PO literals over positions.  b.dg[g].cpos must hold each
+    // graph's constant position.  Replaces b's arrays with the result.
+    int strash_core(Batch &b, int64_t M, const int *L0, const int *L1, const int *gid, const int *lid, const int *po,
+                    bool idOrder, bool removeDangling, bool foldTrivial);
 
     std::string err_;
     cudaStream_t s_ = nullptr;

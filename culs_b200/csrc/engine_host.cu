@@ -1,0 +1,279 @@
+// Engine set-up, batch upload/download and the `st` command.
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "rw_work.cuh"
+
+extern "C" const unsigned char culs_rwlib_blob[];
+extern "C" const size_t culs_rwlib_blob_size;
+
+namespace culs {
+
+int ExecCtx::status_check(const char *what) {
+    int st = 0;
+    cudaError_t e = cudaMemcpy(&st, status, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return check(e, what);
+    if (st == kDevOk) return 0;
+    cudaMemset(status, 0, sizeof(int));
+    static const char *names[] = {"ok", "dependency wait timed out", "hash table full", "traversal stack overflow",
+                                  "malformed graph", "work buffer too small"};
+    if (err) *err = std::string(what) + ": " + (st >= 0 && st <= 5 ? names[st] : "device error");
+    if (st == kDevWaitTimeout || st == kDevTableFull || st == kDevStackOverflow) return CULS_E_PROBE;
+    return CULS_E_INVALID;
+}
+
+Batch::~Batch() { release(); }
+
+void Batch::release() {
+    cudaFree(F0);
+    cudaFree(F1);
+    cudaFree(PO);
+    cudaFree(dg);
+    F0 = F1 = PO = nullptr;
+    dg = nullptr;
+    G = 0;
+    nObj = nPO = 0;
+    hg.clear();
+}
+
+// Decodes the embedded rwlib.bin (culs_b200/data/make_rwlib.py layout).
+static bool decode_lib(const unsigned char *b, size_t n, RwLib &L) {
+    if (n < 40 || memcmp(b, "CULSRWL1", 8) != 0) return false;
+    size_t cur = 40;
+    auto need = [&](size_t k) { return cur + k <= n; };
+    const int kNtt = 1 << 16;
+    if (!need(3 * (size_t)kNtt + 96 + 2 * kNumClasses)) return false;
+    const unsigned char *ph = b + cur;
+    const unsigned char *pe = ph + kNtt;
+    const unsigned char *p4 = pe + kNtt;
+    const unsigned char *cl = p4 + 96;
+    const unsigned char *nn = cl + kNtt;
+    const unsigned char *nr = nn + kNumClasses;
+    cur = (size_t)(nr + kNumClasses - b);
+    for (int t = 0; t < kNtt; t++) L.npn[t] = (uint32_t)ph[t] | ((uint32_t)pe[t] << 8) | ((uint32_t)cl[t] << 16);
+    memcpy(&L.perm4[0][0], p4, 96);
+    memcpy(L.nNodes, nn, kNumClasses);
+    memcpy(L.nRoots, nr, kNumClasses);
+    memset(L.node, 0, sizeof L.node);
+    memset(L.roots, 0, sizeof L.roots);
+    for (int c = 0; c < kNumClasses; c++) {
+        if (L.nNodes[c] > kMaxLibNodes - 4 || L.nRoots[c] > 16) return false;
+        if (!need((size_t)L.nNodes[c] * 4 + L.nRoots[c])) return false;
+        for (int i = 0; i < L.nNodes[c]; i++) {
+            const unsigned char *q = b + cur;
+            L.node[c][i] = (uint32_t)q[0] | ((uint32_t)q[1] << 8) | ((uint32_t)(q[2] & 1) << 16) |
+                           ((uint32_t)(q[3] & 1) << 17);
+            cur += 4;
+        }
+        memcpy(L.roots[c], b + cur, L.nRoots[c]);
+        cur += L.nRoots[c];
+    }
+    return cur == n;
+}
+
+Engine::Engine() = default;
+
+Engine::~Engine() {
+    if (s_) cudaStreamSynchronize(s_);
+    cudaFree(lib_);
+    cudaFree(status_);
+    cudaFree(counters_);
+    if (hostSmall_) cudaFreeHost(hostSmall_);
+    if (s_) cudaStreamDestroy(s_);
+}
+
+int Engine::fail(int code, const std::string &msg) {
+    err_ = msg;
+    return code;
+}
+
+int Engine::check(cudaError_t e, const char *what) {
+    if (e == cudaSuccess) return 0;
+    err_ = std::string(what) + ": " + cudaGetErrorString(e);
+    return CULS_E_DEVICE;
+}
+
+int Engine::sync() { return check(cudaStreamSynchronize(s_), "stream sync"); }
+
+int Engine::check_status(const char *what) {
+    ExecCtx X = ctx();
+    return X.status_check(what);
+}
+
+ExecCtx Engine::ctx() {
+    ExecCtx X;
+    X.s = s_;
+    X.ar = &ar_;
+    X.status = status_;
+    X.counters = counters_;
+    X.hostSmall = hostSmall_;
+    X.lib = lib_;
+    X.sms = sms_;
+    X.launches = &launches_;
+    X.err = &err_;
+    return X;
+}
+
+int Engine::init(size_t hbmBudget) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) return fail(CULS_E_DEVICE, "no CUDA device");
+    int rc;
+    if ((rc = check(cudaStreamCreateWithFlags(&s_, cudaStreamNonBlocking), "stream"))) return rc;
+    sms_ = num_sms();
+    RwLib *h = new RwLib;
+    bool ok = decode_lib(culs_rwlib_blob, culs_rwlib_blob_size, *h);
+    if (!ok) {
+        delete h;
+        return fail(CULS_E_INVALID, "embedded rewriting library is malformed");
+    }
+    rc = check(cudaMalloc(&lib_, sizeof(RwLib)), "cudaMalloc");
+    if (!rc) rc = check(cudaMemcpy(lib_, h, sizeof(RwLib), cudaMemcpyHostToDevice), "library upload");
+    delete h;
+    if (rc) return rc;
+    if ((rc = check(cudaMalloc(&status_, sizeof(int)), "cudaMalloc"))) return rc;
+    if ((rc = check(cudaMemset(status_, 0, sizeof(int)), "memset"))) return rc;
+    if ((rc = check(cudaMalloc(&counters_, sizeof(int) * 64), "cudaMalloc"))) return rc;
+    if ((rc = check(cudaMallocHost(&hostSmall_, sizeof(int) * 64), "cudaMallocHost"))) return rc;
+    size_t freeB = 0, totalB = 0;
+    cudaMemGetInfo(&freeB, &totalB);
+    budget_ = hbmBudget ? hbmBudget : totalB;
+    return 0;
+}
+
+int Engine::ensure_arena(size_t bytes) {
+    bytes = (bytes + (64u << 20)) & ~(size_t)((1u << 20) - 1);
+    if (bytes <= ar_.capacity()) return 0;
+    if (bytes > budget_) return fail(CULS_E_BUDGET, "request exceeds the HBM budget");
+    ar_.reset();
+    cudaError_t e = ar_.reserve(bytes);
+    if (e != cudaSuccess) return fail(CULS_E_OOM, std::string("device arena: ") + cudaGetErrorString(e));
+    return 0;
+}
+
+// ------------------------------------------------------------ upload
+int Engine::upload(Batch &b, int count, const int32_t *const *f0, const int32_t *const *f1,
+                   const int32_t *const *outs, const int32_t *nPIs, const int32_t *nPOs, const int32_t *nAnds) {
+    if (count < 1) return fail(CULS_E_INVALID, "upload: no graphs");
+    std::vector<DevGraph> hg(count);
+    int64_t nObj = 0, nPO = 0;
+    for (int g = 0; g < count; g++) {
+        if (nPIs[g] < 0 || nPOs[g] < 0 || nAnds[g] < 0) return fail(CULS_E_INVALID, "upload: negative size");
+        hg[g] = DevGraph{nPIs[g], nPOs[g], nAnds[g], 0, (int)nObj, (int)nPO, (int)nObj, 0};
+        nObj += 1 + (int64_t)nPIs[g] + nAnds[g];
+        nPO += nPOs[g];
+        if (nObj >= (1ll << 29)) return fail(CULS_E_INVALID, "upload: batch too large for 30-bit node positions");
+    }
+    // validate: fanins precede their node, literals in range
+    for (int g = 0; g < count; g++) {
+        const int n = 1 + nPIs[g] + nAnds[g];
+        for (int i = nPIs[g] + 1; i < n; i++) {
+            int a = f0[g][i], c = f1[g][i];
+            if (a < 0 || c < 0 || (a >> 1) >= i || (c >> 1) >= i)
+                return fail(CULS_E_INVALID, "upload: fanin literal out of range or not topological");
+        }
+        for (int k = 0; k < nPOs[g]; k++)
+            if (outs[g][k] < 0 || (outs[g][k] >> 1) >= n) return fail(CULS_E_INVALID, "upload: PO literal out of range");
+    }
+    // depth (AIGMan::readFromMemory's nLevels) on the host while staging
+    std::vector<int32_t> hF0(nObj), hF1(nObj), hPO(std::max<int64_t>(nPO, 1));
+    for (int g = 0; g < count; g++) {
+        const int n = 1 + nPIs[g] + nAnds[g];
+        int64_t base = hg[g].base;
+        std::vector<int> d(n, 0);
+        int mx = 0;
+        for (int i = 0; i < n; i++) {
+            if (i <= nPIs[g]) {
+                hF0[base + i] = hF1[base + i] = -1;
+                continue;
+            }
+            hF0[base + i] = f0[g][i];
+            hF1[base + i] = f1[g][i];
+            d[i] = 1 + std::max(d[f0[g][i] >> 1], d[f1[g][i] >> 1]);
+            mx = std::max(mx, d[i]);
+        }
+        hg[g].nLevels = mx;
+        if (nPOs[g]) memcpy(&hPO[hg[g].poOff], outs[g], sizeof(int32_t) * nPOs[g]);
+    }
+    b.release();
+    int rc;
+    if ((rc = check(cudaMalloc(&b.F0, sizeof(int) * nObj), "cudaMalloc"))) return rc;
+    if ((rc = check(cudaMalloc(&b.F1, sizeof(int) * nObj), "cudaMalloc"))) return rc;
+    if ((rc = check(cudaMalloc(&b.PO, sizeof(int) * std::max<int64_t>(nPO, 1)), "cudaMalloc"))) return rc;
+    if ((rc = check(cudaMalloc(&b.dg, sizeof(DevGraph) * count), "cudaMalloc"))) return rc;
+    cudaMemcpyAsync(b.F0, hF0.data(), sizeof(int) * nObj, cudaMemcpyHostToDevice, s_);
+    cudaMemcpyAsync(b.F1, hF1.data(), sizeof(int) * nObj, cudaMemcpyHostToDevice, s_);
+    if (nPO) cudaMemcpyAsync(b.PO, hPO.data(), sizeof(int) * nPO, cudaMemcpyHostToDevice, s_);
+    cudaMemcpyAsync(b.dg, hg.data(), sizeof(DevGraph) * count, cudaMemcpyHostToDevice, s_);
+    b.G = count;
+    b.nObj = nObj;
+    b.nPO = nPO;
+    b.hg = hg;
+    return sync();
+}
+
+int Engine::download(const Batch &b, int g, int32_t *f0, int32_t *f1, int32_t *outs) {
+    if (g < 0 || g >= b.G) return fail(CULS_E_INVALID, "download: graph index out of range");
+    const DevGraph &d = b.hg[g];
+    const int64_t n = 1 + (int64_t)d.nPIs + d.nAnds;
+    int rc;
+    if (f0 && (rc = check(cudaMemcpyAsync(f0, b.F0 + d.base, sizeof(int) * n, cudaMemcpyDeviceToHost, s_), "d2h")))
+        return rc;
+    if (f1 && (rc = check(cudaMemcpyAsync(f1, b.F1 + d.base, sizeof(int) * n, cudaMemcpyDeviceToHost, s_), "d2h")))
+        return rc;
+    if (outs && d.nPOs &&
+        (rc = check(cudaMemcpyAsync(outs, b.PO + d.poOff, sizeof(int) * d.nPOs, cudaMemcpyDeviceToHost, s_), "d2h")))
+        return rc;
+    return sync();
+}
+
+// ---------------------------------------------------------------- st
+namespace {
+
+__global__ void k_st_prep(int64_t N, int G, const DevGraph *dg, const int *F0, const int *F1, int *L0, int *L1,
+                          int *gid, int *lid) {
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < N; p += stride) {
+        int g = graph_of_pos(dg, G, (int)p);
+        int base = dg[g].base;
+        int local = (int)p - base;
+        gid[p] = g;
+        lid[p] = local;
+        if (local <= dg[g].nPIs) {
+            L0[p] = L1[p] = -1;
+        } else {
+            L0[p] = F0[p] + 2 * base;
+            L1[p] = F1[p] + 2 * base;
+        }
+    }
+}
+
+__global__ void k_st_po(int64_t nPO, int G, const DevGraph *dg, const int *PO, int *po) {
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < nPO; k += stride)
+        po[k] = PO[k] + 2 * dg[graph_of_po(dg, G, (int)k)].base;
+}
+
+}  // namespace
+
+int Engine::st(Batch &b, bool cpuOrder) {
+    const int64_t N = b.nObj;
+    int rc;
+    if ((rc = ensure_arena((size_t)N * 160 + (size_t)b.nPO * 8 + ((size_t)64 << 20)))) return rc;
+    ar_.reset();
+    int *L0 = ar_.get<int>(N), *L1 = ar_.get<int>(N), *gid = ar_.get<int>(N), *lid = ar_.get<int>(N);
+    int *po = ar_.get<int>(b.nPO + 1);
+    if (!L0 || !L1 || !gid || !lid || !po) return fail(CULS_E_OOM, "st: arena exhausted");
+    for (auto &g : b.hg) g.cpos = g.base;
+    if ((rc = check(cudaMemcpyAsync(b.dg, b.hg.data(), sizeof(DevGraph) * b.G, cudaMemcpyHostToDevice, s_), "h2d")))
+        return rc;
+    ExecCtx X = ctx();
+    k_st_prep<<<X.grid(N), kBlock, 0, s_>>>(N, b.G, b.dg, b.F0, b.F1, L0, L1, gid, lid);
+    if (b.nPO) k_st_po<<<X.grid(b.nPO), kBlock, 0, s_>>>(b.nPO, b.G, b.dg, b.PO, po);
+    launches_ += 2;
+    // `st` = GPU strash (frontier order, trivial folding); `st -c` = CPU strash
+    // (id order, no folding), both with dangling removal
+    return strash_core(b, N, L0, L1, gid, lid, po, cpuOrder, true, !cpuOrder);
+}
+
+}  // namespace culs

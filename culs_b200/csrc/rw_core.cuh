@@ -327,4 +327,155 @@ CULS_HD int and_lookup(const AndTable &t, int in0, int in1, int c0, int c1, int 
     return table_find(t, and_key(in0, in1, c0, c1), status);
 }
 
+// --------------------------------------------------------- evaluation
+struct EvalIn {
+    const int *L0, *L1;  // fanin literals (the constant and PIs point at the constant)
+    const int *ref;      // fanout counts incl. PO references
+    const int *level;
+    const RwLib *lib;
+    AndTable tab;
+    int *status;
+};
+
+// 8-entry reference table of CalcMFFC (src/algorithms/rewrite.cu:296-316)
+struct MffcTab {
+    int size;
+    int id[8];
+    int num[8];
+};
+
+// Decrease, src/algorithms/rewrite.cu:296-309
+CULS_HD int mffc_decrease(int v, MffcTab &t, const int *leaves, const int *ref) {
+    for (int i = 0; i < 4; i++)
+        if (v == leaves[i]) return 1;
+    for (int i = 0; i < t.size; i++)
+        if (t.id[i] == v) return --t.num[i];
+    if (t.size == 8) return 1;
+    t.id[t.size] = v;
+    t.num[t.size] = ref[v] - 1;
+    t.size++;
+    return ref[v] - 1;
+}
+
+// IsDeleted, src/algorithms/rewrite.cu:312-316
+CULS_HD int mffc_deleted(int v, const MffcTab &t) {
+    for (int i = 0; i < t.size; i++)
+        if (t.id[i] == v) return t.num[i] == 0;
+    return 0;
+}
+
+// CalcMFFC, src/algorithms/rewrite.cu:319-326, with the recursion unrolled
+// onto a stack of at most nine frames (a node is entered only when its table
+// count reaches zero, which happens once per table entry).
+CULS_HD int mffc_size(const EvalIn &E, int root, const int *leaves, MffcTab &t) {
+    int node[10], state[10], ans[10];
+    int sp = 0;
+    node[0] = root;
+    state[0] = 0;
+    ans[0] = 1;
+    while (true) {
+        int cur = node[sp];
+        if (state[sp] < 2) {
+            int v = (state[sp] == 0 ? E.L0[cur] : E.L1[cur]) >> 1;
+            state[sp]++;
+            if (mffc_decrease(v, t, leaves, E.ref) == 0) {
+                if (sp + 1 >= 10) {
+                    set_status(E.status, kDevStackOverflow);
+                    return ans[0];
+                }
+                sp++;
+                node[sp] = v;
+                state[sp] = 0;
+                ans[sp] = 1;
+            }
+            continue;
+        }
+        if (sp == 0) return ans[0];
+        ans[sp - 1] += ans[sp];
+        sp--;
+    }
+}
+
+// Number of library nodes the subgraph rooted at rt adds: unmatched nodes
+// reachable from rt through unmatched nodes (Eval, rewrite.cu:369-374).
+// unmatched has bit j set for library node j without a match.
+CULS_HD int lib_added(const RwLib *lib, int cls, int rt, uint64_t unmatched) {
+    if (!((unmatched >> rt) & 1ull)) return 0;
+    uint64_t reach = 1ull << rt;
+    for (int j = rt; j >= 4; j--) {
+        if (!((reach >> j) & 1ull)) continue;
+        uint32_t w = lib->node[cls][j - 4];
+        int f0 = ln_f0(w), f1 = ln_f1(w);
+        if ((unmatched >> f0) & 1ull) reach |= 1ull << f0;
+        if ((unmatched >> f1) & 1ull) reach |= 1ull << f1;
+    }
+    return popc64(reach);
+}
+
+// EvaluateNode for one node, src/algorithms/rewrite.cu:378-447.  `cuts`
+// holds the node's 8 slots; match/mlev are 54-entry scratch arrays.
+// Writes the chosen slot (or -1) and root index.
+CULS_HD void eval_node(const EvalIn &E, int q, int cpos, const Cut *cuts, bool useZeros, int *match, int *mlev,
+                       int &bestCut, int &bestOut) {
+    int reduction = -1, bestLevel = 99999999;
+    bestCut = -1;
+    bestOut = -1;
+    for (int i = 0; i < 8; i++) {
+        const Cut &c = cuts[i];
+        if (!c.used || c.nLeaves < 3) continue;
+        int leaves[4] = {c.leaves[0], c.leaves[1], c.leaves[2], c.nLeaves == 3 ? cpos : c.leaves[3]};
+        MffcTab tab;
+        tab.size = 0;
+        int saved = mffc_size(E, q, leaves, tab);
+        uint32_t npn = E.lib->npn[c.tt];
+        int uPhase = npn_phase(npn), cls = npn_class(npn);
+        const uint8_t *perm = E.lib->perm4[npn_perm(npn)];
+        int isC = 0;
+        for (int j = 0; j < 4; j++) {
+            match[j] = leaves[perm[j]];
+            mlev[j] = E.level[match[j]];
+            if (uPhase >> j & 1) isC |= 1 << j;
+        }
+        uint64_t unmatched = 0;
+        const int nn = E.lib->nNodes[cls];
+        for (int j = 0; j < nn; j++) {
+            int num = j + 4;
+            uint32_t w = E.lib->node[cls][j];
+            int in0 = ln_f0(w), in1 = ln_f1(w);
+            mlev[num] = 1 + (mlev[in0] > mlev[in1] ? mlev[in0] : mlev[in1]);
+            match[num] = -1;
+            bool uin0 = in0 >= 4 && ((unmatched >> in0) & 1ull);
+            bool uin1 = in1 >= 4 && ((unmatched >> in1) & 1ull);
+            if (uin0 || uin1 || match[in0] == q || match[in1] == q) {
+                unmatched |= 1ull << num;
+                continue;
+            }
+            // the reference's isC mask only has input bits (0..3)
+            int cc0 = (in0 < 4 ? ((isC >> in0) & 1) : 0) ^ ln_c0(w);
+            int cc1 = (in1 < 4 ? ((isC >> in1) & 1) : 0) ^ ln_c1(w);
+            int nodeId = and_lookup(E.tab, match[in0], match[in1], cc0, cc1, E.status);
+            if (nodeId != -1 && !mffc_deleted(nodeId, tab)) {
+                match[num] = nodeId;
+                mlev[num] = E.level[nodeId];
+            } else {
+                unmatched |= 1ull << num;
+            }
+        }
+        const int nr = E.lib->nRoots[cls];
+        for (int out = 0; out < nr; out++) {
+            int rt = E.lib->roots[cls][out];
+            if (match[rt] == q) continue;
+            int added = lib_added(E.lib, cls, rt, unmatched);
+            int rtLevel = mlev[rt];
+            int gain = saved - added;
+            if (gain < 0 || (gain == 0 && !useZeros)) continue;
+            if (gain < reduction || (gain == reduction && rtLevel >= bestLevel)) continue;
+            reduction = gain;
+            bestLevel = rtLevel;
+            bestCut = i;
+            bestOut = out;
+        }
+    }
+}
+
 }  // namespace culs

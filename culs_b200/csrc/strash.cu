@@ -153,8 +153,9 @@ __global__ void k_inverse(int64_t n, const int *srt, int *tOf) {
 
 struct DedupArgs {
     int64_t nLive;
-    const int *srt;     // live AND positions in processing order
-    const int *rankOf;  // per position: tentative rank (min wins)
+    const int *srt;        // live AND positions in processing order
+    const int *rankOf;     // per position: tentative rank (min wins)
+    const int *posOfRank;  // rank -> position
     const int *L0, *L1;
     const int *level;
     const int *lvlCnt;
@@ -172,8 +173,8 @@ struct DedupArgs {
 __device__ __forceinline__ int resolve_map(const DedupArgs &A, int u) {
     int e = __ldcg(&A.mapEnc[u]);
     if (e >= 0) return e;
-    int t = __ldcg(&A.tab.vals[-e - 1]);
-    return 2 * A.srt[t];
+    int r = __ldcg(&A.tab.vals[-e - 1]);
+    return 2 * A.posOfRank[r];
 }
 
 // In-order dataflow over the processing order: each node waits until every
@@ -183,9 +184,10 @@ __global__ void __launch_bounds__(kBlock) k_dedup(DedupArgs A) {
     while (true) {
         if (threadIdx.x == 0) s_chunk = atomicAdd(A.counter, 1);
         __syncthreads();
-        int64_t t = (int64_t)s_chunk * kBlock + threadIdx.x;
+        const int64_t start = (int64_t)s_chunk * kBlock;
         __syncthreads();
-        if ((int64_t)s_chunk * kBlock >= A.nLive) break;
+        if (start >= A.nLive) break;
+        const int64_t t = start + threadIdx.x;
         if (t >= A.nLive) continue;
         int v = A.srt[t];
         int lits[2] = {A.L0[v], A.L1[v]};
@@ -248,6 +250,12 @@ __global__ void k_winner_flags(int64_t n, const int *srt, const int *rankOf, con
     }
 }
 
+__global__ void k_gather_rank(int64_t n, const int *wl, const int *srt, const int *rankOf, uint32_t *keys) {
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+        keys[i] = (uint32_t)rankOf[srt[wl[i]]];
+}
+
 // Winners of each graph in output order: key = gid, stable.
 __global__ void k_winner_keys(int64_t n, const int *wl, const int *srt, const int *gid, uint32_t *keys, int *cntG) {
     int64_t stride = (int64_t)gridDim.x * blockDim.x;
@@ -269,7 +277,7 @@ __global__ void k_winner_local(int64_t n, const int *wlByG, const int *srt, cons
 }
 
 struct OutArgs {
-    const int *srt, *tOf, *gid, *lidIn, *L0, *kl0, *kl1, *newLocalT, *mapEnc, *vals, *po;
+    const int *srt, *posOfRank, *tOf, *gid, *lidIn, *L0, *kl0, *kl1, *newLocalT, *mapEnc, *vals, *po;
     const DevGraph *dgNew;
     int *F0, *F1, *PO;
     int64_t nPO;
@@ -289,8 +297,11 @@ __global__ void k_strash_out(int64_t nW, const int *wl, OutArgs A) {
         int v = A.srt[t];
         int g = A.gid[v];
         int p = A.dgNew[g].base + A.newLocalT[t];
-        A.F0[p] = local_lit(A, A.kl0[t]);
-        A.F1[p] = local_lit(A, A.kl1[t]);
+        // the reference forms keys over the final numbering, so the
+        // smaller literal comes first there
+        int a = local_lit(A, A.kl0[t]), b = local_lit(A, A.kl1[t]);
+        A.F0[p] = a < b ? a : b;
+        A.F1[p] = a < b ? b : a;
     }
     for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < A.nPO; k += stride) {
         int lit = A.po[k];
@@ -298,7 +309,7 @@ __global__ void k_strash_out(int64_t nW, const int *wl, OutArgs A) {
         int m = lit;
         if (A.L0[u] >= 0) {
             int e = A.mapEnc[u];
-            int base = e >= 0 ? e : 2 * A.srt[A.vals[-e - 1]];
+            int base = e >= 0 ? e : 2 * A.posOfRank[A.vals[-e - 1]];
             m = base ^ (lit & 1);
         }
         A.PO[k] = local_lit(A, m);
@@ -399,7 +410,7 @@ int Engine::strash_core(Batch &b, int64_t M, const int *L0, const int *L1, const
     while (cap < (uint32_t)std::min<int64_t>(nLive * 2, 1ll << 31)) cap <<= 1;
     unsigned long long *tk = ar_.get<unsigned long long>(cap);
     int *tv = ar_.get<int>(cap);
-    int *mapEnc = level == nullptr ? nullptr : ar_.get<int>(M + 1);
+    int *mapEnc = ar_.get<int>(M + 1);
     int *kl0 = ar_.get<int>(nLive + 1), *kl1 = ar_.get<int>(nLive + 1);
     uint8_t *wflags = ar_.get<uint8_t>(nLive + 1);
     int *wl = ar_.get<int>(nLive + 1);
@@ -408,7 +419,7 @@ int Engine::strash_core(Batch &b, int64_t M, const int *L0, const int *L1, const
     check(cudaMemsetAsync(tv, 0x7F, sizeof(int) * cap, s), "memset");
     check(cudaMemsetAsync(qc + 5, 0, sizeof(int), s), "memset");
     if (nLive > 0) {
-        DedupArgs A{nLive, srt,     rankOf, L0,     L1,     level,      lvlCnt,         lvlDone,  gidA,
+        DedupArgs A{nLive, srt,     rankOf, idOrder ? liveIdx : srt, L0,     L1,     level,      lvlCnt,         lvlDone,  gidA,
                     b.dg,  AndTable{tk, tv, cap - 1}, mapEnc, kl0, kl1, foldTrivial ? 1 : 0, qc + 5, status_};
         k_dedup<<<(unsigned)(sms_ * 8), kBlock, 0, s>>>(A);
         k_winner_flags<<<grid_1d(nLive, kBlock, sms_ * 16), kBlock, 0, s>>>(nLive, srt, rankOf, mapEnc, tv, wflags);
@@ -486,7 +497,7 @@ int Engine::strash_core(Batch &b, int64_t M, const int *L0, const int *L1, const
         k_winner_local<<<gw, kBlock, 0, s>>>(nW, wlByG, srt, gidA, gStart, b.dg, newLocalT);
         launches_ += 1;
     }
-    OutArgs O{srt, tOf, gidA, lidIn, L0, kl0, kl1, newLocalT, mapEnc, tv, po, dgNew, F0n, F1n, POn, nPO, G};
+    OutArgs O{srt, idOrder ? liveIdx : srt, tOf, gidA, lidIn, L0, kl0, kl1, newLocalT, mapEnc, tv, po, dgNew, F0n, F1n, POn, nPO, G};
     k_strash_out<<<grid_1d(std::max<int64_t>(std::max<int64_t>(nW, nPO), 1), kBlock, sms_ * 16), kBlock, 0, s>>>(nW, wl,
                                                                                                              O);
     launches_ += 1;

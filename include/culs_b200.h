@@ -60,6 +60,82 @@ int culs_gen_multiplier(int n, culs_host_graph *out);
 int culs_gen_batch(uint64_t tag, int first, int count, int64_t minAnds, int64_t maxAnds, int minPIs, int maxPIs,
                    int threads, culs_host_graph *out);
 
+/* ------------------------------------------------------ device engine */
+typedef struct culs_ctx culs_ctx;     /* one GPU context: stream, library, scratch arena */
+typedef struct culs_graph culs_graph; /* one or more AIGs resident in device memory */
+
+/* flags of culs_rw: `rw -z` (fUseZeros) and `rw -d` (fGPUDeduplicate);
+ * CULS_RW_DUMP records per-node intermediate results for parity checks
+ * (single-graph handles only). */
+#define CULS_RW_ZEROS 1u
+#define CULS_RW_GPU_DEDUP 2u
+#define CULS_RW_DUMP 4u
+/* flag of culs_st: `st -c` (CPU strash ordering, no trivial folding) */
+#define CULS_ST_CPU 1u
+
+/* Creates a context on the current CUDA device.  hbm_budget (bytes, 0 = the
+ * device's memory) bounds the scratch arena; a request above it fails with
+ * CULS_E_BUDGET.  Replaces AIGMan construction (CULS src/aig_manager.cu:22-33).
+ * Returns NULL on failure; culs_last_error(NULL) then explains why. */
+culs_ctx *culs_create(size_t hbm_budget);
+void culs_destroy(culs_ctx *ctx);
+const char *culs_last_error(culs_ctx *ctx);
+int culs_sync(culs_ctx *ctx);
+
+/* Copies one AIG (AIGMan layout, see above) into device memory; replaces
+ * AIGMan::readFile + toDevice (src/aig_manager.cu:80-229,294-312).  The
+ * caller keeps ownership of the input arrays. */
+int culs_graph_upload(culs_ctx *ctx, const int32_t *fanin0, const int32_t *fanin1, const int32_t *outs, int32_t nPIs,
+                      int32_t nPOs, int32_t nAnds, culs_graph **g);
+/* Copies `count` AIGs into one device-resident batch. */
+int culs_batch_upload(culs_ctx *ctx, int count, const culs_host_graph *graphs, culs_graph **g);
+void culs_graph_free(culs_graph *g);
+int culs_graph_count(const culs_graph *g);
+/* Sizes and level of graph `index` (AIGMan::printStats, src/aig_manager.cu:604-612). */
+int culs_graph_stats(const culs_graph *g, int index, int32_t *nPIs, int32_t *nPOs, int32_t *nAnds, int32_t *nLevels);
+/* Copies graph `index` back (AIGMan::toHost, src/aig_manager.cu:314-336);
+ * fanin arrays need 1 + nPIs + nAnds entries, outs nPOs. */
+int culs_graph_download(culs_ctx *ctx, const culs_graph *g, int index, int32_t *fanin0, int32_t *fanin1,
+                        int32_t *outs);
+
+/* `rw` on every graph of the handle: AIGMan::rewrite(fUseZeros,
+ * fGPUDeduplicate) (CULS src/aig_manager.cu:632-672, command handler
+ * src/command_manager.cpp:81-95). */
+int culs_rw(culs_ctx *ctx, culs_graph *g, uint32_t flags);
+/* `st` on every graph of the handle: AIGMan::strash(fCPU)
+ * (src/aig/strash.cu:317-503, handler src/command_manager.cpp:115-128). */
+int culs_st(culs_ctx *ctx, culs_graph *g, uint32_t flags);
+/* `rw; st` in one call (the rewrite-then-strash step of the reference's
+ * scripts), on one graph or a whole batch. */
+int culs_rw_st(culs_ctx *ctx, culs_graph *g, uint32_t rwFlags, uint32_t stFlags);
+
+/* Counters of the last culs_rw (the summary CPUSolver::Rewrite prints,
+ * src/algorithms/rewrite.cu:896-897,926): replaced, replaced with positive
+ * gain, replaced with zero gain, reverted, compromised, without a cut, small
+ * cut, without a replacement, real reduction, new nodes built, candidates. */
+int culs_rw_stats(culs_ctx *ctx, int64_t *out, int n);
+
+/* Per-node intermediate results of the last culs_rw run with CULS_RW_DUMP,
+ * indexed by the ids CPUSolver::Reorder assigns: fanin literals after the
+ * reorder (AIGER constant convention), the 8 cut slots per node (9 ints:
+ * used, nLeaves, leaves[4], truth table, signature, value), the selected cut
+ * plus root index, replace[] after the rebuild, the rebuilt new nodes'
+ * fanins, the choice-loop outcome per node.  For parity checks. */
+#define CULS_DUMP_REORDER_F0 0
+#define CULS_DUMP_REORDER_F1 1
+#define CULS_DUMP_REORDER_OUT 2
+#define CULS_DUMP_CUTS 3
+#define CULS_DUMP_SELECTED 4
+#define CULS_DUMP_REPLACE 5
+#define CULS_DUMP_NEW_F0 6
+#define CULS_DUMP_NEW_F1 7
+#define CULS_DUMP_CHOICE 8
+int64_t culs_dump_size(culs_ctx *ctx, int which);
+int culs_dump_copy(culs_ctx *ctx, int which, int32_t *out);
+
+/* Kernels this context has launched so far. */
+int64_t culs_kernel_launches(culs_ctx *ctx);
+
 #ifdef __cplusplus
 }
 #endif
