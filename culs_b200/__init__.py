@@ -66,6 +66,10 @@ _lib.culs_dump_size.argtypes = [_vp, ctypes.c_int]
 _lib.culs_dump_copy.argtypes = [_vp, ctypes.c_int, _ip]
 _lib.culs_kernel_launches.restype = ctypes.c_int64
 _lib.culs_kernel_launches.argtypes = [_vp]
+_lib.culs_graph_clone.argtypes = [_vp, _vp, ctypes.POINTER(_vp)]
+_lib.culs_profile.argtypes = [_vp, ctypes.c_int]
+_lib.culs_mark.argtypes = [_vp, ctypes.c_int]
+_lib.culs_profile_read.argtypes = [_vp, ctypes.POINTER(ctypes.c_float), ctypes.c_int]
 _lib.culs_aiger_read.argtypes = [ctypes.c_char_p, ctypes.POINTER(_HostGraph)]
 _lib.culs_aiger_write.argtypes = [ctypes.c_char_p, ctypes.POINTER(_HostGraph)]
 _lib.culs_gen_layered.argtypes = [ctypes.c_uint64, ctypes.c_int, ctypes.c_int, ctypes.c_int64, ctypes.c_int,
@@ -211,6 +215,26 @@ class Context:
             _lib.culs_dump_copy(self.h, i, _p(a))
             res[name] = a[:n]
         return res
+
+    PROFILE_NAMES = ["front", "enumerate", "evaluate", "replace", "choice", "redundancy", "dedup", "st",
+                     "k_enumerate", "k_evaluate", "k_dedup", "user"]
+
+    def clone(self, d, into=None):
+        out = _vp(into.h if into is not None else None)
+        self._err(_lib.culs_graph_clone(self.h, d.h, ctypes.byref(out)), "clone")
+        return into if into is not None else DeviceGraphs(self, out)
+
+    def profile(self, on=True):
+        _lib.culs_profile(self.h, int(on))
+
+    def mark(self, slot):
+        _lib.culs_mark(self.h, slot)
+
+    def profile_read(self):
+        n = len(self.PROFILE_NAMES)
+        out = (ctypes.c_float * n)()
+        _lib.culs_profile_read(self.h, out, n)
+        return dict(zip(self.PROFILE_NAMES, [float(x) for x in out]))
 
     def kernel_launches(self):
         return _lib.culs_kernel_launches(self.h)

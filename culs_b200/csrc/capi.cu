@@ -177,6 +177,44 @@ int culs_dump_copy(culs_ctx *ctx, int which, int32_t *out) {
 
 int64_t culs_kernel_launches(culs_ctx *ctx) { return ctx ? ctx->eng.kernelLaunches() : 0; }
 
+int culs_graph_clone(culs_ctx *ctx, const culs_graph *src, culs_graph **dst) {
+    if (!ctx || !src || !dst) return CULS_E_INVALID;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    culs_graph *h = *dst ? *dst : new culs_graph();
+    h->owner = ctx;
+    int rc = ctx->eng.clone(src->b, h->b);
+    if (rc != CULS_OK) {
+        if (!*dst) delete h;
+        return set_err(ctx, rc);
+    }
+    *dst = h;
+    return CULS_OK;
+}
+
+int culs_profile(culs_ctx *ctx, int enable) {
+    if (!ctx) return CULS_E_INVALID;
+    ctx->eng.setProfile(enable != 0);
+    return CULS_OK;
+}
+
+int culs_mark(culs_ctx *ctx, int slot) {
+    if (!ctx || slot < 0 || slot > 1) return CULS_E_INVALID;
+    ctx->eng.mark(culs::kMkUser0 + slot);
+    return CULS_OK;
+}
+
+int culs_profile_read(culs_ctx *ctx, float *ms, int n) {
+    if (!ctx || !ms) return CULS_E_INVALID;
+    using namespace culs;
+    const int pairs[][2] = {{kMkRwStart, kMkFront}, {kMkFront, kMkEnum},     {kMkEnum, kMkEval},
+                            {kMkEval, kMkReplace},  {kMkReplace, kMkChoice}, {kMkChoice, kMkRedund},
+                            {kMkRedund, kMkRwEnd},  {kMkStStart, kMkStEnd},  {kMkEnumK0, kMkEnumK1},
+                            {kMkEvalK0, kMkEvalK1}, {kMkDedupK0, kMkDedupK1}, {kMkUser0, kMkUser1}};
+    const int np = (int)(sizeof pairs / sizeof pairs[0]);
+    for (int i = 0; i < n && i < np; i++) ms[i] = ctx->eng.elapsed(pairs[i][0], pairs[i][1]);
+    return CULS_OK;
+}
+
 int culs_sync(culs_ctx *ctx) {
     if (!ctx) return CULS_E_INVALID;
     return set_err(ctx, ctx->eng.sync());

@@ -60,6 +60,29 @@ struct RwDump {
     std::vector<int> choice;                            // per node outcome code
 };
 
+// CUDA-event marks recorded on the engine stream when profiling is on.
+enum Mark : int {
+    kMkRwStart = 0,
+    kMkFront,
+    kMkEnum,
+    kMkEval,
+    kMkReplace,
+    kMkChoice,
+    kMkRedund,
+    kMkRwEnd,
+    kMkStStart,
+    kMkStEnd,
+    kMkEnumK0,
+    kMkEnumK1,
+    kMkEvalK0,
+    kMkEvalK1,
+    kMkDedupK0,
+    kMkDedupK1,
+    kMkUser0,
+    kMkUser1,
+    kNumMarks
+};
+
 class Engine {
   public:
     Engine();
@@ -78,6 +101,10 @@ class Engine {
     size_t budget() const { return budget_; }
     size_t arenaHighWater() const { return ar_.high_water(); }
     int kernelLaunches() const { return launches_; }
+    void setProfile(bool on) { prof_ = on; }
+    void mark(int m);
+    float elapsed(int a, int b);  // ms between two recorded marks (-1 if missing)
+    int clone(const Batch &src, Batch &dst);
     void resetLaunchCount() { launches_ = 0; }
 
   private:
@@ -106,6 +133,9 @@ class Engine {
     Arena ar_;
     int launches_ = 0;
     int sms_ = 148;
+    bool prof_ = false;
+    cudaEvent_t ev_[kNumMarks] = {};
+    bool evSet_[kNumMarks] = {};
 };
 
 }  // namespace culs

@@ -80,6 +80,8 @@ Engine::~Engine() {
     cudaFree(status_);
     cudaFree(counters_);
     if (hostSmall_) cudaFreeHost(hostSmall_);
+    for (auto &e : ev_)
+        if (e) cudaEventDestroy(e);
     if (s_) cudaStreamDestroy(s_);
 }
 
@@ -112,6 +114,8 @@ ExecCtx Engine::ctx() {
     X.sms = sms_;
     X.launches = &launches_;
     X.err = &err_;
+    X.ev = prof_ ? ev_ : nullptr;
+    X.evSet = evSet_;
     return X;
 }
 
@@ -135,6 +139,8 @@ int Engine::init(size_t hbmBudget) {
     if ((rc = check(cudaMemset(status_, 0, sizeof(int)), "memset"))) return rc;
     if ((rc = check(cudaMalloc(&counters_, sizeof(int) * 64), "cudaMalloc"))) return rc;
     if ((rc = check(cudaMallocHost(&hostSmall_, sizeof(int) * 64), "cudaMallocHost"))) return rc;
+    for (auto &e : ev_)
+        if ((rc = check(cudaEventCreate(&e), "event"))) return rc;
     size_t freeB = 0, totalB = 0;
     cudaMemGetInfo(&freeB, &totalB);
     budget_ = hbmBudget ? hbmBudget : totalB;
@@ -149,6 +155,40 @@ int Engine::ensure_arena(size_t bytes) {
     cudaError_t e = ar_.reserve(bytes);
     if (e != cudaSuccess) return fail(CULS_E_OOM, std::string("device arena: ") + cudaGetErrorString(e));
     return 0;
+}
+
+void Engine::mark(int m) {
+    if (m < 0 || m >= kNumMarks) return;
+    cudaEventRecord(ev_[m], s_);
+    evSet_[m] = true;
+}
+
+float Engine::elapsed(int a, int b) {
+    if (a < 0 || b < 0 || a >= kNumMarks || b >= kNumMarks || !evSet_[a] || !evSet_[b]) return -1.f;
+    float ms = -1.f;
+    if (cudaEventSynchronize(ev_[b]) != cudaSuccess) return -1.f;
+    if (cudaEventElapsedTime(&ms, ev_[a], ev_[b]) != cudaSuccess) return -1.f;
+    return ms;
+}
+
+int Engine::clone(const Batch &src, Batch &dst) {
+    if (&src == &dst) return 0;
+    dst.release();
+    int rc;
+    const int64_t n = std::max<int64_t>(src.nObj, 1), np = std::max<int64_t>(src.nPO, 1);
+    if ((rc = check(cudaMalloc(&dst.F0, sizeof(int) * n), "cudaMalloc"))) return rc;
+    if ((rc = check(cudaMalloc(&dst.F1, sizeof(int) * n), "cudaMalloc"))) return rc;
+    if ((rc = check(cudaMalloc(&dst.PO, sizeof(int) * np), "cudaMalloc"))) return rc;
+    if ((rc = check(cudaMalloc(&dst.dg, sizeof(DevGraph) * std::max(src.G, 1)), "cudaMalloc"))) return rc;
+    cudaMemcpyAsync(dst.F0, src.F0, sizeof(int) * src.nObj, cudaMemcpyDeviceToDevice, s_);
+    cudaMemcpyAsync(dst.F1, src.F1, sizeof(int) * src.nObj, cudaMemcpyDeviceToDevice, s_);
+    if (src.nPO) cudaMemcpyAsync(dst.PO, src.PO, sizeof(int) * src.nPO, cudaMemcpyDeviceToDevice, s_);
+    cudaMemcpyAsync(dst.dg, src.dg, sizeof(DevGraph) * src.G, cudaMemcpyDeviceToDevice, s_);
+    dst.G = src.G;
+    dst.nObj = src.nObj;
+    dst.nPO = src.nPO;
+    dst.hg = src.hg;
+    return check(cudaGetLastError(), "clone");
 }
 
 // ------------------------------------------------------------ upload
@@ -258,6 +298,7 @@ __global__ void k_st_po(int64_t nPO, int G, const DevGraph *dg, const int *PO, i
 
 int Engine::st(Batch &b, bool cpuOrder) {
     const int64_t N = b.nObj;
+    if (prof_) mark(kMkStStart);
     int rc;
     if ((rc = ensure_arena((size_t)N * 160 + (size_t)b.nPO * 8 + ((size_t)64 << 20)))) return rc;
     ar_.reset();
@@ -273,7 +314,9 @@ int Engine::st(Batch &b, bool cpuOrder) {
     launches_ += 2;
     // `st` = GPU strash (frontier order, trivial folding); `st -c` = CPU strash
     // (id order, no folding), both with dangling removal
-    return strash_core(b, N, L0, L1, gid, lid, po, cpuOrder, true, !cpuOrder);
+    rc = strash_core(b, N, L0, L1, gid, lid, po, cpuOrder, true, !cpuOrder);
+    if (prof_) mark(kMkStEnd);
+    return rc;
 }
 
 }  // namespace culs

@@ -83,8 +83,11 @@ void remove_dangling(Aig &g) {
 // uniformly from the `window` previous layers (plus all PIs when withPIs), and
 // otherwise uniformly from every earlier object except the constant.  Each
 // fanin edge is complemented with probability 1/2.  POs are the first nPOs
-// nodes of the last layer (all of it when it is narrower).
-Aig layered(uint64_t seed, int nPIs, int nPOs, int64_t nAnds, int nLayers, int window, double pFar, bool withPIs) {
+// nodes of the last layer (all of it when it is narrower), or, with
+// sinksArePOs, every AND node without fanouts (then no node dangles and the
+// AIG keeps exactly nAnds AND nodes).
+Aig layered(uint64_t seed, int nPIs, int nPOs, int64_t nAnds, int nLayers, int window, double pFar, bool withPIs,
+            bool sinksArePOs = false) {
     Rng r(seed);
     Aig g;
     g.nPIs = nPIs;
@@ -128,8 +131,18 @@ Aig layered(uint64_t seed, int nPIs, int nPOs, int64_t nAnds, int nLayers, int w
             g.f1[v] = b;
         }
     }
-    int64_t lastLo = layerStart[nLayers], lastHi = layerStart[nLayers + 1];
-    for (int64_t v = lastLo; v < lastHi && (int)g.outs.size() < nPOs; v++) g.outs.push_back((int)(2 * v));
+    if (sinksArePOs) {
+        std::vector<char> hasFanout(nObjs, 0);
+        for (int64_t v = 1 + nPIs; v < nObjs; v++) {
+            hasFanout[g.f0[v] >> 1] = 1;
+            hasFanout[g.f1[v] >> 1] = 1;
+        }
+        for (int64_t v = 1 + nPIs; v < nObjs; v++)
+            if (!hasFanout[v]) g.outs.push_back((int)(2 * v));
+    } else {
+        int64_t lastLo = layerStart[nLayers], lastHi = layerStart[nLayers + 1];
+        for (int64_t v = lastLo; v < lastHi && (int)g.outs.size() < nPOs; v++) g.outs.push_back((int)(2 * v));
+    }
     remove_dangling(g);
     return g;
 }
@@ -239,9 +252,9 @@ int culs_gen_multiplier(int n, culs_host_graph *out) {
 
 // Batch of `count` layered graphs with sizes log-uniform in [minAnds,
 // maxAnds], PI counts uniform in [minPIs, maxPIs], nLayers = round(sqrt(nAnds)),
-// a 4-layer window plus PIs, POs the first 32 nodes of the last layer.  Graph
-// i is seeded with splitmix64(tag * 2^32 + i).  Generated on `threads` host
-// threads; output order is graph order.
+// a 4-layer window plus PIs; every sink is a PO, so each graph keeps its drawn
+// AND count.  Graph i is seeded with splitmix64(tag * 2^32 + i).  Generated on
+// `threads` host threads; output order is graph order.
 int culs_gen_batch(uint64_t tag, int first, int count, int64_t minAnds, int64_t maxAnds, int minPIs, int maxPIs,
                    int threads, culs_host_graph *out) {
     if (!out || count < 0 || minAnds < 1 || maxAnds < minAnds || minPIs < 2 || maxPIs < minPIs) return CULS_E_INVALID;
@@ -256,7 +269,7 @@ int culs_gen_batch(uint64_t tag, int first, int count, int64_t minAnds, int64_t 
                                                            u * (std::log((double)maxAnds) - std::log((double)minAnds))));
             int nPIs = minPIs + (int)r.below((uint64_t)(maxPIs - minPIs + 1));
             int nLayers = std::max(1, (int)std::llround(std::sqrt((double)nAnds)));
-            Aig g = layered(r.next(), nPIs, 32, nAnds, nLayers, 4, 0.0, true);
+            Aig g = layered(r.next(), nPIs, 0, nAnds, nLayers, 4, 0.0, true, true);
             rc[k] = export_graph(g, &out[k]);
         }
     };

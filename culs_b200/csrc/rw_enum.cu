@@ -130,7 +130,9 @@ int rw_enumerate(ExecCtx &X, RwWork &w) {
     if ((rc = X.check(cudaMemsetAsync(X.counters, 0, sizeof(int) * 4, s), "memset"))) return rc;
     k_enum_init<<<X.grid(N), kBlock, 0, s>>>(N, w.wlev, w.wl, w.lidLow, w.cutL, w.cutM, done);
     EnumArgs A{w.nL0, N, w.w0, w.w1, w.ref, w.lidLow, w.cutL, w.cutM, done, X.counters, X.status};
+    X.mark(kMkEnumK0);
     k_enumerate<<<(unsigned)(X.sms * 6), kEnumBlock, 0, s>>>(A);
+    X.mark(kMkEnumK1);
     X.launched(2);
     if ((rc = X.check(cudaGetLastError(), "enumerate launch"))) return rc;
     return 0;

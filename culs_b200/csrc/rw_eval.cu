@@ -93,7 +93,9 @@ int rw_evaluate(ExecCtx &X, RwWork &w) {
         k_table_build<<<X.grid(nAnd), kBlock, 0, s>>>(w.nL0, N, w.w0, w.w1, w.wg, w.dg, w.tab, X.status);
         EvalArgs A{w.nL0, N, EvalIn{w.w0, w.w1, w.ref, w.wlev, X.lib, w.tab, X.status}, w.cutL, w.cutM, w.wg, w.dg,
                    w.useZeros ? 1 : 0, w.bestCut, w.bestOut, candFlag};
+        X.mark(kMkEvalK0);
         k_evaluate<<<X.grid(nAnd, kEvalBlock), kEvalBlock, 0, s>>>(A);
+        X.mark(kMkEvalK1);
         X.launched(2);
     }
     if ((rc = X.check(compact_flags(candFlag, N, w.cand, X.counters + 8, *X.ar, s), "compact"))) return rc;

@@ -62,9 +62,13 @@ int Engine::rw(Batch &b, bool useZeros, bool gpuDedup, RwStats *stats, RwDump *d
     RwWork w;
     w.useZeros = useZeros;
     const bool wantDump = dump && dump->enabled && b.G == 1;
+    X.mark(kMkRwStart);
     if ((rc = rw_front(X, b, w))) return rc;
+    X.mark(kMkFront);
     if ((rc = rw_enumerate(X, w))) return rc;
+    X.mark(kMkEnum);
     if ((rc = rw_evaluate(X, w))) return rc;
+    X.mark(kMkEval);
     if (wantDump) {
         std::vector<int4> L(N * 8);
         std::vector<int2> Mt(N * 8);
@@ -94,6 +98,7 @@ int Engine::rw(Batch &b, bool useZeros, bool gpuDedup, RwStats *stats, RwDump *d
         }
     }
     if ((rc = rw_replace(X, b, w))) return rc;
+    X.mark(kMkReplace);
     if (wantDump) {
         std::vector<int> cand(w.nCand), rep(w.nCand);
         if (w.nCand) {
@@ -110,6 +115,7 @@ int Engine::rw(Batch &b, bool useZeros, bool gpuDedup, RwStats *stats, RwDump *d
         }
     }
     if ((rc = rw_choice(X, b, w, stats))) return rc;
+    X.mark(kMkChoice);
     if (wantDump) {
         std::vector<int> cand(w.nCand), ch(w.nCand), lev(N);
         if (w.nCand) {
@@ -123,6 +129,7 @@ int Engine::rw(Batch &b, bool useZeros, bool gpuDedup, RwStats *stats, RwDump *d
         for (int64_t c = 0; c < w.nCand; c++) dump->choice[cand[c]] = ch[c];
     }
     if ((rc = rw_redundancy(X, b, w))) return rc;
+    X.mark(kMkRedund);
     const int64_t M = N + w.nNew;
     int *o0 = ar_.get<int>(M), *o1 = ar_.get<int>(M), *opo = ar_.get<int>(b.nPO + 1);
     if (!o0 || !o1 || !opo) return fail(CULS_E_OOM, "rw: arena exhausted (dedup)");
@@ -130,7 +137,9 @@ int Engine::rw(Batch &b, bool useZeros, bool gpuDedup, RwStats *stats, RwDump *d
                                                                            o1, b.nPO, w.wpo, opo);
     launches_ += 1;
     // updateFromRewriteManager(2) -> GPU strash; (1) -> CPU deduplicate
-    return strash_core(b, M, o0, o1, w.gidAll, w.wl, opo, false, gpuDedup, gpuDedup);
+    rc = strash_core(b, M, o0, o1, w.gidAll, w.wl, opo, false, gpuDedup, gpuDedup);
+    X.mark(kMkRwEnd);
+    return rc;
 }
 
 }  // namespace culs

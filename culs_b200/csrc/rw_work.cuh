@@ -22,6 +22,14 @@ struct ExecCtx {
     int sms = 148;
     int *launches = nullptr;
     std::string *err = nullptr;
+    cudaEvent_t *ev = nullptr;  // profiling marks (null when profiling is off)
+    bool *evSet = nullptr;
+    void mark(int m) {
+        if (ev) {
+            cudaEventRecord(ev[m], s);
+            evSet[m] = true;
+        }
+    }
 
     int fail(int code, const std::string &m) {
         if (err) *err = m;

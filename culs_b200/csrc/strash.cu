@@ -421,7 +421,9 @@ int Engine::strash_core(Batch &b, int64_t M, const int *L0, const int *L1, const
     if (nLive > 0) {
         DedupArgs A{nLive, srt,     rankOf, idOrder ? liveIdx : srt, L0,     L1,     level,      lvlCnt,         lvlDone,  gidA,
                     b.dg,  AndTable{tk, tv, cap - 1}, mapEnc, kl0, kl1, foldTrivial ? 1 : 0, qc + 5, status_};
+        if (prof_) this->mark(kMkDedupK0);
         k_dedup<<<(unsigned)(sms_ * 8), kBlock, 0, s>>>(A);
+        if (prof_) this->mark(kMkDedupK1);
         k_winner_flags<<<grid_1d(nLive, kBlock, sms_ * 16), kBlock, 0, s>>>(nLive, srt, rankOf, mapEnc, tv, wflags);
         launches_ += 2;
     }

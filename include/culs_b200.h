@@ -136,6 +136,21 @@ int culs_dump_copy(culs_ctx *ctx, int which, int32_t *out);
 /* Kernels this context has launched so far. */
 int64_t culs_kernel_launches(culs_ctx *ctx);
 
+/* Device copy of a handle's graphs into *dst (allocated when *dst is NULL),
+ * e.g. to rerun a pass on the same input. */
+int culs_graph_clone(culs_ctx *ctx, const culs_graph *src, culs_graph **dst);
+
+/* Profiling: with profiling on, every pass records CUDA events on the
+ * context's stream.  culs_mark(ctx, 0|1) records a user mark.
+ * culs_profile_read fills up to n device-time intervals in ms: rw front
+ * (reset/levelize/reorder), cut enumeration, evaluation, replacement,
+ * choice, redundancy removal, rw's deduplication, `st`, the enumeration
+ * kernel alone, the evaluation kernel alone, the last strash hashing kernel,
+ * user mark 0 -> 1 (-1 where an interval was not recorded). */
+int culs_profile(culs_ctx *ctx, int enable);
+int culs_mark(culs_ctx *ctx, int slot);
+int culs_profile_read(culs_ctx *ctx, float *ms, int n);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1291,3 +1291,35 @@ int orc_prededup_graph(void *h, int *f0, int *f1, int *outs) {
 }
 
 }  // extern "C"
+
+// Bit-parallel simulation of an AIG (AIGMan layout) on `words` 64-bit random
+// patterns per PI drawn from splitmix64(seed, pi, word); writes nPOs * words
+// output words.  Used to check functional equivalence of large results.
+extern "C" int orc_simulate(int nPIs, int nPOs, int nAnds, const int *f0, const int *f1, const int *outs, int words,
+                            unsigned long long seed, unsigned long long *out) {
+    const int n = 1 + nPIs + nAnds;
+    std::vector<unsigned long long> val((size_t)n * words);
+    auto mix = [](unsigned long long x) {
+        x += 0x9E3779B97F4A7C15ull;
+        x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+        x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+        return x ^ (x >> 31);
+    };
+    for (int w = 0; w < words; w++) val[w] = ~0ull;
+    for (int i = 1; i <= nPIs; i++)
+        for (int w = 0; w < words; w++) val[(size_t)i * words + w] = mix(seed ^ mix((unsigned long long)i * 1000003ull + w));
+    for (int v = nPIs + 1; v < n; v++) {
+        int a = f0[v], b = f1[v];
+        if ((a >> 1) >= v || (b >> 1) >= v || a < 0 || b < 0) return -1;
+        const unsigned long long ca = (a & 1) ? ~0ull : 0ull, cb = (b & 1) ? ~0ull : 0ull;
+        const unsigned long long *pa = &val[(size_t)(a >> 1) * words], *pb = &val[(size_t)(b >> 1) * words];
+        unsigned long long *pv = &val[(size_t)v * words];
+        for (int w = 0; w < words; w++) pv[w] = (pa[w] ^ ca) & (pb[w] ^ cb);
+    }
+    for (int k = 0; k < nPOs; k++) {
+        int o = outs[k];
+        const unsigned long long c = (o & 1) ? ~0ull : 0ull;
+        for (int w = 0; w < words; w++) out[(size_t)k * words + w] = val[(size_t)(o >> 1) * words + w] ^ c;
+    }
+    return 0;
+}

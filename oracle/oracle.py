@@ -58,6 +58,8 @@ def _load():
         lib.orc_dump_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
         lib.orc_prededup_sizes.argtypes = [vp, ip, ip]
         lib.orc_prededup_graph.argtypes = [vp, ip, ip, ip]
+        lib.orc_simulate.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ip, ip, ip, ctypes.c_int,
+                                     ctypes.c_ulonglong, ctypes.POINTER(ctypes.c_ulonglong)]
         _lib = lib
     return _lib
 
@@ -190,3 +192,22 @@ def rw_st(g: Graph, zeros=False, st=True):
     if st:
         o.st()
     return o.graph()
+
+
+def simulate(g, words=4, seed=1):
+    """PO words of g under seeded random PI patterns (C simulator)."""
+    lib = _load()
+    f0 = np.ascontiguousarray(g.fanin0, dtype=np.int32)
+    f1 = np.ascontiguousarray(g.fanin1, dtype=np.int32)
+    outs = np.ascontiguousarray(g.outs, dtype=np.int32) if len(g.outs) else np.zeros(1, np.int32)
+    res = np.zeros(max(len(g.outs), 1) * words, dtype=np.uint64)
+    rc = lib.orc_simulate(g.nPIs, len(g.outs), len(f0) - 1 - g.nPIs, _ip(f0), _ip(f1), _ip(outs), words, seed,
+                          res.ctypes.data_as(ctypes.POINTER(ctypes.c_ulonglong)))
+    if rc != 0:
+        raise ValueError("simulate: not topological")
+    return res[:len(g.outs) * words].reshape(len(g.outs), words)
+
+
+def equivalent_sim(a, b, words=4, seed=1):
+    return a.nPIs == b.nPIs and len(a.outs) == len(b.outs) and np.array_equal(simulate(a, words, seed),
+                                                                                simulate(b, words, seed))
