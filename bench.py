@@ -1,0 +1,282 @@
+"""Benchmark of `rw; st` (CULS AIG rewriting + strash) on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c4|c3|c2|c1] [--impl ours|reference]
+
+Metric: input AND nodes processed by one `rw; st` per second (whole job).
+A step is one `rw; st` over the workload's graphs:
+  c4  4,096 seeded layered AIGs, AND counts log-uniform 1k-200k, PIs 16-512,
+      depth ~ sqrt(size), window-4 fanins, every sink a PO (batched mode, the
+      headline workload; inputs ~1.2 GB, larger than the 126 MB L2)
+  c3  one 10M-AND layered AIG, 4,096 PIs/POs, 2,000 layers, 80% window-3 /
+      20% far fanins
+  c2  64x64 array multiplier; c1  5,000-AND 40-layer AIG (parity cases)
+`value` times device-resident steps (a device clone of the input, rw, st);
+`e2e` times the public C-ABI path from host arrays: upload, rw, st,
+download.  With --gpus N (under torchrun) every rank rewrites its own
+4,096 graphs (weak scaling, no data-path collective).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from concurrent.futures import ThreadPoolExecutor
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+import numpy as np  # noqa: E402
+
+from culs_b200.dist import Group  # noqa: E402
+
+METRIC = "rw+st AND-nodes/sec"
+UNIT = "AND-nodes/s"
+ALG_BYTES_ENUM = 584  # algorithmic bytes per AND node of cut enumeration (2 fanin cut sets + own set)
+
+
+def make_workload(name, rank):
+    import culs_b200 as C
+    threads = os.cpu_count() or 8
+    if name == "c4":
+        return C.gen_batch(4, rank * 4096, 4096, 1000, 200000, 16, 512, threads=threads)
+    if name == "c3":
+        return [C.gen_layered(3 + rank, 4096, 4096, 10_000_000, 2000, 3, 0.2, False)]
+    if name == "c3m":  # profiling case: a 1M-AND member of the c3 family
+        return [C.gen_layered(3 + rank, 4096, 4096, 1_000_000, 200, 3, 0.2, False)]
+    if name == "c2":
+        return [C.gen_multiplier(64)]
+    if name == "c1":
+        return [C.gen_layered(1 + rank, 64, 32, 5000, 40, 4, 0.0, True)]
+    raise SystemExit(f"unknown workload {name}")
+
+
+WORKLOAD_DESC = {"c4": "c4_batched_4096_layered_1k-200k", "c3": "c3_single_10M_layered_2000",
+                 "c3m": "c3_family_1M_layered_200", "c2": "c2_mult64x64", "c1": "c1_layered5k_40"}
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+
+    def __init__(self, device):
+        self.device = device
+        self.samples = []
+        self.stop = threading.Event()
+        self.th = None
+
+    def _run(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        while not self.stop.is_set():
+            try:
+                r = subprocess.run(["nvidia-smi", "-i", str(self.device), f"--query-gpu={q}",
+                                    "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                f = [x.strip() for x in r.stdout.strip().split(",")]
+                if len(f) == 7:
+                    self.samples.append(f)
+            except Exception:
+                pass
+            self.stop.wait(0.2)
+
+    def __enter__(self):
+        self.th = threading.Thread(target=self._run, daemon=True)
+        self.th.start()
+        return self
+
+    def __exit__(self, *a):
+        self.stop.set()
+        self.th.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[3 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": float(self.samples[0][1]), "reasons": reasons,
+                "samples": len(sm)}
+
+
+def measured_peak():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def enum_traffic_per_node():
+    """DRAM bytes per AND node of the enumeration kernel from the committed
+    ncu summary (profiles/k_enumerate_traffic.json), if present."""
+    p = ROOT / "profiles" / "k_enumerate_traffic.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["dram_bytes_per_and_node"]), d.get("source", "")
+    return None, None
+
+
+def cpu_baseline(name, graphs, budget_s=12.0, threads=None):
+    """Times the CPU restatement of the reference rw;st (oracle/, kind
+    "port") on a bounded sample of the workload, on `threads` host threads
+    (ctypes releases the GIL, one graph per call)."""
+    import culs_b200 as C
+    from oracle.oracle import Graph, Oracle
+    threads = threads or (os.cpu_count() or 1)
+    if name in ("c3", "c3m"):  # the 10M graph takes minutes on one core: a 1M-AND member of the same family
+        sample = [C.gen_layered(3, 4096, 4096, 1_000_000, 200, 3, 0.2, False)]
+        desc = "c3 family (80% window-3 / 20% far fanins), one 1M-AND graph, 1 thread"
+        threads = 1
+    else:
+        sample = list(graphs)
+        desc = f"first graphs of the workload until {budget_s:.0f} s elapse, one graph per thread"
+
+    def one(g):
+        o = Oracle()
+        o.set_graph(Graph(g.nPIs, g.fanin0, g.fanin1, g.outs))
+        o.rw()
+        o.st()
+        return g.nAnds
+
+    done = 0
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(max_workers=threads) as ex:
+        futs = []
+        it = iter(sample)
+        for g in it:
+            futs.append(ex.submit(one, g))
+            if len(futs) >= threads:
+                done += futs.pop(0).result()
+                if time.perf_counter() - t0 > budget_s:
+                    break
+        for f in futs:
+            done += f.result()
+    dt = time.perf_counter() - t0
+    return {"value": done / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{desc}: {done} AND nodes in {dt:.1f} s"}
+
+
+def reference_arm(args, group):
+    """`--impl reference`: the reference's rw;st restated on the CPU (oracle
+    port; the reference's own rw needs a GPU for cut enumeration, so it has no
+    CPU implementation to run), all host threads, a bounded sample per step."""
+    if group.rank != 0:
+        return 0
+    graphs = make_workload(args.workload, 0)
+    budget = 6.0
+    for _ in range(args.warmup):
+        cpu_baseline(args.workload, graphs, budget_s=1.0)
+    vals = [cpu_baseline(args.workload, graphs, budget_s=budget) for _ in range(args.steps)]
+    v = statistics.median(x["value"] for x in vals)
+    cb = dict(vals[0])
+    cb["value"] = v
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded generators)",
+            "config": {"workload": WORKLOAD_DESC[args.workload]}, "cpu_baseline": cb,
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def our_arm(args, group):
+    import culs_b200 as C
+    ctx = C.Context(device=group.local)
+    graphs = make_workload(args.workload, group.rank)
+    n_and = sum(g.nAnds for g in graphs)
+    in_bytes = sum(4 * (2 * g.nObjs + g.nPOs) for g in graphs)
+    d0 = ctx.upload_batch(graphs)
+    dw = ctx.clone(d0)
+    ctx.profile(True)
+    for _ in range(args.warmup):
+        ctx.clone(d0, into=dw)
+        ctx.rw_st(dw)
+    ctx.sync()
+    # device-resident steps
+    group.barrier()
+    ctx.sync()
+    l0 = ctx.kernel_launches()
+    with ClockSampler(group.local) as clk:
+        ctx.mark(0)
+        for _ in range(args.steps):
+            ctx.clone(d0, into=dw)
+            ctx.rw_st(dw)
+        ctx.mark(1)
+        ctx.sync()
+    launches = ctx.kernel_launches() - l0
+    prof = ctx.profile_read()
+    t_ms = group.max(prof["user"])
+    group.barrier()
+    total_and = group.sum(n_and)
+    value = total_and * args.steps / (t_ms / 1e3)
+    out_and = sum(dw.stats(i)["nAnds"] for i in range(len(dw)))
+    # end to end through the C ABI from host arrays
+    e2e_steps = max(1, min(args.steps, 3))
+    group.barrier()
+    ctx.sync()
+    ctx.mark(0)
+    out_bytes = 0
+    for _ in range(e2e_steps):
+        d = ctx.upload_batch(graphs)
+        ctx.rw_st(d)
+        res = d.download_all()
+        out_bytes = sum(4 * (2 * r.nObjs + r.nPOs) for r in res)
+        d.free()
+    ctx.mark(1)
+    ctx.sync()
+    e2e_ms = group.max(ctx.profile_read()["user"])
+    e2e_value = total_and * e2e_steps / (e2e_ms / 1e3)
+    # roofline of the dominant kernel (cut enumeration)
+    peak, peak_kind = measured_peak()
+    k_ms = prof["k_enumerate"]
+    achieved = ALG_BYTES_ENUM * n_and / (k_ms / 1e3) / 1e9 if k_ms > 0 else None
+    tpn, tsrc = enum_traffic_per_node()
+    roof = {"kernel": "k_enumerate (cut enumeration)", "bound": "hbm", "achieved": achieved, "peak": peak,
+            "peak_kind": f"{peak_kind} hbm_gbs", "unit": "GB/s", "frac": achieved / peak if achieved else None,
+            "traffic": tpn * n_and if tpn else None, "traffic_source": tsrc,
+            "algorithmic_bytes_per_and": ALG_BYTES_ENUM, "launch_ms": k_ms}
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": group.world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+            "data": "synthetic (seeded generators; CULS ships no benchmark inputs)",
+            "config": {"workload": WORKLOAD_DESC[args.workload], "graphs_per_gpu": len(graphs),
+                       "and_nodes_per_gpu": n_and, "and_nodes_out_per_gpu": out_and,
+                       "input_bytes_per_gpu": in_bytes, "l2": "inputs and working set larger than L2",
+                       "parallelism": f"graph-sharded x{group.world}" if group.world > 1 else "single GPU"},
+            "roofline": roof,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": in_bytes,
+                    "d2h_bytes_per_step": out_bytes, "steps": e2e_steps},
+            "clocks": clk.summary(), "gpu_launches": launches,
+            "stages_ms_last_step": {k: round(v, 3) for k, v in prof.items() if k not in ("user",)}}
+    if group.rank == 0:
+        line["cpu_baseline"] = cpu_baseline(args.workload, graphs) if group.world == 1 else None
+        print(json.dumps(line), flush=True)
+    dw.free()
+    d0.free()
+    ctx.close()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--workload", default="c4", choices=["c4", "c3", "c3m", "c2", "c1"])
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    group = Group()
+    try:
+        rc = reference_arm(args, group) if args.impl == "reference" else our_arm(args, group)
+    finally:
+        group.close()
+    return rc
+
+
+if __name__ == "__main__":
+    sys.exit(main())

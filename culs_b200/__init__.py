@@ -47,6 +47,7 @@ _ip = ctypes.POINTER(ctypes.c_int32)
 _lib.culs_create.restype = _vp
 _lib.culs_create.argtypes = [ctypes.c_size_t]
 _lib.culs_destroy.argtypes = [_vp]
+_lib.culs_set_device.argtypes = [ctypes.c_int]
 _lib.culs_last_error.restype = ctypes.c_char_p
 _lib.culs_last_error.argtypes = [_vp]
 _lib.culs_sync.argtypes = [_vp]
@@ -56,6 +57,7 @@ _lib.culs_batch_upload.argtypes = [_vp, ctypes.c_int, ctypes.POINTER(_HostGraph)
 _lib.culs_graph_free.argtypes = [_vp]
 _lib.culs_graph_count.argtypes = [_vp]
 _lib.culs_graph_stats.argtypes = [_vp, ctypes.c_int, _ip, _ip, _ip, _ip]
+_lib.culs_batch_download.argtypes = [_vp, _vp, ctypes.POINTER(_HostGraph)]
 _lib.culs_graph_download.argtypes = [_vp, _vp, ctypes.c_int, _ip, _ip, _ip]
 _lib.culs_rw.argtypes = [_vp, _vp, ctypes.c_uint32]
 _lib.culs_st.argtypes = [_vp, _vp, ctypes.c_uint32]
@@ -161,7 +163,9 @@ def gen_batch(tag, first, count, minAnds, maxAnds, minPIs, maxPIs, threads=8):
 class Context:
     """One GPU context (stream, rewriting library, scratch arena)."""
 
-    def __init__(self, hbm_budget=0):
+    def __init__(self, hbm_budget=0, device=None):
+        if device is not None:
+            _check(_lib.culs_set_device(int(device)), "set device")
         self.h = _lib.culs_create(hbm_budget)
         if not self.h:
             raise CulsError(-5, _lib.culs_last_error(None).decode())
@@ -220,9 +224,12 @@ class Context:
                      "k_enumerate", "k_evaluate", "k_dedup", "user"]
 
     def clone(self, d, into=None):
-        out = _vp(into.h if into is not None else None)
+        if into is not None:
+            self._err(_lib.culs_graph_clone(self.h, d.h, ctypes.byref(into.h)), "clone")
+            return into
+        out = _vp()
         self._err(_lib.culs_graph_clone(self.h, d.h, ctypes.byref(out)), "clone")
-        return into if into is not None else DeviceGraphs(self, out)
+        return DeviceGraphs(self, out)
 
     def profile(self, on=True):
         _lib.culs_profile(self.h, int(on))
@@ -265,6 +272,17 @@ class DeviceGraphs:
         v = [ctypes.c_int32() for _ in range(4)]
         _check(_lib.culs_graph_stats(self.h, i, *[ctypes.byref(x) for x in v]), "stats")
         return dict(zip(["nPIs", "nPOs", "nAnds", "nLevels"], [x.value for x in v]))
+
+    def download_all(self):
+        n = len(self)
+        arr = (_HostGraph * n)()
+        self.ctx._err(_lib.culs_batch_download(self.ctx.h, self.h, arr), "batch download")
+        out = []
+        for i in range(n):
+            a = _take(arr[i])
+            a.nLevels = self.stats(i)["nLevels"]
+            out.append(a)
+        return out
 
     def download(self, i=0) -> Aig:
         s = self.stats(i)

@@ -31,6 +31,15 @@ int set_err(culs_ctx *c, int rc) {
 
 extern "C" {
 
+int culs_set_device(int device) {
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) {
+        g_err = cudaGetErrorString(e);
+        return CULS_E_DEVICE;
+    }
+    return CULS_OK;
+}
+
 culs_ctx *culs_create(size_t hbm_budget) {
     culs_ctx *c = new culs_ctx();
     int rc = c->eng.init(hbm_budget);
@@ -107,6 +116,35 @@ int culs_graph_download(culs_ctx *ctx, const culs_graph *g, int index, int32_t *
     if (!ctx || !g) return CULS_E_INVALID;
     std::lock_guard<std::mutex> lk(ctx->mu);
     return set_err(ctx, ctx->eng.download(g->b, index, fanin0, fanin1, outs));
+}
+
+int culs_batch_download(culs_ctx *ctx, const culs_graph *g, culs_host_graph *outs) {
+    if (!ctx || !g || !outs) return CULS_E_INVALID;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    const culs::Batch &b = g->b;
+    std::vector<int32_t> f0(b.nObj), f1(b.nObj), po(b.nPO > 0 ? b.nPO : 1);
+    cudaStream_t s = ctx->eng.stream();
+    cudaMemcpyAsync(f0.data(), b.F0, sizeof(int32_t) * b.nObj, cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(f1.data(), b.F1, sizeof(int32_t) * b.nObj, cudaMemcpyDeviceToHost, s);
+    if (b.nPO) cudaMemcpyAsync(po.data(), b.PO, sizeof(int32_t) * b.nPO, cudaMemcpyDeviceToHost, s);
+    int rc = ctx->eng.sync();
+    if (rc != CULS_OK) return set_err(ctx, rc);
+    for (int i = 0; i < b.G; i++) {
+        const culs::DevGraph &d = b.hg[i];
+        const size_t n = 1 + (size_t)d.nPIs + d.nAnds;
+        culs_host_graph &o = outs[i];
+        o.nPIs = d.nPIs;
+        o.nPOs = d.nPOs;
+        o.nAnds = d.nAnds;
+        o.fanin0 = (int32_t *)malloc(sizeof(int32_t) * n);
+        o.fanin1 = (int32_t *)malloc(sizeof(int32_t) * n);
+        o.outs = (int32_t *)malloc(sizeof(int32_t) * (d.nPOs > 0 ? d.nPOs : 1));
+        if (!o.fanin0 || !o.fanin1 || !o.outs) return CULS_E_OOM;
+        memcpy(o.fanin0, f0.data() + d.base, sizeof(int32_t) * n);
+        memcpy(o.fanin1, f1.data() + d.base, sizeof(int32_t) * n);
+        if (d.nPOs) memcpy(o.outs, po.data() + d.poOff, sizeof(int32_t) * d.nPOs);
+    }
+    return CULS_OK;
 }
 
 int culs_rw(culs_ctx *ctx, culs_graph *g, uint32_t flags) {

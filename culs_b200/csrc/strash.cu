@@ -475,7 +475,9 @@ int Engine::strash_core(Batch &b, int64_t M, const int *L0, const int *L1, const
     int64_t base = 0;
     for (int g = 0; g < G; g++) {
         ng[g].nAnds = hCnt[g];
-        ng[g].nLevels = hLev[g];
+        // the CPU strash reports maxDelay, -1 without AND nodes
+        // (src/aig/strash.cu:396,454)
+        ng[g].nLevels = (idOrder && hCnt[g] == 0) ? -1 : hLev[g];
         ng[g].base = (int)base;
         base += 1 + ng[g].nPIs + hCnt[g];
     }

@@ -78,6 +78,8 @@ typedef struct culs_graph culs_graph; /* one or more AIGs resident in device mem
  * CULS_E_BUDGET.  Replaces AIGMan construction (CULS src/aig_manager.cu:22-33).
  * Returns NULL on failure; culs_last_error(NULL) then explains why. */
 culs_ctx *culs_create(size_t hbm_budget);
+/* Selects the CUDA device that the next culs_create on this thread uses. */
+int culs_set_device(int device);
 void culs_destroy(culs_ctx *ctx);
 const char *culs_last_error(culs_ctx *ctx);
 int culs_sync(culs_ctx *ctx);
@@ -97,6 +99,10 @@ int culs_graph_stats(const culs_graph *g, int index, int32_t *nPIs, int32_t *nPO
  * fanin arrays need 1 + nPIs + nAnds entries, outs nPOs. */
 int culs_graph_download(culs_ctx *ctx, const culs_graph *g, int index, int32_t *fanin0, int32_t *fanin1,
                         int32_t *outs);
+
+/* Copies every graph of the handle back into outs[0..count) (arrays
+ * allocated by the library; free each with culs_host_graph_free). */
+int culs_batch_download(culs_ctx *ctx, const culs_graph *g, culs_host_graph *outs);
 
 /* `rw` on every graph of the handle: AIGMan::rewrite(fUseZeros,
  * fGPUDeduplicate) (CULS src/aig_manager.cu:632-672, command handler

@@ -1,0 +1,203 @@
+"""GPU path (libculs_b200.so through the C ABI) against the oracle and
+against the reference's golden fixtures.  Integer work: every comparison is
+exact (tolerance 0)."""
+import hashlib
+import json
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import aigcanon
+import culs_b200 as C
+from oracle.oracle import Oracle
+from oracle import oracle as O
+from util import oracle_rw_st, same_graph, to_oracle
+
+pytestmark = pytest.mark.gpu
+GOLDEN = Path(__file__).resolve().parent / "golden"
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = C.Context()
+    yield c
+    c.close()
+
+
+def random_unstrashed(seed, nPIs, nAnds, nPOs, pconst=0.05, pdup=0.05):
+    """Topological AIG with constant fanins, x&x / x&!x nodes, duplicate
+    nodes, dangling nodes and PO literals on constants and PIs."""
+    rng = np.random.default_rng(seed)
+    n = 1 + nPIs + nAnds
+    f0 = np.full(n, -1, np.int32)
+    f1 = np.full(n, -1, np.int32)
+    for v in range(nPIs + 1, n):
+        if v > nPIs + 2 and rng.random() < pdup:
+            u = int(rng.integers(nPIs + 1, v))
+            f0[v], f1[v] = f0[u], f1[u]
+            continue
+        def lit():
+            if rng.random() < pconst:
+                return int(rng.integers(0, 2))
+            return int(2 * rng.integers(1, v) + rng.integers(0, 2))
+        a = lit()
+        b = a if rng.random() < 0.03 else (a ^ 1 if rng.random() < 0.03 else lit())
+        f0[v], f1[v] = min(a, b), max(a, b)
+    outs = np.array([int(rng.integers(0, 2 * n)) for _ in range(nPOs)], np.int32)
+    return C.Aig(nPIs, f0, f1, outs)
+
+
+def edge_graphs():
+    gs = {}
+    gs["no_ands"] = C.Aig(3, np.full(4, -1, np.int32), np.full(4, -1, np.int32), np.array([0, 1, 2, 7], np.int32))
+    gs["no_pos"] = C.Aig(4, *[np.concatenate([np.full(5, -1), x]).astype(np.int32)
+                              for x in ([2, 4, 10], [4, 6, 12])], np.zeros(0, np.int32))
+    gs["single_and"] = C.Aig(2, np.array([-1, -1, -1, 2], np.int32), np.array([-1, -1, -1, 5], np.int32),
+                             np.array([7, 6], np.int32))
+    for s in range(6):
+        gs[f"unstrashed{s}"] = random_unstrashed(s, 6 + s, 200 + 150 * s, 4 + s)
+    gs["mult6"] = C.gen_multiplier(6)
+    gs["mult12"] = C.gen_multiplier(12)
+    gs["c1"] = C.gen_layered(1, 64, 32, 5000, 40, 4, 0.0, True)
+    gs["far20k"] = C.gen_layered(7, 100, 50, 20000, 60, 3, 0.2, False)
+    return gs
+
+
+GRAPHS = edge_graphs()
+
+
+def gpu_run(ctx, g, ops):
+    d = ctx.upload(g)
+    for op in ops:
+        op(ctx, d)
+    return d.download()
+
+
+def oracle_run(g, ops):
+    o = Oracle()
+    o.set_graph(to_oracle(g))
+    for op in ops:
+        op(o)
+    return o.graph()
+
+
+FLOWS = {
+    "rw;st": ([lambda c, d: c.rw(d), lambda c, d: c.st(d)], [lambda o: o.rw(), lambda o: o.st()]),
+    "rw -z;st": ([lambda c, d: c.rw(d, zeros=True), lambda c, d: c.st(d)],
+                 [lambda o: o.rw(zeros=True), lambda o: o.st()]),
+    "st": ([lambda c, d: c.st(d)], [lambda o: o.st()]),
+    "st -c": ([lambda c, d: c.st(d, cpu=True)], [lambda o: o.st(cpu=True)]),
+    "rw (cpu dedup)": ([lambda c, d: c.rw(d, gpu_dedup=False)], [lambda o: o.rw(dedup=1)]),
+    "rw;rw;st": ([lambda c, d: c.rw(d), lambda c, d: c.rw(d), lambda c, d: c.st(d)],
+                 [lambda o: o.rw(), lambda o: o.rw(), lambda o: o.st()]),
+}
+
+
+@pytest.mark.parametrize("flow", list(FLOWS))
+@pytest.mark.parametrize("name", list(GRAPHS))
+def test_gpu_matches_oracle(ctx, name, flow):
+    g = GRAPHS[name]
+    gops, oops = FLOWS[flow]
+    a = gpu_run(ctx, g, gops)
+    b = oracle_run(g, oops)
+    assert same_graph(a, b), f"{name} {flow}: gpu {a.nAnds} ands vs oracle {b.nAnds}"
+    if g.nAnds:
+        assert a.nLevels == b.nLevels
+
+
+@pytest.mark.parametrize("name", ["mult12", "c1", "far20k", "unstrashed3", "unstrashed5"])
+def test_gpu_per_node_dumps_match_oracle(ctx, name):
+    g = GRAPHS[name]
+    d = ctx.upload(g)
+    ctx.rw(d, dump=True)
+    D = ctx.dump()
+    st = ctx.rw_stats()
+    o = Oracle()
+    o.set_graph(to_oracle(g))
+    o.rw()
+    f0, f1, outs = o.dump_reorder(g.nPOs)
+    np.testing.assert_array_equal(D["reorder_f0"], f0)
+    np.testing.assert_array_equal(D["reorder_f1"], f1)
+    np.testing.assert_array_equal(D["reorder_out"], outs)
+    np.testing.assert_array_equal(D["cuts"].reshape(-1, 8, 9), o.dump_cuts())
+    np.testing.assert_array_equal(D["selected"].reshape(-1, 10), o.dump_selected())
+    rep, nf0, nf1 = o.dump_replace()
+    np.testing.assert_array_equal(D["replace"], rep)
+    np.testing.assert_array_equal(D["new_f0"], nf0)
+    np.testing.assert_array_equal(D["new_f1"], nf1)
+    np.testing.assert_array_equal(D["choice"], o.dump_choice())
+    ost = o.dump_stats()
+    for k in ["replaced", "replaced_pos", "replaced_zero", "reverted", "compromised", "expected"]:
+        assert st[k] == ost[k], k
+
+
+def test_batch_equals_single(ctx):
+    names = ["no_ands", "mult6", "unstrashed2", "no_pos", "c1", "single_and", "unstrashed4"]
+    gs = [GRAPHS[n] for n in names]
+    db = ctx.upload_batch(gs)
+    ctx.rw_st(db)
+    assert len(db) == len(gs)
+    for i, g in enumerate(gs):
+        single = gpu_run(ctx, g, FLOWS["rw;st"][0])
+        got = db.download(i)
+        assert same_graph(got, single), names[i]
+        assert got.nLevels == single.nLevels
+
+
+@pytest.mark.parametrize("name", sorted(p.stem for p in GOLDEN.glob("*.npz")))
+def test_gpu_matches_reference_fixture(ctx, name):
+    f = dict(np.load(GOLDEN / f"{name}.npz"))
+    g = C.Aig(int(f["nPIs"]), f["in_f0"], f["in_f1"], f["in_outs"])
+    d = ctx.upload(g)
+    ctx.rw(d, dump=True)
+    D = ctx.dump()
+    assert aigcanon.digest(D["cuts"]) == str(f["cuts_sha"])
+    assert aigcanon.digest(D["selected"]) == str(f["selected_sha"])
+    stats = ctx.rw_stats()
+    assert [stats[k] for k in ["replaced", "replaced_pos", "replaced_zero", "reverted", "compromised"]] == \
+        [int(x) for x in f["z0_stats"][:5]]
+    ctx.st(d)
+    out = d.download()
+    assert (out.nAnds, out.nLevels) == tuple(int(x) for x in f["z0_st"])
+    ands, pos = aigcanon.signature(out.nPIs, out.fanin0, out.fanin1, out.outs)
+    assert hashlib.sha256(json.dumps([ands, pos]).encode()).hexdigest() == str(f["z0_sig"])
+
+
+def test_large_single_graph_matches_oracle(ctx):
+    g = C.gen_layered(3, 4096, 4096, 1_000_000, 200, 3, 0.2, False)
+    a = gpu_run(ctx, g, FLOWS["rw;st"][0])
+    b = oracle_rw_st(g).graph()
+    assert same_graph(a, b)
+    assert a.nLevels == b.nLevels
+
+
+def test_batch_of_generated_graphs_matches_oracle(ctx):
+    gs = C.gen_batch(4, 0, 24, 1000, 20000, 16, 512, threads=8)
+    db = ctx.upload_batch(gs)
+    ctx.rw_st(db)
+    for i, g in enumerate(gs):
+        assert same_graph(db.download(i), oracle_rw_st(g).graph()), i
+
+
+def test_rewrite_preserves_function(ctx):
+    for g in [GRAPHS["mult12"], GRAPHS["c1"], GRAPHS["unstrashed5"], C.gen_multiplier(32)]:
+        out = gpu_run(ctx, g, FLOWS["rw;st"][0])
+        assert O.equivalent_sim(to_oracle(g), to_oracle(out), words=8)
+        assert out.nAnds <= g.nAnds or g.nAnds == 0
+
+
+def test_budget_refusal(ctx):
+    small = C.Context(hbm_budget=1 << 20)
+    d = small.upload(C.gen_multiplier(64))
+    with pytest.raises(C.CulsError) as e:
+        small.rw(d)
+    assert e.value.code == -3
+    small.close()
+
+
+def test_invalid_graph_rejected(ctx):
+    bad = C.Aig(2, np.array([-1, -1, -1, 8], np.int32), np.array([-1, -1, -1, 2], np.int32), np.array([6], np.int32))
+    with pytest.raises(C.CulsError) as e:
+        ctx.upload(bad)
+    assert e.value.code == -1
