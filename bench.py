@@ -1,6 +1,6 @@
 """Benchmark of `rw; st` (CULS AIG rewriting + strash) on B200.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c4|c3|c2|c1] [--impl ours|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c4|c4m|c3|c3m|c2|c1] [--impl ours|reference]
 
 Metric: input AND nodes processed by one `rw; st` per second (whole job).
 A step is one `rw; st` over the workload's graphs:
@@ -35,7 +35,14 @@ from culs_b200.dist import Group  # noqa: E402
 
 METRIC = "rw+st AND-nodes/sec"
 UNIT = "AND-nodes/s"
-ALG_BYTES_ENUM = 584  # algorithmic bytes per AND node of cut enumeration (2 fanin cut sets + own set)
+# Kernels timed live (CUDA-event marks around their launches) with the
+# algorithmic bytes each moves per input AND node; the roofline reports the
+# one that takes longest.
+KERNELS = {
+    "k_enumerate": ("cut enumeration", 584),  # 2 fanin cut sets read + own set written
+    "k_evaluate": ("MFFC + NPN match + gain", 328),  # own cuts, fanins, refs, levels, table probes
+    "k_dedup": ("strash hashing dataflow", 52),  # fanins, level, map, table slot, key out
+}
 
 
 def make_workload(name, rank):
@@ -43,6 +50,8 @@ def make_workload(name, rank):
     threads = os.cpu_count() or 8
     if name == "c4":
         return C.gen_batch(4, rank * 4096, 4096, 1000, 200000, 16, 512, threads=threads)
+    if name == "c4m":  # profiling case: the first 256 graphs of the c4 family
+        return C.gen_batch(4, rank * 4096, 256, 1000, 200000, 16, 512, threads=threads)
     if name == "c3":
         return [C.gen_layered(3 + rank, 4096, 4096, 10_000_000, 2000, 3, 0.2, False)]
     if name == "c3m":  # profiling case: a 1M-AND member of the c3 family
@@ -54,7 +63,7 @@ def make_workload(name, rank):
     raise SystemExit(f"unknown workload {name}")
 
 
-WORKLOAD_DESC = {"c4": "c4_batched_4096_layered_1k-200k", "c3": "c3_single_10M_layered_2000",
+WORKLOAD_DESC = {"c4": "c4_batched_4096_layered_1k-200k", "c4m": "c4_family_batched_256_layered_1k-200k", "c3": "c3_single_10M_layered_2000",
                  "c3m": "c3_family_1M_layered_200", "c2": "c2_mult64x64", "c1": "c1_layered5k_40"}
 
 
@@ -109,10 +118,10 @@ def measured_peak():
     return 6650.0, "fallback"
 
 
-def enum_traffic_per_node():
-    """DRAM bytes per AND node of the enumeration kernel from the committed
-    ncu summary (profiles/k_enumerate_traffic.json), if present."""
-    p = ROOT / "profiles" / "k_enumerate_traffic.json"
+def traffic_per_node(kernel):
+    """DRAM bytes per AND node of `kernel` from its committed ncu summary
+    (profiles/<kernel>_traffic.json), if present."""
+    p = ROOT / "profiles" / f"{kernel}_traffic.json"
     if p.exists():
         d = json.loads(p.read_text())
         return float(d["dram_bytes_per_and_node"]), d.get("source", "")
@@ -229,15 +238,18 @@ def our_arm(args, group):
     ctx.sync()
     e2e_ms = group.max(ctx.profile_read()["user"])
     e2e_value = total_and * e2e_steps / (e2e_ms / 1e3)
-    # roofline of the dominant kernel (cut enumeration)
+    # roofline of the dominant kernel
     peak, peak_kind = measured_peak()
-    k_ms = prof["k_enumerate"]
-    achieved = ALG_BYTES_ENUM * n_and / (k_ms / 1e3) / 1e9 if k_ms > 0 else None
-    tpn, tsrc = enum_traffic_per_node()
-    roof = {"kernel": "k_enumerate (cut enumeration)", "bound": "hbm", "achieved": achieved, "peak": peak,
+    kname = max(KERNELS, key=lambda k: prof.get(k, 0.0))
+    kdesc, alg = KERNELS[kname]
+    k_ms = prof[kname]
+    achieved = alg * n_and / (k_ms / 1e3) / 1e9 if k_ms > 0 else None
+    tpn, tsrc = traffic_per_node(kname)
+    roof = {"kernel": f"{kname} ({kdesc})", "bound": "hbm", "achieved": achieved, "peak": peak,
             "peak_kind": f"{peak_kind} hbm_gbs", "unit": "GB/s", "frac": achieved / peak if achieved else None,
             "traffic": tpn * n_and if tpn else None, "traffic_source": tsrc,
-            "algorithmic_bytes_per_and": ALG_BYTES_ENUM, "launch_ms": k_ms}
+            "algorithmic_bytes_per_and": alg, "launch_ms": k_ms,
+            "kernel_ms": {k: prof.get(k) for k in KERNELS}}
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": group.world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "int32",
@@ -265,7 +277,7 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--workload", default="c4", choices=["c4", "c3", "c3m", "c2", "c1"])
+    ap.add_argument("--workload", default="c4", choices=["c4", "c4m", "c3", "c3m", "c2", "c1"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     args = ap.parse_args()
     if args.warmup < 3:

@@ -47,30 +47,111 @@ struct WorkQueue {
     int cap;
 };
 
-__device__ __forceinline__ void queue_push(const WorkQueue &q, int v) {
-    int t = atomicAdd(q.tail, 1);
-    __threadfence();
-    st_release(&q.items[t], v);
+// ------------------------------------------------ warp-aggregated atomics
+// Per-item atomics on a handful of hot addresses (a level's completion
+// counter, a queue tail, a graph's counter) serialise in L2; these helpers
+// issue one atomic per group of converged lanes that share the address.
+
+// atomicAdd(&base[key], v), one atomic per group of lanes with equal key.
+__device__ __forceinline__ void agg_add(int *base, int key, int v) {
+    const unsigned mask = __activemask();
+    const unsigned peers = __match_any_sync(mask, key);
+    const int sum = __reduce_add_sync(peers, v);
+    if ((int)(threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&base[key], sum);
 }
 
-// Each lane takes one queue index; returns -1 when the queue is drained (or a
-// wait expired, recorded in *status).
-__device__ __forceinline__ int queue_pop_wait(const WorkQueue &q, int h, int *status) {
-    int64_t it = 0;
-    while (true) {
-        if (h < q.cap) {
-            int v = ld_acquire(&q.items[h]);
-            if (v >= 0) return v;
-        }
-        int d = ld_acquire(q.done);
-        int t = ld_acquire(q.tail);
-        if (d == t && h >= t) return -1;
-        if (++it > kSpinLimit) {
-            set_status(status, kDevWaitTimeout);
-            return -1;
-        }
-        backoff(it);
+// atomicMax(&base[key], v), one atomic per group of lanes with equal key.
+__device__ __forceinline__ void agg_max(int *base, int key, int v) {
+    const unsigned mask = __activemask();
+    const unsigned peers = __match_any_sync(mask, key);
+    const int mx = __reduce_max_sync(peers, v);
+    if ((int)(threadIdx.x & 31) == __ffs(peers) - 1) atomicMax(&base[key], mx);
+}
+
+// agg_add for a completion counter: every lane's earlier writes are visible
+// (at GPU scope) before the group's single increment is.
+__device__ __forceinline__ void agg_add_release(int *base, int key, int v) {
+    __threadfence();
+    const unsigned mask = __activemask();
+    const unsigned peers = __match_any_sync(mask, key);
+    const int sum = __reduce_add_sync(peers, v);
+    __syncwarp(peers);
+    if ((int)(threadIdx.x & 31) == __ffs(peers) - 1) {
+        __threadfence();
+        atomicAdd(&base[key], sum);
     }
+}
+
+// Pushes v (when v >= 0) of every lane; all 32 lanes of the warp must call it
+// together.  One tail reservation per warp.
+__device__ __forceinline__ void queue_push_warp(const WorkQueue &q, int v) {
+    const unsigned b = __ballot_sync(0xffffffffu, v >= 0);
+    if (!b) return;
+    const int lane = threadIdx.x & 31;
+    int base = 0;
+    if (lane == 0) base = atomicAdd(q.tail, __popc(b));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (v >= 0) {
+        __threadfence();
+        st_release(&q.items[base + __popc(b & ((1u << lane) - 1u))], v);
+    }
+}
+
+// Counts the items this warp finished (lanes with `finished`); all 32 lanes
+// call it after their pushes, so tail never lags done.
+__device__ __forceinline__ void queue_done_warp(const WorkQueue &q, bool finished) {
+    const unsigned b = __ballot_sync(0xffffffffu, finished);
+    __syncwarp();
+    if (b && (threadIdx.x & 31) == 0) {
+        __threadfence();
+        atomicAdd(q.done, __popc(b));
+    }
+}
+
+// Warp-cooperative, non-blocking pop; all 32 lanes call it together.  Each
+// lane keeps the queue index it claimed in h (-1: claim a new one) and fin
+// (true once the queue is drained for it).  Returns the lane's item, or -1
+// when it has none this round.  A lane never blocks on its own index, so a
+// lane whose item is pushed by a warp-mate cannot stall that warp-mate.
+__device__ __forceinline__ int queue_try_pop_warp(const WorkQueue &q, int &h, bool &fin) {
+    const int lane = threadIdx.x & 31;
+    const unsigned need = __ballot_sync(0xffffffffu, !fin && h < 0);
+    if (need) {
+        int base = 0;
+        if (lane == 0) base = atomicAdd(q.head, __popc(need));
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (!fin && h < 0) h = base + __popc(need & ((1u << lane) - 1u));
+    }
+    if (fin) return -1;
+    if (h < q.cap) {
+        const int v = ld_acquire(&q.items[h]);
+        if (v >= 0) {
+            h = -1;
+            return v;
+        }
+    }
+    // drained: every pushed item is processed and this index lies beyond them
+    const int d = ld_acquire(q.done);
+    const int t = ld_acquire(q.tail);
+    if (d == t && h >= t) fin = true;
+    return -1;
+}
+
+// End-of-round bookkeeping of a worklist warp: returns true when the warp
+// must leave (all lanes drained, or no progress for kSpinLimit rounds, which
+// is recorded in *status).
+__device__ __forceinline__ bool queue_round_end(bool fin, bool progressed, int64_t &idle, int *status) {
+    if (__all_sync(0xffffffffu, fin)) return true;
+    if (__any_sync(0xffffffffu, progressed)) {
+        idle = 0;
+        return false;
+    }
+    if (++idle > kSpinLimit) {
+        if ((threadIdx.x & 31) == 0) set_status(status, kDevWaitTimeout);
+        return true;
+    }
+    backoff(idle);
+    return false;
 }
 
 inline unsigned grid_1d(int64_t n, int block = kBlock, int maxBlocks = 1 << 20) {

@@ -327,133 +327,267 @@ CULS_HD int and_lookup(const AndTable &t, int in0, int in1, int c0, int c1, int 
     return table_find(t, and_key(in0, in1, c0, c1), status);
 }
 
+// ---------------------------------------- per-graph existence table
+// The existence table of one rewriting pass, split by graph: graph g owns
+// slots [off[g], off[g + 1]) and only its own nodes are inserted into or
+// looked up in that region, so passes that visit the nodes graph by graph
+// keep the region they probe resident in L2.  A slot is 16 bytes {key,
+// value}, so a probe touches one sector.  Duplicate keys keep the smallest
+// position, as in AndTable.
+struct alignas(16) TabSlot {
+    unsigned long long key;
+    int val;
+    int pad;
+};
+
+struct RegionTable {
+    TabSlot *slots;
+    const int64_t *off;  // G + 1 slot offsets
+};
+
+struct TabRegion {
+    TabSlot *slots;
+    uint32_t size;
+};
+
+CULS_HD TabRegion table_region(const RegionTable &t, int g) {
+    const int64_t a = t.off[g], b = t.off[g + 1];
+    return TabRegion{t.slots + a, (uint32_t)(b - a)};
+}
+
+// Home slot: the hash scaled onto [0, size) (multiply-high range reduction).
+CULS_HD uint32_t region_home(unsigned long long key, uint32_t size) {
+    return (uint32_t)(((unsigned long long)(uint32_t)mix64(key) * size) >> 32);
+}
+
+CULS_HD int region_insert(const TabRegion &t, unsigned long long key, int val, int *status) {
+    uint32_t h = region_home(key, t.size);
+    for (uint32_t probe = 0; probe < t.size; probe++) {
+        unsigned long long prev = at_cas(&t.slots[h].key, kEmptyKey, key);
+        if (prev == kEmptyKey || prev == key) {
+            at_min(&t.slots[h].val, val);
+            return (int)h;
+        }
+        if (++h == t.size) h = 0;
+    }
+    set_status(status, kDevTableFull);
+    return -1;
+}
+
+// Lookup in a region that no thread writes during the calling kernel.
+CULS_HD int region_find(const TabRegion &t, unsigned long long key, int *status) {
+    uint32_t h = region_home(key, t.size);
+    for (uint32_t probe = 0; probe < t.size; probe++) {
+#if defined(__CUDA_ARCH__)
+        const int4 s = *reinterpret_cast<const int4 *>(&t.slots[h]);
+        const unsigned long long k = ((unsigned long long)(uint32_t)s.y << 32) | (uint32_t)s.x;
+        if (k == key) return s.z;
+#else
+        const unsigned long long k = t.slots[h].key;
+        if (k == key) return t.slots[h].val;
+#endif
+        if (k == kEmptyKey) return -1;
+        if (++h == t.size) h = 0;
+    }
+    set_status(status, kDevTableFull);
+    return -1;
+}
+
+// TableLookup (src/algorithms/rewrite.cu:346-367) on a graph's region.
+CULS_HD int region_and_lookup(const TabRegion &t, int in0, int in1, int c0, int c1, int *status) {
+    if (in0 > in1) {
+        int x = in0;
+        in0 = in1;
+        in1 = x;
+        x = c0;
+        c0 = c1;
+        c1 = x;
+    }
+    return region_find(t, and_key(in0, in1, c0, c1), status);
+}
+
 // --------------------------------------------------------- evaluation
 struct EvalIn {
     const int *L0, *L1;  // fanin literals (the constant and PIs point at the constant)
     const int *ref;      // fanout counts incl. PO references
     const int *level;
     const RwLib *lib;
-    AndTable tab;
+    TabRegion tab;       // the region of the evaluated node's graph
     int *status;
 };
 
-// 8-entry reference table of CalcMFFC (src/algorithms/rewrite.cu:296-316)
+// 8-entry reference table of CalcMFFC (src/algorithms/rewrite.cu:296-316).
+// Every access below uses a compile-time index after unrolling, so the
+// table stays in registers.
 struct MffcTab {
     int size;
     int id[8];
     int num[8];
 };
 
-// Decrease, src/algorithms/rewrite.cu:296-309
-CULS_HD int mffc_decrease(int v, MffcTab &t, const int *leaves, const int *ref) {
+CULS_HD int pick8(const int (&v)[8], int i) {
+    int r = v[0];
+#pragma unroll
+    for (int k = 1; k < 8; k++)
+        if (k == i) r = v[k];
+    return r;
+}
+
+// Decrease, src/algorithms/rewrite.cu:296-309.  *slot receives the table
+// entry whose count was returned (unchanged for leaves and a full table).
+CULS_HD int mffc_decrease(int v, MffcTab &t, const int (&leaves)[4], const int *ref, int *slot) {
+#pragma unroll
     for (int i = 0; i < 4; i++)
         if (v == leaves[i]) return 1;
-    for (int i = 0; i < t.size; i++)
-        if (t.id[i] == v) return --t.num[i];
+    int found = -1;
+#pragma unroll
+    for (int i = 0; i < 8; i++)
+        if (found < 0 && i < t.size && t.id[i] == v) found = i;
+    if (found >= 0) {
+        int r = 0;
+#pragma unroll
+        for (int i = 0; i < 8; i++)
+            if (i == found) r = --t.num[i];
+        *slot = found;
+        return r;
+    }
     if (t.size == 8) return 1;
-    t.id[t.size] = v;
-    t.num[t.size] = ref[v] - 1;
+    const int r = ref[v] - 1;
+#pragma unroll
+    for (int i = 0; i < 8; i++)
+        if (i == t.size) {
+            t.id[i] = v;
+            t.num[i] = r;
+        }
+    *slot = t.size;
     t.size++;
-    return ref[v] - 1;
+    return r;
 }
 
 // IsDeleted, src/algorithms/rewrite.cu:312-316
 CULS_HD int mffc_deleted(int v, const MffcTab &t) {
-    for (int i = 0; i < t.size; i++)
-        if (t.id[i] == v) return t.num[i] == 0;
-    return 0;
+    int del = 0, found = 0;
+#pragma unroll
+    for (int i = 0; i < 8; i++)
+        if (!found && i < t.size && t.id[i] == v) {
+            found = 1;
+            del = t.num[i] == 0;
+        }
+    return del;
 }
 
-// CalcMFFC, src/algorithms/rewrite.cu:319-326, with the recursion unrolled
-// onto a stack of at most nine frames (a node is entered only when its table
-// count reaches zero, which happens once per table entry).
-CULS_HD int mffc_size(const EvalIn &E, int root, const int *leaves, MffcTab &t) {
-    int node[10], state[10], ans[10];
-    int sp = 0;
-    node[0] = root;
-    state[0] = 0;
-    ans[0] = 1;
+// CalcMFFC, src/algorithms/rewrite.cu:319-326, with the recursion replayed
+// on a register stack.  A frame above the root is entered only when a table
+// count reaches zero, so it is named by its table entry (3 bits); its state
+// (next fanin to visit) takes 2 bits.  At most nine frames exist (eight
+// table entries plus the root), and the result -- the root plus every node
+// entered -- is the number of frames pushed.
+CULS_HD int mffc_size(const EvalIn &E, int root, const int (&leaves)[4], MffcTab &t) {
+    uint32_t idxs = 0, states = 0;
+    int sp = 0, count = 1;
     while (true) {
-        int cur = node[sp];
-        if (state[sp] < 2) {
-            int v = (state[sp] == 0 ? E.L0[cur] : E.L1[cur]) >> 1;
-            state[sp]++;
-            if (mffc_decrease(v, t, leaves, E.ref) == 0) {
+        const int cur = sp == 0 ? root : pick8(t.id, (int)((idxs >> (3 * sp)) & 7u));
+        const uint32_t st = (states >> (2 * sp)) & 3u;
+        if (st < 2) {
+            const int v = (st == 0 ? E.L0[cur] : E.L1[cur]) >> 1;
+            states += 1u << (2 * sp);
+            int slot = 0;
+            if (mffc_decrease(v, t, leaves, E.ref, &slot) == 0) {
                 if (sp + 1 >= 10) {
                     set_status(E.status, kDevStackOverflow);
-                    return ans[0];
+                    return count;
                 }
                 sp++;
-                node[sp] = v;
-                state[sp] = 0;
-                ans[sp] = 1;
+                idxs = (idxs & ~(7u << (3 * sp))) | ((uint32_t)slot << (3 * sp));
+                states &= ~(3u << (2 * sp));
+                count++;
             }
             continue;
         }
-        if (sp == 0) return ans[0];
-        ans[sp - 1] += ans[sp];
+        if (sp == 0) return count;
         sp--;
     }
 }
 
+CULS_HD int clz64(uint64_t x) {
+#if defined(__CUDA_ARCH__)
+    return __clzll((long long)x);
+#else
+    return __builtin_clzll(x);
+#endif
+}
+
 // Number of library nodes the subgraph rooted at rt adds: unmatched nodes
 // reachable from rt through unmatched nodes (Eval, rewrite.cu:369-374).
-// unmatched has bit j set for library node j without a match.
+// unmatched has bit j set for library node j without a match.  Visits only
+// the reached nodes, highest index first.
 CULS_HD int lib_added(const RwLib *lib, int cls, int rt, uint64_t unmatched) {
     if (!((unmatched >> rt) & 1ull)) return 0;
-    uint64_t reach = 1ull << rt;
-    for (int j = rt; j >= 4; j--) {
-        if (!((reach >> j) & 1ull)) continue;
-        uint32_t w = lib->node[cls][j - 4];
-        int f0 = ln_f0(w), f1 = ln_f1(w);
-        if ((unmatched >> f0) & 1ull) reach |= 1ull << f0;
-        if ((unmatched >> f1) & 1ull) reach |= 1ull << f1;
+    uint64_t reach = 1ull << rt, todo = reach;
+    while (todo) {
+        const int j = 63 - clz64(todo);
+        todo &= ~(1ull << j);
+        const uint32_t w = lib->node[cls][j - 4];
+        const uint64_t nf = ((1ull << ln_f0(w)) | (1ull << ln_f1(w))) & unmatched & ~reach;
+        reach |= nf;
+        todo |= nf;
     }
     return popc64(reach);
 }
 
-// EvaluateNode for one node, src/algorithms/rewrite.cu:378-447.  `cuts`
-// holds the node's 8 slots; match/mlev are 54-entry scratch arrays.
-// Writes the chosen slot (or -1) and root index.
-CULS_HD void eval_node(const EvalIn &E, int q, int cpos, const Cut *cuts, bool useZeros, int *match, int *mlev,
-                       int &bestCut, int &bestOut) {
+template <class T>
+CULS_HD T pick4v(const T (&v)[4], int i) {
+    return i == 0 ? v[0] : (i == 1 ? v[1] : (i == 2 ? v[2] : v[3]));
+}
+
+// EvaluateNode for one node, src/algorithms/rewrite.cu:378-447.  cl/cm are
+// the node's 8 cut slots (leaves, {sign, packed}); match/mlev are 54-entry
+// scratch arrays.  Writes the chosen slot (or -1) and root index.
+CULS_HD void eval_node(const EvalIn &E, int q, int cpos, const int4 *cl, const int2 *cm, bool useZeros, int *match,
+                       int *mlev, int &bestCut, int &bestOut) {
     int reduction = -1, bestLevel = 99999999;
     bestCut = -1;
     bestOut = -1;
     for (int i = 0; i < 8; i++) {
-        const Cut &c = cuts[i];
-        if (!c.used || c.nLeaves < 3) continue;
-        int leaves[4] = {c.leaves[0], c.leaves[1], c.leaves[2], c.nLeaves == 3 ? cpos : c.leaves[3]};
+        const uint32_t pk = (uint32_t)cm[i].y;
+        const uint32_t nLeaves = packed_nleaves(pk);
+        if (!packed_used(pk) || nLeaves < 3) continue;
+        const int4 l = cl[i];
+        const int leaves[4] = {l.x, l.y, l.z, nLeaves == 3 ? cpos : l.w};
         MffcTab tab;
         tab.size = 0;
-        int saved = mffc_size(E, q, leaves, tab);
-        uint32_t npn = E.lib->npn[c.tt];
-        int uPhase = npn_phase(npn), cls = npn_class(npn);
-        const uint8_t *perm = E.lib->perm4[npn_perm(npn)];
+        const int saved = mffc_size(E, q, leaves, tab);
+        const uint32_t npn = E.lib->npn[pk & 0xFFFFu];
+        const int uPhase = npn_phase(npn), cls = npn_class(npn);
+        const uint32_t perm = *reinterpret_cast<const uint32_t *>(E.lib->perm4[npn_perm(npn)]);
         int isC = 0;
+#pragma unroll
         for (int j = 0; j < 4; j++) {
-            match[j] = leaves[perm[j]];
+            match[j] = pick4v(leaves, (int)((perm >> (8 * j)) & 255u));
             mlev[j] = E.level[match[j]];
             if (uPhase >> j & 1) isC |= 1 << j;
         }
         uint64_t unmatched = 0;
         const int nn = E.lib->nNodes[cls];
+        const uint32_t *lnodes = E.lib->node[cls];
         for (int j = 0; j < nn; j++) {
-            int num = j + 4;
-            uint32_t w = E.lib->node[cls][j];
-            int in0 = ln_f0(w), in1 = ln_f1(w);
-            mlev[num] = 1 + (mlev[in0] > mlev[in1] ? mlev[in0] : mlev[in1]);
+            const int num = j + 4;
+            const uint32_t w = lnodes[j];
+            const int in0 = ln_f0(w), in1 = ln_f1(w);
+            const int m0 = match[in0], m1 = match[in1];
+            const int lv0 = mlev[in0], lv1 = mlev[in1];
+            mlev[num] = 1 + (lv0 > lv1 ? lv0 : lv1);
             match[num] = -1;
-            bool uin0 = in0 >= 4 && ((unmatched >> in0) & 1ull);
-            bool uin1 = in1 >= 4 && ((unmatched >> in1) & 1ull);
-            if (uin0 || uin1 || match[in0] == q || match[in1] == q) {
+            const bool uin0 = in0 >= 4 && ((unmatched >> in0) & 1ull);
+            const bool uin1 = in1 >= 4 && ((unmatched >> in1) & 1ull);
+            if (uin0 || uin1 || m0 == q || m1 == q) {
                 unmatched |= 1ull << num;
                 continue;
             }
             // the reference's isC mask only has input bits (0..3)
-            int cc0 = (in0 < 4 ? ((isC >> in0) & 1) : 0) ^ ln_c0(w);
-            int cc1 = (in1 < 4 ? ((isC >> in1) & 1) : 0) ^ ln_c1(w);
-            int nodeId = and_lookup(E.tab, match[in0], match[in1], cc0, cc1, E.status);
+            const int cc0 = (in0 < 4 ? ((isC >> in0) & 1) : 0) ^ ln_c0(w);
+            const int cc1 = (in1 < 4 ? ((isC >> in1) & 1) : 0) ^ ln_c1(w);
+            const int nodeId = region_and_lookup(E.tab, m0, m1, cc0, cc1, E.status);
             if (nodeId != -1 && !mffc_deleted(nodeId, tab)) {
                 match[num] = nodeId;
                 mlev[num] = E.level[nodeId];
@@ -463,11 +597,11 @@ CULS_HD void eval_node(const EvalIn &E, int q, int cpos, const Cut *cuts, bool u
         }
         const int nr = E.lib->nRoots[cls];
         for (int out = 0; out < nr; out++) {
-            int rt = E.lib->roots[cls][out];
+            const int rt = E.lib->roots[cls][out];
             if (match[rt] == q) continue;
-            int added = lib_added(E.lib, cls, rt, unmatched);
-            int rtLevel = mlev[rt];
-            int gain = saved - added;
+            const int added = lib_added(E.lib, cls, rt, unmatched);
+            const int rtLevel = mlev[rt];
+            const int gain = saved - added;
             if (gain < 0 || (gain == 0 && !useZeros)) continue;
             if (gain < reduction || (gain == reduction && rtLevel >= bestLevel)) continue;
             reduction = gain;

@@ -14,6 +14,7 @@
 #include <algorithm>
 
 #include "rw_work.cuh"
+#include "sched.cuh"
 
 namespace culs {
 
@@ -43,19 +44,28 @@ __global__ void k_front_load(int64_t N, int G, const DevGraph *dg, const int *F0
     }
 }
 
-// lp = 2*level + phase.  Fanins precede their node in a graph-major layout,
-// so claiming chunks in increasing order never waits on an unclaimed chunk.
-__global__ void __launch_bounds__(kBlock) k_front_levelize(int64_t N, const int *a0, const int *a1, int *lp, int *done,
-                                                            int *counter, int *maxLevel, int *status) {
-    __shared__ int s_chunk;
+// lp = 2*level + phase.  Fanins precede their node inside its graph, and the
+// chunks are claimed in the interleaved schedule order (sched.cuh), so a
+// claimed chunk never waits on an unclaimed one.
+__global__ void __launch_bounds__(kBlock) k_front_levelize(ChunkSched S, const int *a0, const int *a1, int *lp,
+                                                            int *done, int *counter, int *maxLevel, int *status) {
+    __shared__ int64_t s_begin, s_end;
+    int myMax = 0;
     while (true) {
-        if (threadIdx.x == 0) s_chunk = atomicAdd(counter, 1);
+        if (threadIdx.x == 0) {
+            const int64_t c = atomicAdd(counter, 1);
+            if (c < S.total) {
+                sched_chunk(S, c, s_begin, s_end);
+            } else {
+                s_begin = s_end = -1;
+            }
+        }
         __syncthreads();
-        int64_t start = (int64_t)s_chunk * kBlock;
+        const int64_t begin = s_begin, end = s_end;
         __syncthreads();
-        if (start >= N) break;
-        int64_t p = start + threadIdx.x;
-        if (p >= N || lp[p] != -1) continue;
+        if (begin < 0) break;
+        int64_t p = begin + threadIdx.x;
+        if (p >= end || lp[p] != -1) continue;
         int f0 = a0[p], f1 = a1[p];
         int u0 = f0 >> 1, u1 = f1 >> 1;
         if (!wait_ge(&done[u0], 1, status) || !wait_ge(&done[u1], 1, status)) continue;
@@ -63,10 +73,13 @@ __global__ void __launch_bounds__(kBlock) k_front_levelize(int64_t N, const int 
         int lv = 1 + max(x0 >> 1, x1 >> 1);
         int ph = ((x0 & 1) ^ (f0 & 1)) & ((x1 & 1) ^ (f1 & 1));
         __stcg(&lp[p], 2 * lv + ph);
-        atomicMax(maxLevel, lv);
+        myMax = lv > myMax ? lv : myMax;
         __threadfence();
         st_release(&done[p], 1);
     }
+    // every thread of the block leaves the loop at the same claim
+    myMax = __reduce_max_sync(0xffffffffu, myMax);
+    if ((threadIdx.x & 31) == 0 && myMax > 0) atomicMax(maxLevel, myMax);
 }
 
 __global__ void k_front_keys(int64_t N, const int *lp, uint32_t *keys, int *vals) {
@@ -179,8 +192,10 @@ int rw_front(ExecCtx &X, Batch &b, RwWork &w) {
     int *cnt = X.counters;
     int rc;
     if ((rc = X.check(cudaMemsetAsync(cnt, 0, sizeof(int) * 8, s), "memset"))) return rc;
+    ChunkSched sched;
+    if ((rc = build_chunk_sched(X, b, kBlock, sched))) return rc;
     k_front_load<<<X.grid(N), kBlock, 0, s>>>(N, G, b.dg, b.F0, b.F1, gidIn, a0, a1, lp, done);
-    k_front_levelize<<<(unsigned)(X.sms * 8), kBlock, 0, s>>>(N, a0, a1, lp, done, cnt + 0, cnt + 1, X.status);
+    k_front_levelize<<<(unsigned)(X.sms * 8), kBlock, 0, s>>>(sched, a0, a1, lp, done, cnt + 0, cnt + 1, X.status);
     k_front_keys<<<X.grid(N), kBlock, 0, s>>>(N, lp, keys, vals);
     X.launched(3);
     if ((rc = X.check(cudaMemcpyAsync(X.hostSmall, cnt, sizeof(int) * 8, cudaMemcpyDeviceToHost, s), "d2h"))) return rc;
@@ -206,6 +221,7 @@ int rw_front(ExecCtx &X, Batch &b, RwWork &w) {
         X.launched(1);
         if ((rc = X.check(radix_sort_pairs(keys, vals, keys2, byGraph, N, gb, ar, s), "sort"))) return rc;
     }
+    w.byGraph = byGraph;
     k_front_local_ids<<<X.grid(N), kBlock, 0, s>>>(N, byGraph, w.wg, b.dg, w.wl, w.lidLow);
     if (b.nPO > 0) k_front_po<<<X.grid(b.nPO), kBlock, 0, s>>>(b.nPO, G, b.dg, b.PO, newPos, w.wpo);
     if ((rc = X.check(cudaMemsetAsync(w.ref, 0, sizeof(int) * N, s), "memset"))) return rc;

@@ -67,7 +67,7 @@ int Engine::rw(Batch &b, bool useZeros, bool gpuDedup, RwStats *stats, RwDump *d
     X.mark(kMkFront);
     if ((rc = rw_enumerate(X, w))) return rc;
     X.mark(kMkEnum);
-    if ((rc = rw_evaluate(X, w))) return rc;
+    if ((rc = rw_evaluate(X, w, b))) return rc;
     X.mark(kMkEval);
     if (wantDump) {
         std::vector<int4> L(N * 8);

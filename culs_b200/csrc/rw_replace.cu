@@ -31,7 +31,7 @@ struct RepArgs {
     const int *wg;
     const DevGraph *dg;
     const RwLib *lib;
-    AndTable tab;
+    RegionTable tab;
     const uint8_t *wph;
     int *status;
     // outputs
@@ -48,7 +48,9 @@ struct RepArgs {
 __device__ void rep_candidate(const RepArgs &A, int c, bool fill) {
     const int q = A.cand[c];
     const int slot = A.bestCut[q];
-    const int cpos = A.dg[A.wg[q]].cpos;
+    const int g = A.wg[q];
+    const int cpos = A.dg[g].cpos;
+    const TabRegion T = table_region(A.tab, g);
     int4 l = A.cutL[(int64_t)q * 8 + slot];
     Cut cut;
     cut_unpack((uint32_t)A.cutM[(int64_t)q * 8 + slot].y, cut);
@@ -79,7 +81,7 @@ __device__ void rep_candidate(const RepArgs &A, int c, bool fill) {
         if (match[in0] == -1 || match[in1] == -1) continue;
         int cc0 = (in0 < 4 ? ((isC >> in0) & 1) : 0) ^ ln_c0(w);
         int cc1 = (in1 < 4 ? ((isC >> in1) & 1) : 0) ^ ln_c1(w);
-        int id = and_lookup(A.tab, match[in0], match[in1], cc0, cc1, A.status);
+        int id = region_and_lookup(T, match[in0], match[in1], cc0, cc1, A.status);
         if (id != -1) match[j + 4] = id;
     }
     if (match[rt] == q) {  // the whole subgraph exists already: no replacement

@@ -71,7 +71,8 @@ struct RwWork {
     int *wpo = nullptr;                // PO literals
     int4 *cutL = nullptr;              // 8 cut slots per object: leaves
     int2 *cutM = nullptr;              //   {sign, packed}
-    AndTable tab{};
+    int *byGraph = nullptr;            // W positions grouped by graph (W order inside a graph)
+    RegionTable tab{};                 // existence table, one region per graph
     int8_t *bestCut = nullptr;  // chosen slot or -1
     uint8_t *bestOut = nullptr; // chosen subgraph root index
 
@@ -101,7 +102,7 @@ enum ChoiceCode : int {
 
 int rw_front(ExecCtx &X, Batch &b, RwWork &w);     // levelize, reorder, refs
 int rw_enumerate(ExecCtx &X, RwWork &w);           // cut enumeration
-int rw_evaluate(ExecCtx &X, RwWork &w);            // table + evaluation + candidates
+int rw_evaluate(ExecCtx &X, RwWork &w, const Batch &b);  // table + evaluation + candidates
 int rw_replace(ExecCtx &X, Batch &b, RwWork &w);   // subgraph build + rebuild ids
 int rw_choice(ExecCtx &X, Batch &b, RwWork &w, RwStats *stats);  // sequential choice per graph
 int rw_redundancy(ExecCtx &X, Batch &b, RwWork &w);  // buffer chasing

@@ -53,21 +53,22 @@ __global__ void k_dead_seed_flags(int64_t M, const int *L0, const int *cnt, uint
 // Reverse Kahn: a node whose fanout count reaches zero is dangling.
 __global__ void __launch_bounds__(kBlock) k_dead_queue(WorkQueue q, const int *L0, const int *L1, int *cnt,
                                                         uint8_t *dead, int *status) {
-    const int lane = threadIdx.x & 31;
+    int h = -1;
+    bool fin = false;
+    int64_t idle = 0;
     while (true) {
-        int base = 0;
-        if (lane == 0) base = atomicAdd(q.head, 32);
-        base = __shfl_sync(0xffffffffu, base, 0);
-        int v = queue_pop_wait(q, base + lane, status);
+        const int v = queue_try_pop_warp(q, h, fin);
+        int p0 = -1, p1 = -1;
         if (v >= 0) {
             dead[v] = 1;
             int u0 = L0[v] >> 1, u1 = L1[v] >> 1;
-            if (L0[u0] >= 0 && atomicSub(&cnt[u0], 1) == 1) queue_push(q, u0);
-            if (L0[u1] >= 0 && atomicSub(&cnt[u1], 1) == 1) queue_push(q, u1);
-            __threadfence();
-            atomicAdd(q.done, 1);
+            if (L0[u0] >= 0 && atomicSub(&cnt[u0], 1) == 1) p0 = u0;
+            if (L0[u1] >= 0 && atomicSub(&cnt[u1], 1) == 1) p1 = u1;
         }
-        if (__all_sync(0xffffffffu, v < 0)) break;
+        queue_push_warp(q, p0);
+        queue_push_warp(q, p1);
+        queue_done_warp(q, v >= 0);
+        if (queue_round_end(fin, v >= 0, idle, status)) break;
     }
 }
 
@@ -111,30 +112,38 @@ __global__ void __launch_bounds__(kBlock) k_level_queue(WorkQueue q, const int *
                                                          const int *adj, int *pending, int *level, const int *gid,
                                                          int *graphLevels, int *maxLevel, int *status) {
     const int lane = threadIdx.x & 31;
+    int myMax = 0;
+    int h = -1;
+    bool fin = false;
+    int64_t idle = 0;
     while (true) {
-        int base = 0;
-        if (lane == 0) base = atomicAdd(q.head, 32);
-        base = __shfl_sync(0xffffffffu, base, 0);
-        int v = queue_pop_wait(q, base + lane, status);
+        const int v = queue_try_pop_warp(q, h, fin);
+        int k = 0, e = 0;
         if (v >= 0) {
             int u0 = L0[v] >> 1, u1 = L1[v] >> 1;
             int l0 = L0[u0] >= 0 ? __ldcg(&level[u0]) : 0;
             int l1 = L0[u1] >= 0 ? __ldcg(&level[u1]) : 0;
             int lv = 1 + (l0 > l1 ? l0 : l1);
             __stcg(&level[v], lv);
-            atomicMax(&graphLevels[gid[v]], lv);
-            atomicMax(maxLevel, lv);
-            __threadfence();
-            int e = off[v + 1];
-            for (int k = off[v]; k < e; k++) {
-                int w = adj[k];
-                if (atomicSub(&pending[w], 1) == 1) queue_push(q, w);
-            }
-            __threadfence();
-            atomicAdd(q.done, 1);
+            agg_max(graphLevels, gid[v], lv);
+            myMax = lv > myMax ? lv : myMax;
+            k = off[v];
+            e = off[v + 1];
         }
-        if (__all_sync(0xffffffffu, v < 0)) break;
+        // release the fanouts, one fanout per lane per round
+        while (__any_sync(0xffffffffu, k < e)) {
+            int ready = -1;
+            if (k < e) {
+                const int w = adj[k++];
+                if (atomicSub(&pending[w], 1) == 1) ready = w;
+            }
+            queue_push_warp(q, ready);
+        }
+        queue_done_warp(q, v >= 0);
+        if (queue_round_end(fin, v >= 0, idle, status)) break;
     }
+    myMax = __reduce_max_sync(0xffffffffu, myMax);
+    if (lane == 0 && myMax > 0) atomicMax(maxLevel, myMax);
 }
 
 __global__ void k_gather_levels(int64_t n, const int *idx, const int *level, uint32_t *keys, int *lvlCnt) {
@@ -142,7 +151,7 @@ __global__ void k_gather_levels(int64_t n, const int *idx, const int *level, uin
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
         int l = level[idx[i]];
         keys[i] = (uint32_t)l;
-        atomicAdd(&lvlCnt[l], 1);
+        agg_add(lvlCnt, l, 1);
     }
 }
 
@@ -158,7 +167,10 @@ struct DedupArgs {
     const int *posOfRank;  // rank -> position
     const int *L0, *L1;
     const int *level;
-    const int *lvlCnt;
+    const int *lvlCnt;     // live AND nodes per level
+    const int *lvlStart;   // first processing index of each level
+    const int *chunkStart; // first chunk of each level (maxLevel + 2 entries)
+    int maxLevel;
     int *lvlDone;
     const int *gid;
     const DevGraph *dg;
@@ -170,6 +182,8 @@ struct DedupArgs {
     int *status;
 };
 
+constexpr int kDedupChunk = kBlock;
+
 __device__ __forceinline__ int resolve_map(const DedupArgs &A, int u) {
     int e = __ldcg(&A.mapEnc[u]);
     if (e >= 0) return e;
@@ -177,33 +191,72 @@ __device__ __forceinline__ int resolve_map(const DedupArgs &A, int u) {
     return 2 * A.posOfRank[r];
 }
 
-// In-order dataflow over the processing order: each node waits until every
-// node of its fanins' levels has been hashed, then maps, folds and hashes.
-__global__ void __launch_bounds__(kBlock) k_dedup(DedupArgs A) {
-    __shared__ int s_chunk;
+// chunks per level, for the level-aligned claim order of k_dedup
+__global__ void k_level_chunks(int n, const int *lvlCnt, int *cc) {
+    int stride = gridDim.x * blockDim.x;
+    for (int l = blockIdx.x * blockDim.x + threadIdx.x; l < n; l += stride)
+        cc[l] = (lvlCnt[l] + kDedupChunk - 1) / kDedupChunk;
+}
+
+// Dataflow over the processing order in chunks that never cross a level.
+// A chunk of level L needs its fanins' levels (< L) hashed: one thread waits
+// for the highest of them, since a level completes only after the level
+// below it has (every node of level L has a fanin on level L - 1).  The
+// chunk then maps, folds and hashes its nodes and adds its size to its
+// level's completion counter with one atomic.
+__global__ void __launch_bounds__(kDedupChunk) k_dedup(DedupArgs A) {
+    __shared__ int s_begin, s_end, s_level, s_need, s_ok;
     while (true) {
-        if (threadIdx.x == 0) s_chunk = atomicAdd(A.counter, 1);
-        __syncthreads();
-        const int64_t start = (int64_t)s_chunk * kBlock;
-        __syncthreads();
-        if (start >= A.nLive) break;
-        const int64_t t = start + threadIdx.x;
-        if (t >= A.nLive) continue;
-        int v = A.srt[t];
-        int lits[2] = {A.L0[v], A.L1[v]};
-        bool ok = true;
-        for (int k = 0; k < 2; k++) {
-            int u = lits[k] >> 1;
-            if (A.L0[u] < 0) continue;  // PI or constant keeps its literal
-            int lu = A.level[u];
-            if (!wait_ge(&A.lvlDone[lu], A.lvlCnt[lu], A.status)) {
-                ok = false;
-                break;
+        if (threadIdx.x == 0) {
+            const int c = atomicAdd(A.counter, 1);
+            if (c < A.chunkStart[A.maxLevel + 1]) {
+                int lo = 0, hi = A.maxLevel;
+                while (lo < hi) {  // last level whose first chunk is <= c
+                    int mid = (lo + hi + 1) >> 1;
+                    if (A.chunkStart[mid] <= c)
+                        lo = mid;
+                    else
+                        hi = mid - 1;
+                }
+                const int b = A.lvlStart[lo] + (c - A.chunkStart[lo]) * kDedupChunk;
+                const int e = A.lvlStart[lo] + A.lvlCnt[lo];
+                s_begin = b;
+                s_end = b + kDedupChunk < e ? b + kDedupChunk : e;
+                s_level = lo;
+            } else {
+                s_begin = -1;
             }
-            lits[k] = resolve_map(A, u) ^ (lits[k] & 1);
+            s_need = -1;
         }
-        int lv = A.level[v];
-        if (ok) {
+        __syncthreads();
+        const int begin = s_begin, end = s_end, lv = s_level;
+        if (begin < 0) break;
+        const int t = begin + (int)threadIdx.x;
+        const bool valid = t < end;
+        int v = 0, lits[2] = {0, 0};
+        if (valid) {
+            v = A.srt[t];
+            lits[0] = A.L0[v];
+            lits[1] = A.L1[v];
+            int need = -1;
+            for (int k = 0; k < 2; k++) {
+                const int u = lits[k] >> 1;
+                if (A.L0[u] >= 0) need = max(need, A.level[u]);
+            }
+            if (need >= 0) atomicMax(&s_need, need);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const int need = s_need;
+            s_ok = need < 0 ? 1 : (wait_ge(&A.lvlDone[need], A.lvlCnt[need], A.status) ? 1 : 0);
+        }
+        __syncthreads();
+        if (valid && s_ok) {
+            for (int k = 0; k < 2; k++) {
+                const int u = lits[k] >> 1;
+                if (A.L0[u] < 0) continue;  // PI or constant keeps its literal
+                lits[k] = resolve_map(A, u) ^ (lits[k] & 1);
+            }
             int l0 = lits[0], l1 = lits[1];
             if (l0 > l1) {
                 int x = l0;
@@ -236,7 +289,11 @@ __global__ void __launch_bounds__(kBlock) k_dedup(DedupArgs A) {
             }
         }
         __threadfence();
-        atomicAdd(&A.lvlDone[lv], 1);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            __threadfence();
+            atomicAdd(&A.lvlDone[lv], end - begin);
+        }
     }
 }
 
@@ -262,7 +319,7 @@ __global__ void k_winner_keys(int64_t n, const int *wl, const int *srt, const in
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
         int g = gid[srt[wl[i]]];
         keys[i] = (uint32_t)g;
-        atomicAdd(&cntG[g], 1);
+        agg_add(cntG, g, 1);
     }
 }
 
@@ -388,9 +445,13 @@ int Engine::strash_core(Batch &b, int64_t M, const int *L0, const int *L1, const
     int *vals2 = ar_.get<int>(nLive + 1);
     int *lvlCnt = ar_.get<int>(maxLevel + 2);
     int *lvlDone = ar_.get<int>(maxLevel + 2);
+    int *lvlStart = ar_.get<int>(maxLevel + 2);
+    int *chunkCnt = ar_.get<int>(maxLevel + 2);
+    int *chunkStart = ar_.get<int>(maxLevel + 2);
     int *tOf = pending;  // reuse
     int *rankOf = off;   // reuse (only needs M entries)
-    if (!srt || !keys || !keys2 || !vals2 || !lvlCnt || !lvlDone) return fail(CULS_E_OOM, "strash: arena exhausted");
+    if (!srt || !keys || !keys2 || !vals2 || !lvlCnt || !lvlDone || !lvlStart || !chunkCnt || !chunkStart)
+        return fail(CULS_E_OOM, "strash: arena exhausted");
     check(cudaMemsetAsync(lvlCnt, 0, sizeof(int) * (maxLevel + 2), s), "memset");
     check(cudaMemsetAsync(lvlDone, 0, sizeof(int) * (maxLevel + 2), s), "memset");
     if (nLive > 0) {
@@ -403,7 +464,11 @@ int Engine::strash_core(Batch &b, int64_t M, const int *L0, const int *L1, const
         k_inverse<<<gl, kBlock, 0, s>>>(nLive, srt, tOf);
         // tentative rank: processing order, or id order for the CPU variants
         k_inverse<<<gl, kBlock, 0, s>>>(nLive, idOrder ? liveIdx : srt, rankOf);
-        launches_ += 3;
+        // level-aligned chunks for the hashing dataflow
+        k_level_chunks<<<grid_1d(maxLevel + 1, kBlock, sms_ * 16), kBlock, 0, s>>>(maxLevel + 1, lvlCnt, chunkCnt);
+        launches_ += 4;
+        check(scan_exclusive(lvlCnt, lvlStart, maxLevel + 1, nullptr, ar_, s), "scan");
+        check(scan_exclusive(chunkCnt, chunkStart, maxLevel + 1, chunkStart + maxLevel + 1, ar_, s), "scan");
     }
     // 4. hash in dataflow order
     uint32_t cap = 1024;
@@ -419,8 +484,12 @@ int Engine::strash_core(Batch &b, int64_t M, const int *L0, const int *L1, const
     check(cudaMemsetAsync(tv, 0x7F, sizeof(int) * cap, s), "memset");
     check(cudaMemsetAsync(qc + 5, 0, sizeof(int), s), "memset");
     if (nLive > 0) {
-        DedupArgs A{nLive, srt,     rankOf, idOrder ? liveIdx : srt, L0,     L1,     level,      lvlCnt,         lvlDone,  gidA,
-                    b.dg,  AndTable{tk, tv, cap - 1}, mapEnc, kl0, kl1, foldTrivial ? 1 : 0, qc + 5, status_};
+        DedupArgs A{nLive,      srt,      rankOf,  idOrder ? liveIdx : srt,
+                    L0,         L1,       level,   lvlCnt,
+                    lvlStart,   chunkStart, maxLevel, lvlDone,
+                    gidA,       b.dg,     AndTable{tk, tv, cap - 1}, mapEnc,
+                    kl0,        kl1,      foldTrivial ? 1 : 0, qc + 5,
+                    status_};
         if (prof_) this->mark(kMkDedupK0);
         k_dedup<<<(unsigned)(sms_ * 8), kBlock, 0, s>>>(A);
         if (prof_) this->mark(kMkDedupK1);
