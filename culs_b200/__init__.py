@@ -221,7 +221,7 @@ class Context:
         return res
 
     PROFILE_NAMES = ["front", "enumerate", "evaluate", "replace", "choice", "redundancy", "dedup", "st",
-                     "k_enumerate", "k_evaluate", "k_dedup", "user"]
+                     "k_enumerate", "k_evaluate", "k_dedup", "user", "k_level"]
 
     def clone(self, d, into=None):
         if into is not None:

@@ -247,7 +247,8 @@ int culs_profile_read(culs_ctx *ctx, float *ms, int n) {
     const int pairs[][2] = {{kMkRwStart, kMkFront}, {kMkFront, kMkEnum},     {kMkEnum, kMkEval},
                             {kMkEval, kMkReplace},  {kMkReplace, kMkChoice}, {kMkChoice, kMkRedund},
                             {kMkRedund, kMkRwEnd},  {kMkStStart, kMkStEnd},  {kMkEnumK0, kMkEnumK1},
-                            {kMkEvalK0, kMkEvalK1}, {kMkDedupK0, kMkDedupK1}, {kMkUser0, kMkUser1}};
+                            {kMkEvalK0, kMkEvalK1}, {kMkDedupK0, kMkDedupK1}, {kMkUser0, kMkUser1},
+                            {kMkLevelK0, kMkLevelK1}};
     const int np = (int)(sizeof pairs / sizeof pairs[0]);
     for (int i = 0; i < n && i < np; i++) ms[i] = ctx->eng.elapsed(pairs[i][0], pairs[i][1]);
     return CULS_OK;

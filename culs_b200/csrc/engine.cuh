@@ -80,6 +80,8 @@ enum Mark : int {
     kMkDedupK1,
     kMkUser0,
     kMkUser1,
+    kMkLevelK0,
+    kMkLevelK1,
     kNumMarks
 };
 

@@ -68,6 +68,8 @@ static bool decode_lib(const unsigned char *b, size_t n, RwLib &L) {
         }
         memcpy(L.roots[c], b + cur, L.nRoots[c]);
         cur += L.nRoots[c];
+        for (int i = 0; i < L.nNodes[c]; i++)  // fanins precede their node
+            if (ln_f0(L.node[c][i]) >= i + 4 || ln_f1(L.node[c][i]) >= i + 4) return false;
     }
     return cur == n;
 }

@@ -336,8 +336,8 @@ CULS_HD int and_lookup(const AndTable &t, int in0, int in1, int c0, int c1, int 
 // position, as in AndTable.
 struct alignas(16) TabSlot {
     unsigned long long key;
-    int val;
-    int pad;
+    int val;  // smallest position with this key
+    int lvl;  // its level (equal for all nodes with one key: same fanins)
 };
 
 struct RegionTable {
@@ -360,12 +360,13 @@ CULS_HD uint32_t region_home(unsigned long long key, uint32_t size) {
     return (uint32_t)(((unsigned long long)(uint32_t)mix64(key) * size) >> 32);
 }
 
-CULS_HD int region_insert(const TabRegion &t, unsigned long long key, int val, int *status) {
+CULS_HD int region_insert(const TabRegion &t, unsigned long long key, int val, int lvl, int *status) {
     uint32_t h = region_home(key, t.size);
     for (uint32_t probe = 0; probe < t.size; probe++) {
         unsigned long long prev = at_cas(&t.slots[h].key, kEmptyKey, key);
         if (prev == kEmptyKey || prev == key) {
             at_min(&t.slots[h].val, val);
+            t.slots[h].lvl = lvl;
             return (int)h;
         }
         if (++h == t.size) h = 0;
@@ -391,6 +392,31 @@ CULS_HD int region_find(const TabRegion &t, unsigned long long key, int *status)
     }
     set_status(status, kDevTableFull);
     return -1;
+}
+
+CULS_HD int4 region_load(const TabRegion &t, uint32_t h) {
+#if defined(__CUDA_ARCH__)
+    return *reinterpret_cast<const int4 *>(&t.slots[h]);
+#else
+    const TabSlot &x = t.slots[h];
+    return int4{(int)(uint32_t)x.key, (int)(uint32_t)(x.key >> 32), x.val, x.lvl};
+#endif
+}
+
+// Finishes a lookup whose home slot h was already loaded into s: returns
+// {position, level} of the key, or {-1, 0} when absent.
+CULS_HD int2 region_resolve(const TabRegion &t, unsigned long long key, uint32_t h, int4 s, int *status) {
+    for (uint32_t probe = 0; probe < t.size; probe++) {
+        if (probe > 0) {
+            if (++h == t.size) h = 0;
+            s = region_load(t, h);
+        }
+        const unsigned long long k = ((unsigned long long)(uint32_t)s.y << 32) | (uint32_t)s.x;
+        if (k == key) return int2{s.z, s.w};
+        if (k == kEmptyKey) return int2{-1, 0};
+    }
+    set_status(status, kDevTableFull);
+    return int2{-1, 0};
 }
 
 // TableLookup (src/algorithms/rewrite.cu:346-367) on a graph's region.
@@ -540,76 +566,100 @@ CULS_HD T pick4v(const T (&v)[4], int i) {
     return i == 0 ? v[0] : (i == 1 ? v[1] : (i == 2 ? v[2] : v[3]));
 }
 
-// EvaluateNode for one node, src/algorithms/rewrite.cu:378-447.  cl/cm are
-// the node's 8 cut slots (leaves, {sign, packed}); match/mlev are 54-entry
-// scratch arrays.  Writes the chosen slot (or -1) and root index.
-CULS_HD void eval_node(const EvalIn &E, int q, int cpos, const int4 *cl, const int2 *cm, bool useZeros, int *match,
-                       int *mlev, int &bestCut, int &bestOut) {
-    int reduction = -1, bestLevel = 99999999;
-    bestCut = -1;
-    bestOut = -1;
-    for (int i = 0; i < 8; i++) {
-        const uint32_t pk = (uint32_t)cm[i].y;
-        const uint32_t nLeaves = packed_nleaves(pk);
-        if (!packed_used(pk) || nLeaves < 3) continue;
-        const int4 l = cl[i];
-        const int leaves[4] = {l.x, l.y, l.z, nLeaves == 3 ? cpos : l.w};
-        MffcTab tab;
-        tab.size = 0;
-        const int saved = mffc_size(E, q, leaves, tab);
-        const uint32_t npn = E.lib->npn[pk & 0xFFFFu];
-        const int uPhase = npn_phase(npn), cls = npn_class(npn);
-        const uint32_t perm = *reinterpret_cast<const uint32_t *>(E.lib->perm4[npn_perm(npn)]);
-        int isC = 0;
+// Best replacement of one cut: the body of EvaluateNode's cut loop
+// (src/algorithms/rewrite.cu:386-445) for cut slot packed word pk with
+// leaves l.  match/mlev are 54-entry scratch arrays with element j at
+// index j * stride.  Returns the first root (in root order) with the highest
+// gain and, among equal gains, the lowest level: out < 0 when no root
+// qualifies.
+struct CutBest {
+    int gain, level, out;
+};
+
+CULS_HD CutBest eval_cut(const EvalIn &E, int q, int cpos, uint32_t pk, int4 l, bool useZeros, int *match, int *mlev,
+                         int stride) {
+    CutBest best{-1, 0, -1};
+    const uint32_t nLeaves = packed_nleaves(pk);
+    const int leaves[4] = {l.x, l.y, l.z, nLeaves == 3 ? cpos : l.w};
+    MffcTab tab;
+    tab.size = 0;
+    const int saved = mffc_size(E, q, leaves, tab);
+    const uint32_t npn = E.lib->npn[pk & 0xFFFFu];
+    const int uPhase = npn_phase(npn), cls = npn_class(npn);
+    const uint32_t perm = *reinterpret_cast<const uint32_t *>(E.lib->perm4[npn_perm(npn)]);
+    int isC = 0;
 #pragma unroll
-        for (int j = 0; j < 4; j++) {
-            match[j] = pick4v(leaves, (int)((perm >> (8 * j)) & 255u));
-            mlev[j] = E.level[match[j]];
-            if (uPhase >> j & 1) isC |= 1 << j;
+    for (int j = 0; j < 4; j++) {
+        const int m = pick4v(leaves, (int)((perm >> (8 * j)) & 255u));
+        match[j * stride] = m;
+        mlev[j * stride] = E.level[m];
+        if (uPhase >> j & 1) isC |= 1 << j;
+    }
+    uint64_t unmatched = 0;
+    const int nn = E.lib->nNodes[cls];
+    const uint32_t *lnodes = E.lib->node[cls];
+    for (int j = 0; j < nn; j++) {
+        const int num = j + 4;
+        const uint32_t w = lnodes[j];
+        const int in0 = ln_f0(w), in1 = ln_f1(w);
+        const int m0 = match[in0 * stride], m1 = match[in1 * stride];
+        const int lv0 = mlev[in0 * stride], lv1 = mlev[in1 * stride];
+        mlev[num * stride] = 1 + (lv0 > lv1 ? lv0 : lv1);
+        match[num * stride] = -1;
+        const bool uin0 = in0 >= 4 && ((unmatched >> in0) & 1ull);
+        const bool uin1 = in1 >= 4 && ((unmatched >> in1) & 1ull);
+        if (uin0 || uin1 || m0 == q || m1 == q) {
+            unmatched |= 1ull << num;
+            continue;
         }
-        uint64_t unmatched = 0;
-        const int nn = E.lib->nNodes[cls];
-        const uint32_t *lnodes = E.lib->node[cls];
-        for (int j = 0; j < nn; j++) {
-            const int num = j + 4;
-            const uint32_t w = lnodes[j];
-            const int in0 = ln_f0(w), in1 = ln_f1(w);
-            const int m0 = match[in0], m1 = match[in1];
-            const int lv0 = mlev[in0], lv1 = mlev[in1];
-            mlev[num] = 1 + (lv0 > lv1 ? lv0 : lv1);
-            match[num] = -1;
-            const bool uin0 = in0 >= 4 && ((unmatched >> in0) & 1ull);
-            const bool uin1 = in1 >= 4 && ((unmatched >> in1) & 1ull);
-            if (uin0 || uin1 || m0 == q || m1 == q) {
-                unmatched |= 1ull << num;
-                continue;
-            }
-            // the reference's isC mask only has input bits (0..3)
-            const int cc0 = (in0 < 4 ? ((isC >> in0) & 1) : 0) ^ ln_c0(w);
-            const int cc1 = (in1 < 4 ? ((isC >> in1) & 1) : 0) ^ ln_c1(w);
-            const int nodeId = region_and_lookup(E.tab, m0, m1, cc0, cc1, E.status);
-            if (nodeId != -1 && !mffc_deleted(nodeId, tab)) {
-                match[num] = nodeId;
-                mlev[num] = E.level[nodeId];
-            } else {
-                unmatched |= 1ull << num;
-            }
+        // the reference's isC mask only has input bits (0..3)
+        int cc0 = (in0 < 4 ? ((isC >> in0) & 1) : 0) ^ ln_c0(w);
+        int cc1 = (in1 < 4 ? ((isC >> in1) & 1) : 0) ^ ln_c1(w);
+        int a = m0, b = m1;
+        if (a > b) {  // TableLookup orders the ids
+            const int x = a;
+            a = b;
+            b = x;
+            const int y = cc0;
+            cc0 = cc1;
+            cc1 = y;
         }
-        const int nr = E.lib->nRoots[cls];
-        for (int out = 0; out < nr; out++) {
-            const int rt = E.lib->roots[cls][out];
-            if (match[rt] == q) continue;
-            const int added = lib_added(E.lib, cls, rt, unmatched);
-            const int rtLevel = mlev[rt];
-            const int gain = saved - added;
-            if (gain < 0 || (gain == 0 && !useZeros)) continue;
-            if (gain < reduction || (gain == reduction && rtLevel >= bestLevel)) continue;
-            reduction = gain;
-            bestLevel = rtLevel;
-            bestCut = i;
-            bestOut = out;
+        const unsigned long long key = and_key(a, b, cc0, cc1);
+        const uint32_t home = region_home(key, E.tab.size);
+        // the slot carries the node's level, so a hit needs no second load
+        const int2 r = region_resolve(E.tab, key, home, region_load(E.tab, home), E.status);
+        if (r.x != -1 && !mffc_deleted(r.x, tab)) {
+            match[num * stride] = r.x;
+            mlev[num * stride] = r.y;
+        } else {
+            unmatched |= 1ull << num;
         }
     }
+    const int nr = E.lib->nRoots[cls];
+    for (int out = 0; out < nr; out++) {
+        const int rt = E.lib->roots[cls][out];
+        if (match[rt * stride] == q) continue;
+        const int added = lib_added(E.lib, cls, rt, unmatched);
+        const int rtLevel = mlev[rt * stride];
+        const int gain = saved - added;
+        if (gain < 0 || (gain == 0 && !useZeros)) continue;
+        if (best.out >= 0 && (gain < best.gain || (gain == best.gain && rtLevel >= best.level))) continue;
+        best = CutBest{gain, rtLevel, out};
+    }
+    return best;
+}
+
+// EvaluateNode's choice across cuts (src/algorithms/rewrite.cu:378-447):
+// cuts in slot order, a later cut wins only with a higher gain or an equal
+// gain at a lower level.  Folds cut i's best into (bestCut, bestOut, gain,
+// level).
+CULS_HD void fold_cut_best(const CutBest &c, int i, int &bestCut, int &bestOut, int &gain, int &level) {
+    if (c.out < 0) return;
+    if (bestCut >= 0 && (c.gain < gain || (c.gain == gain && c.level >= level))) return;
+    bestCut = i;
+    bestOut = c.out;
+    gain = c.gain;
+    level = c.level;
 }
 
 }  // namespace culs

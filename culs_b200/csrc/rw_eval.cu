@@ -1,11 +1,15 @@
 // Existence table and per-node evaluation: BuildHashTable + EvaluateNode
-// (CULS src/algorithms/rewrite.cu:378-471).  One thread per AND node; the
-// 54-entry match/level scratch of EvaluateNode lives in shared memory.  The
-// chained table of the reference becomes an open-addressing table on 64-bit
-// CAS keys (fanin0 id, fanin1 id, compl0, compl1) with one region per graph.
-// Both the build and the evaluation visit the nodes graph by graph (the
-// front's byGraph order), so the region, cuts and fanin arrays a thread
-// touches belong to the few graphs in flight.
+// (CULS src/algorithms/rewrite.cu:378-471).  The chained table of the
+// reference becomes an open-addressing table on 64-bit CAS keys (fanin0 id,
+// fanin1 id, compl0, compl1) with one region per graph.  Both the build and
+// the evaluation visit the nodes graph by graph (the front's byGraph order),
+// so the region, cuts and fanin arrays a block touches belong to the few
+// graphs in flight.
+//
+// One thread evaluates one AND node: its cuts in slot order, each walked
+// through the NPN class's library forest, with the 54-entry match/level
+// scratch in shared memory laid out entry-major, so lanes reading the same
+// library entry hit distinct banks.
 #include <vector>
 
 #include "rw_work.cuh"
@@ -15,6 +19,7 @@ namespace culs {
 namespace {
 
 constexpr int kEvalBlock = 64;
+constexpr int kLibSlots = 54;  // 4 inputs + at most 50 library nodes
 
 __global__ void k_table_clear(int64_t n, TabSlot *slots) {
     int64_t stride = (int64_t)gridDim.x * blockDim.x;
@@ -23,7 +28,7 @@ __global__ void k_table_clear(int64_t n, TabSlot *slots) {
 }
 
 __global__ void k_table_build(int64_t nL0, int64_t N, const int *byGraph, const int *w0, const int *w1, const int *wg,
-                              const DevGraph *dg, RegionTable tab, int *status) {
+                              const int *wlev, const DevGraph *dg, RegionTable tab, int *status) {
     int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += stride) {
         const int q = byGraph[i];
@@ -33,7 +38,7 @@ __global__ void k_table_build(int64_t nL0, int64_t N, const int *byGraph, const 
         int cp = dg[g].cpos;
         // rewrite.cu:454 skips nodes whose fanins are both the constant
         if ((f0 >> 1) == cp && (f1 >> 1) == cp) continue;
-        region_insert(table_region(tab, g), and_key(f0 >> 1, f1 >> 1, f0 & 1, f1 & 1), q, status);
+        region_insert(table_region(tab, g), and_key(f0 >> 1, f1 >> 1, f0 & 1, f1 & 1), q, wlev[q], status);
     }
 }
 
@@ -53,19 +58,26 @@ struct EvalArgs {
 };
 
 __global__ void __launch_bounds__(kEvalBlock) k_evaluate(EvalArgs A) {
-    __shared__ int s_match[kEvalBlock * 54];
-    __shared__ int s_mlev[kEvalBlock * 54];
-    int *match = &s_match[threadIdx.x * 54];
-    int *mlev = &s_mlev[threadIdx.x * 54];
+    __shared__ int s_match[kLibSlots * kEvalBlock];
+    __shared__ int s_mlev[kLibSlots * kEvalBlock];
+    int *match = s_match + threadIdx.x;
+    int *mlev = s_mlev + threadIdx.x;
     int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < A.N; i += stride) {
         const int64_t q = A.byGraph[i];
-        if (q < A.nL0) continue;
-        int bc = -1, bo = -1;
+        if (q < A.nL0) continue;  // constant or PI
         const int g = A.wg[q];
+        const int cpos = A.dg[g].cpos;
         EvalIn E = A.E;
         E.tab = table_region(A.tab, g);
-        eval_node(E, (int)q, A.dg[g].cpos, A.cutL + q * 8, A.cutM + q * 8, A.useZeros != 0, match, mlev, bc, bo);
+        int bc = -1, bo = -1, gain = 0, level = 0;
+        for (int k = 0; k < 8; k++) {
+            const uint32_t pk = (uint32_t)A.cutM[q * 8 + k].y;
+            if (!packed_used(pk) || packed_nleaves(pk) < 3) continue;
+            const CutBest b =
+                eval_cut(E, (int)q, cpos, pk, A.cutL[q * 8 + k], A.useZeros != 0, match, mlev, kEvalBlock);
+            fold_cut_best(b, k, bc, bo, gain, level);
+        }
         A.bestCut[q] = (int8_t)bc;
         A.bestOut[q] = (uint8_t)(bo < 0 ? 0 : bo);
         A.candFlag[q] = bc >= 0;
@@ -100,7 +112,8 @@ int rw_evaluate(ExecCtx &X, RwWork &w, const Batch &b) {
     if ((rc = X.check(cudaMemsetAsync(candFlag, 0, N, s), "memset"))) return rc;
     if (nAnd > 0) {
         k_table_clear<<<X.grid(nSlots), kBlock, 0, s>>>(nSlots, slots);
-        k_table_build<<<X.grid(N), kBlock, 0, s>>>(w.nL0, N, w.byGraph, w.w0, w.w1, w.wg, w.dg, w.tab, X.status);
+        k_table_build<<<X.grid(N), kBlock, 0, s>>>(w.nL0, N, w.byGraph, w.w0, w.w1, w.wg, w.wlev, w.dg, w.tab,
+                                                   X.status);
         EvalArgs A{w.nL0, N, w.byGraph, EvalIn{w.w0, w.w1, w.ref, w.wlev, X.lib, TabRegion{}, X.status}, w.tab,
                    w.cutL, w.cutM, w.wg, w.dg, w.useZeros ? 1 : 0, w.bestCut, w.bestOut, candFlag};
         X.mark(kMkEvalK0);

@@ -107,24 +107,67 @@ __global__ void k_csr_fill(int64_t M, const int *L0, const int *L1, const uint8_
     }
 }
 
+constexpr unsigned long long kNoItem = ~0ull;
+
+__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long *p) {
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_relaxed_u64(unsigned long long *p, unsigned long long v) {
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// Seeds of the level worklist: live AND nodes without AND fanins, level 1.
+__global__ void k_seed_items(int64_t n, const int *seeds, const int *nSeeds, unsigned long long *items) {
+    const int ns = *nSeeds;
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+        items[i] = i < ns ? ((unsigned long long)(uint32_t)seeds[i] | (1ull << 32)) : kNoItem;
+}
+
 // Forward Kahn: ASAP level of every live AND node (PIs and constant: 0).
-__global__ void __launch_bounds__(kBlock) k_level_queue(WorkQueue q, const int *L0, const int *L1, const int *off,
-                                                         const int *adj, int *pending, int *level, const int *gid,
-                                                         int *graphLevels, int *maxLevel, int *status) {
+// pending[v] = (highest level among v's finished AND fanins) << 2 | (AND
+// fanins not finished yet), updated by CAS.  The fanin that finishes last
+// reads v's level off its CAS and publishes the item {v, level} with one
+// 64-bit store, so a consumer needs no other thread's writes and the data
+// path has no fences.  Every live node is published exactly once, so a lane
+// whose queue index reaches the live count has nothing left to wait for.
+__global__ void __launch_bounds__(kBlock) k_level_queue(unsigned long long *items, int *head, int *tail,
+                                                         const int *nLivePtr, const int *L0, const int *L1,
+                                                         const int *off, const int *adj, int *pending, int *level,
+                                                         const int *gid, int *graphLevels, int *maxLevel,
+                                                         int *status) {
     const int lane = threadIdx.x & 31;
+    const int total = *nLivePtr;
     int myMax = 0;
     int h = -1;
     bool fin = false;
     int64_t idle = 0;
     while (true) {
-        const int v = queue_try_pop_warp(q, h, fin);
+        const unsigned need = __ballot_sync(0xffffffffu, !fin && h < 0);
+        if (need) {
+            int base = 0;
+            if (lane == 0) base = atomicAdd(head, __popc(need));
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (!fin && h < 0) h = base + __popc(need & ((1u << lane) - 1u));
+        }
+        int v = -1, lv = 0;
+        if (!fin) {
+            if (h >= total) {
+                fin = true;
+            } else {
+                const unsigned long long it = ld_relaxed_u64(&items[h]);
+                if (it != kNoItem) {
+                    v = (int)(uint32_t)it;
+                    lv = (int)(it >> 32);
+                    h = -1;
+                }
+            }
+        }
         int k = 0, e = 0;
         if (v >= 0) {
-            int u0 = L0[v] >> 1, u1 = L1[v] >> 1;
-            int l0 = L0[u0] >= 0 ? __ldcg(&level[u0]) : 0;
-            int l1 = L0[u1] >= 0 ? __ldcg(&level[u1]) : 0;
-            int lv = 1 + (l0 > l1 ? l0 : l1);
-            __stcg(&level[v], lv);
+            level[v] = lv;
             agg_max(graphLevels, gid[v], lv);
             myMax = lv > myMax ? lv : myMax;
             k = off[v];
@@ -132,15 +175,36 @@ __global__ void __launch_bounds__(kBlock) k_level_queue(WorkQueue q, const int *
         }
         // release the fanouts, one fanout per lane per round
         while (__any_sync(0xffffffffu, k < e)) {
-            int ready = -1;
+            unsigned long long item = kNoItem;
             if (k < e) {
                 const int w = adj[k++];
-                if (atomicSub(&pending[w], 1) == 1) ready = w;
+                int old = __ldcg(&pending[w]), nw;
+                while (true) {  // at most two updaters per word
+                    const int m = (old >> 2) > lv ? (old >> 2) : lv;
+                    nw = (m << 2) | ((old & 3) - 1);
+                    const int prev = atomicCAS(&pending[w], old, nw);
+                    if (prev == old) break;
+                    old = prev;
+                }
+                if ((old & 3) == 1) item = (unsigned long long)(uint32_t)w | ((unsigned long long)(1 + (nw >> 2)) << 32);
             }
-            queue_push_warp(q, ready);
+            const unsigned b = __ballot_sync(0xffffffffu, item != kNoItem);
+            if (b) {
+                int base = 0;
+                if (lane == 0) base = atomicAdd(tail, __popc(b));
+                base = __shfl_sync(0xffffffffu, base, 0);
+                if (item != kNoItem) st_relaxed_u64(&items[base + __popc(b & ((1u << lane) - 1u))], item);
+            }
         }
-        queue_done_warp(q, v >= 0);
-        if (queue_round_end(fin, v >= 0, idle, status)) break;
+        if (__all_sync(0xffffffffu, fin)) break;
+        if (__any_sync(0xffffffffu, v >= 0)) {
+            idle = 0;
+        } else if (++idle > kSpinLimit) {
+            if (lane == 0) set_status(status, kDevWaitTimeout);
+            break;
+        } else {
+            backoff(idle);
+        }
     }
     myMax = __reduce_max_sync(0xffffffffu, myMax);
     if (lane == 0 && myMax > 0) atomicMax(maxLevel, myMax);
@@ -422,23 +486,27 @@ int Engine::strash_core(Batch &b, int64_t M, const int *L0, const int *L1, const
     int *adj = ar_.get<int>(nEdges + 1);
     if (!adj) return fail(CULS_E_OOM, "strash: scratch arena exhausted");
     k_csr_fill<<<gridM, kBlock, 0, s>>>(M, L0, L1, liveFlag, cursor, adj);
-    check(fill_i32(items, -1, M + 1, s), "fill");
+    unsigned long long *items64 = ar_.get<unsigned long long>(M + 1);
+    int *liveIdx = ar_.get<int>(M + 1);
+    if (!items64 || !liveIdx) return fail(CULS_E_OOM, "strash: scratch arena exhausted");
     check(cudaMemsetAsync(qc, 0, sizeof(int) * 8, s), "memset");
     check(cudaMemsetAsync(graphLevels, 0, sizeof(int) * (G + 1), s), "memset");
     check(cudaMemsetAsync(level, 0, sizeof(int) * (M + 1), s), "memset");
-    check(compact_flags(flags, M, items, qc + 1, ar_, s), "compact");
-    k_level_queue<<<gridQ, kBlock, 0, s>>>(WorkQueue{items, qc + 0, qc + 1, qc + 2, (int)(M + 1)}, L0, L1, off, adj,
-                                           pending, level, gidA, graphLevels, qc + 4, status_);
+    check(compact_flags(flags, M, items, qc + 1, ar_, s), "compact");       // seeds; tail starts at their count
+    check(compact_flags(liveFlag, M, liveIdx, qc + 3, ar_, s), "compact");  // live list and count
+    k_seed_items<<<gridM, kBlock, 0, s>>>(M + 1, items, qc + 1, items64);
+    if (prof_) this->mark(kMkLevelK0);
+    k_level_queue<<<gridQ, kBlock, 0, s>>>(items64, qc + 0, qc + 1, qc + 3, L0, L1, off, adj, pending, level, gidA,
+                                           graphLevels, qc + 4, status_);
+    if (prof_) this->mark(kMkLevelK1);
     launches_ += 4;
-    // 3. live list, processing order (level, position) and tentative ranks
-    int *liveIdx = items;  // reuse: queue finished
-    check(compact_flags(liveFlag, M, liveIdx, qc + 3, ar_, s), "compact");
+    // 3. processing order (level, position) and tentative ranks
     check(cudaMemcpyAsync(hostSmall_, qc, sizeof(int) * 8, cudaMemcpyDeviceToHost, s), "d2h");
     if (sync()) return -1;
     if (check_status("strash levels")) return -1;
     int64_t nLive = hostSmall_[3];
     int maxLevel = hostSmall_[4];
-    if (hostSmall_[2] != nLive) return fail(CULS_E_INVALID, "strash: the AIG has a cycle");
+    if (hostSmall_[1] != nLive) return fail(CULS_E_INVALID, "strash: the AIG has a cycle");
     int *srt = ar_.get<int>(nLive + 1);
     uint32_t *keys = ar_.get<uint32_t>(nLive + 1);
     uint32_t *keys2 = ar_.get<uint32_t>(nLive + 1);

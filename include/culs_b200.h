@@ -170,7 +170,8 @@ int culs_graph_clone(culs_ctx *ctx, const culs_graph *src, culs_graph **dst);
  * (reset/levelize/reorder), cut enumeration, evaluation, replacement,
  * choice, redundancy removal, rw's deduplication, `st`, the enumeration
  * kernel alone, the evaluation kernel alone, the last strash hashing kernel,
- * user mark 0 -> 1 (-1 where an interval was not recorded). */
+ * user mark 0 -> 1, the last strash level worklist kernel (-1 where an
+ * interval was not recorded). */
 int culs_profile(culs_ctx *ctx, int enable);
 int culs_mark(culs_ctx *ctx, int slot);
 int culs_profile_read(culs_ctx *ctx, float *ms, int n);
