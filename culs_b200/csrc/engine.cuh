@@ -44,8 +44,16 @@ struct Batch {
     int *F0 = nullptr, *F1 = nullptr, *PO = nullptr;  // graph-local literals
     int64_t capObj = 0, capPO = 0;
     int capG = 0;
+    // spare fanin/PO buffers: strash writes its output there and swaps
+    int *F0s = nullptr, *F1s = nullptr, *POs = nullptr;
+    int64_t capObjS = 0, capPOS = 0;
     ~Batch();
     void release();
+    // Grows the buffers to hold nObj objects, nPO POs and G graphs (their
+    // contents are not kept); allocates nothing when they are large enough.
+    cudaError_t reserve(int64_t nObj, int64_t nPO, int G);
+    cudaError_t reserve_spare(int64_t nObj, int64_t nPO);
+    void swap_spare();
 };
 
 // Per-node dumps of the last rw (for parity checks); indexed by the graph's

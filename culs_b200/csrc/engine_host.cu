@@ -25,13 +25,64 @@ int ExecCtx::status_check(const char *what) {
 
 Batch::~Batch() { release(); }
 
+static cudaError_t grow(int **p, int64_t &cap, int64_t need) {
+    need = std::max<int64_t>(need, 1);
+    if (*p && cap >= need) return cudaSuccess;
+    cudaFree(*p);
+    *p = nullptr;
+    cap = 0;
+    cudaError_t e = cudaMalloc(p, sizeof(int) * need);
+    if (e == cudaSuccess) cap = need;
+    return e;
+}
+
+cudaError_t Batch::reserve(int64_t n, int64_t np, int g) {
+    int64_t c0 = capObj, c1 = capObj;
+    cudaError_t e;
+    if ((e = grow(&F0, c0, n)) != cudaSuccess) return e;
+    if ((e = grow(&F1, c1, n)) != cudaSuccess) return e;
+    capObj = std::min(c0, c1);
+    if ((e = grow(&PO, capPO, np)) != cudaSuccess) return e;
+    if (!dg || capG < std::max(g, 1)) {
+        cudaFree(dg);
+        dg = nullptr;
+        capG = 0;
+        if ((e = cudaMalloc(&dg, sizeof(DevGraph) * std::max(g, 1))) != cudaSuccess) return e;
+        capG = std::max(g, 1);
+    }
+    return cudaSuccess;
+}
+
+cudaError_t Batch::reserve_spare(int64_t n, int64_t np) {
+    int64_t c0 = capObjS, c1 = capObjS;
+    cudaError_t e;
+    if ((e = grow(&F0s, c0, n)) != cudaSuccess) return e;
+    if ((e = grow(&F1s, c1, n)) != cudaSuccess) return e;
+    capObjS = std::min(c0, c1);
+    return grow(&POs, capPOS, np);
+}
+
+void Batch::swap_spare() {
+    std::swap(F0, F0s);
+    std::swap(F1, F1s);
+    std::swap(PO, POs);
+    std::swap(capObj, capObjS);
+    std::swap(capPO, capPOS);
+}
+
 void Batch::release() {
     cudaFree(F0);
     cudaFree(F1);
     cudaFree(PO);
     cudaFree(dg);
+    cudaFree(F0s);
+    cudaFree(F1s);
+    cudaFree(POs);
     F0 = F1 = PO = nullptr;
+    F0s = F1s = POs = nullptr;
     dg = nullptr;
+    capObj = capPO = capObjS = capPOS = 0;
+    capG = 0;
     G = 0;
     nObj = nPO = 0;
     hg.clear();
@@ -175,13 +226,8 @@ float Engine::elapsed(int a, int b) {
 
 int Engine::clone(const Batch &src, Batch &dst) {
     if (&src == &dst) return 0;
-    dst.release();
     int rc;
-    const int64_t n = std::max<int64_t>(src.nObj, 1), np = std::max<int64_t>(src.nPO, 1);
-    if ((rc = check(cudaMalloc(&dst.F0, sizeof(int) * n), "cudaMalloc"))) return rc;
-    if ((rc = check(cudaMalloc(&dst.F1, sizeof(int) * n), "cudaMalloc"))) return rc;
-    if ((rc = check(cudaMalloc(&dst.PO, sizeof(int) * np), "cudaMalloc"))) return rc;
-    if ((rc = check(cudaMalloc(&dst.dg, sizeof(DevGraph) * std::max(src.G, 1)), "cudaMalloc"))) return rc;
+    if ((rc = check(dst.reserve(src.nObj, src.nPO, src.G), "cudaMalloc"))) return rc;
     cudaMemcpyAsync(dst.F0, src.F0, sizeof(int) * src.nObj, cudaMemcpyDeviceToDevice, s_);
     cudaMemcpyAsync(dst.F1, src.F1, sizeof(int) * src.nObj, cudaMemcpyDeviceToDevice, s_);
     if (src.nPO) cudaMemcpyAsync(dst.PO, src.PO, sizeof(int) * src.nPO, cudaMemcpyDeviceToDevice, s_);
@@ -237,12 +283,8 @@ int Engine::upload(Batch &b, int count, const int32_t *const *f0, const int32_t 
         hg[g].nLevels = mx;
         if (nPOs[g]) memcpy(&hPO[hg[g].poOff], outs[g], sizeof(int32_t) * nPOs[g]);
     }
-    b.release();
     int rc;
-    if ((rc = check(cudaMalloc(&b.F0, sizeof(int) * nObj), "cudaMalloc"))) return rc;
-    if ((rc = check(cudaMalloc(&b.F1, sizeof(int) * nObj), "cudaMalloc"))) return rc;
-    if ((rc = check(cudaMalloc(&b.PO, sizeof(int) * std::max<int64_t>(nPO, 1)), "cudaMalloc"))) return rc;
-    if ((rc = check(cudaMalloc(&b.dg, sizeof(DevGraph) * count), "cudaMalloc"))) return rc;
+    if ((rc = check(b.reserve(nObj, nPO, count), "cudaMalloc"))) return rc;
     cudaMemcpyAsync(b.F0, hF0.data(), sizeof(int) * nObj, cudaMemcpyHostToDevice, s_);
     cudaMemcpyAsync(b.F1, hF1.data(), sizeof(int) * nObj, cudaMemcpyHostToDevice, s_);
     if (nPO) cudaMemcpyAsync(b.PO, hPO.data(), sizeof(int) * nPO, cudaMemcpyHostToDevice, s_);

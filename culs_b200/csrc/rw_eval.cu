@@ -6,10 +6,10 @@
 // so the region, cuts and fanin arrays a block touches belong to the few
 // graphs in flight.
 //
-// One thread evaluates one AND node: its cuts in slot order, each walked
-// through the NPN class's library forest, with the 54-entry match/level
-// scratch in shared memory laid out entry-major, so lanes reading the same
-// library entry hit distinct banks.
+// Evaluation works on (node, cut) items grouped by NPN class per warp (see
+// k_evaluate); the match/level scratch of a library walk lives in shared
+// memory laid out entry-major, so lanes reading the same library entry hit
+// distinct banks.
 #include <vector>
 
 #include "rw_work.cuh"
@@ -20,6 +20,13 @@ namespace {
 
 constexpr int kEvalBlock = 64;
 constexpr int kLibSlots = 54;  // 4 inputs + at most 50 library nodes
+// Library scratch entries kept in shared memory per thread: forests of up to
+// kLibFast - 4 nodes (every frequent class) evaluate there; larger ones use
+// a per-thread column of a global scratch array.  The smaller shared
+// footprint keeps 22 warps resident per SM instead of 16.
+constexpr int kLibFast = 38;
+constexpr int kClassSlots = 224;  // >= the library's 222 classes, a multiple of 32
+static_assert(kClassSlots >= kNumClasses && kClassSlots % 32 == 0, "class slots");
 
 __global__ void k_table_clear(int64_t n, TabSlot *slots) {
     int64_t stride = (int64_t)gridDim.x * blockDim.x;
@@ -45,6 +52,7 @@ __global__ void k_table_build(int64_t nL0, int64_t N, const int *byGraph, const 
 struct EvalArgs {
     int64_t nL0, N;
     const int *byGraph;
+    int *scratch;  // 2 * kLibSlots ints per thread of the grid, thread-minor
     EvalIn E;
     RegionTable tab;
     const int4 *cutL;
@@ -57,30 +65,118 @@ struct EvalArgs {
     uint8_t *candFlag;
 };
 
+// Per-warp shared state of k_evaluate: the warp's 32 nodes' evaluable cuts
+// as items grouped by NPN class, and one result per (node, slot).
+struct WarpItems {
+    int off[kClassSlots];    // class counts, then exclusive offsets
+    uint16_t item[32 * 8];   // node lane * 8 + slot, in class order
+    int2 res[32 * 8];        // {gain * 16 + root index, level} or {-1, 0}
+};
+
+// A warp takes 32 consecutive nodes of the graph-major order, sorts their
+// evaluable cuts by NPN class and evaluates them 32 at a time, so the lanes
+// of a round mostly walk the same library forest (the forests' sizes differ
+// several-fold between classes).  Each lane then folds its own node's
+// results in slot order, the order of the reference's loop.  Warps never
+// wait for one another.
 __global__ void __launch_bounds__(kEvalBlock) k_evaluate(EvalArgs A) {
-    __shared__ int s_match[kLibSlots * kEvalBlock];
-    __shared__ int s_mlev[kLibSlots * kEvalBlock];
+    __shared__ int s_match[kLibFast * kEvalBlock];
+    __shared__ int s_mlev[kLibFast * kEvalBlock];
+    __shared__ WarpItems s_w[kEvalBlock / 32];
     int *match = s_match + threadIdx.x;
     int *mlev = s_mlev + threadIdx.x;
-    int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < A.N; i += stride) {
-        const int64_t q = A.byGraph[i];
-        if (q < A.nL0) continue;  // constant or PI
-        const int g = A.wg[q];
-        const int cpos = A.dg[g].cpos;
-        EvalIn E = A.E;
-        E.tab = table_region(A.tab, g);
-        int bc = -1, bo = -1, gain = 0, level = 0;
-        for (int k = 0; k < 8; k++) {
-            const uint32_t pk = (uint32_t)A.cutM[q * 8 + k].y;
-            if (!packed_used(pk) || packed_nleaves(pk) < 3) continue;
-            const CutBest b =
-                eval_cut(E, (int)q, cpos, pk, A.cutL[q * 8 + k], A.useZeros != 0, match, mlev, kEvalBlock);
-            fold_cut_best(b, k, bc, bo, gain, level);
+    const int lane = threadIdx.x & 31;
+    WarpItems &W = s_w[threadIdx.x >> 5];
+    const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int gstride = gridDim.x * blockDim.x;
+    int *gmatch = A.scratch + gtid;
+    int *gmlev = A.scratch + (int64_t)kLibSlots * gstride + gtid;
+    const int64_t nWarpChunks = (A.N + 31) / 32;
+    const int64_t warpStride = (int64_t)gridDim.x * (kEvalBlock / 32);
+    for (int64_t wc = (int64_t)blockIdx.x * (kEvalBlock / 32) + (threadIdx.x >> 5); wc < nWarpChunks;
+         wc += warpStride) {
+        const int64_t base = wc * 32;
+        for (int c = lane; c < kClassSlots; c += 32) W.off[c] = 0;
+        __syncwarp();
+        // 1. this lane's node: its evaluable cuts and their classes
+        int64_t q = -1;
+        if (base + lane < A.N) {
+            q = A.byGraph[base + lane];
+            if (q < A.nL0) q = -1;  // constant or PI
         }
-        A.bestCut[q] = (int8_t)bc;
-        A.bestOut[q] = (uint8_t)(bo < 0 ? 0 : bo);
-        A.candFlag[q] = bc >= 0;
+        uint32_t clsRank[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            clsRank[k] = 0xFFFFFFFFu;
+            W.res[lane * 8 + k] = make_int2(-1, 0);
+            if (q >= 0) {
+                const uint32_t pk = (uint32_t)A.cutM[q * 8 + k].y;
+                if (packed_used(pk) && packed_nleaves(pk) >= 3) {
+                    const int cls = npn_class(A.E.lib->npn[pk & 0xFFFFu]);
+                    clsRank[k] = ((uint32_t)cls << 16) | (uint32_t)atomicAdd(&W.off[cls], 1);
+                }
+            }
+        }
+        __syncwarp();
+        // 2. exclusive scan of the class counts, kClassSlots / 32 per lane
+        int v[kClassSlots / 32], sum = 0;
+#pragma unroll
+        for (int t = 0; t < kClassSlots / 32; t++) {
+            v[t] = W.off[lane * (kClassSlots / 32) + t];
+            sum += v[t];
+        }
+        int inc = sum;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, inc, d);
+            if (lane >= d) inc += y;
+        }
+        const int nItems = __shfl_sync(0xffffffffu, inc, 31);
+        int run = inc - sum;
+        __syncwarp();
+#pragma unroll
+        for (int t = 0; t < kClassSlots / 32; t++) {
+            W.off[lane * (kClassSlots / 32) + t] = run;
+            run += v[t];
+        }
+        __syncwarp();
+#pragma unroll
+        for (int k = 0; k < 8; k++)
+            if (clsRank[k] != 0xFFFFFFFFu)
+                W.item[W.off[clsRank[k] >> 16] + (clsRank[k] & 0xFFFFu)] = (uint16_t)(lane * 8 + k);
+        __syncwarp();
+        // 3. evaluate the items, 32 per round, in class order
+        for (int it = lane; it < nItems; it += 32) {
+            const int slot = W.item[it];
+            const int qq = A.byGraph[base + (slot >> 3)];
+            const int g = A.wg[qq];
+            EvalIn E = A.E;
+            E.tab = table_region(A.tab, g);
+            const int64_t idx = (int64_t)qq * 8 + (slot & 7);
+            const uint32_t pk = (uint32_t)A.cutM[idx].y;
+            const int4 l = A.cutL[idx];
+            const int cpos = A.dg[g].cpos;
+            CutBest b;
+            if (4 + A.E.lib->nNodes[npn_class(A.E.lib->npn[pk & 0xFFFFu])] <= kLibFast)
+                b = eval_cut(E, qq, cpos, pk, l, A.useZeros != 0, match, mlev, kEvalBlock);
+            else  // a large forest: scratch in global memory
+                b = eval_cut(E, qq, cpos, pk, l, A.useZeros != 0, gmatch, gmlev, gstride);
+            if (b.out >= 0) W.res[slot] = make_int2(b.gain * 16 + b.out, b.level);
+        }
+        __syncwarp();
+        // 4. fold this lane's node's cuts in slot order
+        if (q >= 0) {
+            int bc = -1, bo = -1, gain = 0, level = 0;
+#pragma unroll
+            for (int k = 0; k < 8; k++) {
+                const int2 r = W.res[lane * 8 + k];
+                if (r.x >= 0) fold_cut_best(CutBest{r.x >> 4, r.y, r.x & 15}, k, bc, bo, gain, level);
+            }
+            A.bestCut[q] = (int8_t)bc;
+            A.bestOut[q] = (uint8_t)(bo < 0 ? 0 : bo);
+            A.candFlag[q] = bc >= 0;
+        }
+        __syncwarp();
     }
 }
 
@@ -101,7 +197,9 @@ int rw_evaluate(ExecCtx &X, RwWork &w, const Batch &b) {
     w.bestOut = X.ar->get<uint8_t>(N);
     uint8_t *candFlag = X.ar->get<uint8_t>(N);
     w.cand = X.ar->get<int>(N);
-    if (!slots || !dOff || !w.bestCut || !w.bestOut || !candFlag || !w.cand)
+    const unsigned evalGrid = X.grid(N, kEvalBlock);
+    int *scratch = X.ar->get<int>((size_t)2 * kLibSlots * evalGrid * kEvalBlock);
+    if (!slots || !dOff || !w.bestCut || !w.bestOut || !candFlag || !w.cand || !scratch)
         return X.fail(CULS_E_OOM, "rw: scratch arena exhausted (table)");
     w.tab = RegionTable{slots, dOff};
     int rc;
@@ -114,10 +212,10 @@ int rw_evaluate(ExecCtx &X, RwWork &w, const Batch &b) {
         k_table_clear<<<X.grid(nSlots), kBlock, 0, s>>>(nSlots, slots);
         k_table_build<<<X.grid(N), kBlock, 0, s>>>(w.nL0, N, w.byGraph, w.w0, w.w1, w.wg, w.wlev, w.dg, w.tab,
                                                    X.status);
-        EvalArgs A{w.nL0, N, w.byGraph, EvalIn{w.w0, w.w1, w.ref, w.wlev, X.lib, TabRegion{}, X.status}, w.tab,
+        EvalArgs A{w.nL0, N, w.byGraph, scratch, EvalIn{w.w0, w.w1, w.ref, w.wlev, X.lib, TabRegion{}, X.status}, w.tab,
                    w.cutL, w.cutM, w.wg, w.dg, w.useZeros ? 1 : 0, w.bestCut, w.bestOut, candFlag};
         X.mark(kMkEvalK0);
-        k_evaluate<<<X.grid(N, kEvalBlock), kEvalBlock, 0, s>>>(A);
+        k_evaluate<<<evalGrid, kEvalBlock, 0, s>>>(A);
         X.mark(kMkEvalK1);
         X.launched(3);
     }

@@ -620,16 +620,10 @@ int Engine::strash_core(Batch &b, int64_t M, const int *L0, const int *L1, const
     }
     int64_t nObjNew = base;
     DevGraph *dgNew = reinterpret_cast<DevGraph *>(ar_.get<char>(sizeof(DevGraph) * (G + 1)));
-    int *F0n = nullptr, *F1n = nullptr, *POn = nullptr;
     if (!dgNew) return fail(CULS_E_OOM, "strash: arena");
-    if (check(cudaMalloc(&F0n, sizeof(int) * (nObjNew + 1)), "cudaMalloc") ||
-        check(cudaMalloc(&F1n, sizeof(int) * (nObjNew + 1)), "cudaMalloc") ||
-        check(cudaMalloc(&POn, sizeof(int) * (nPO + 1)), "cudaMalloc")) {
-        cudaFree(F0n);
-        cudaFree(F1n);
-        cudaFree(POn);
-        return -1;
-    }
+    // the output goes to the batch's spare buffers, swapped in at the end
+    if (check(b.reserve_spare(nObjNew + 1, nPO + 1), "cudaMalloc")) return -1;
+    int *F0n = b.F0s, *F1n = b.F1s, *POn = b.POs;
     check(cudaMemcpyAsync(dgNew, ng.data(), sizeof(DevGraph) * G, cudaMemcpyHostToDevice, s), "h2d");
     check(fill_i32(F0n, -1, nObjNew, s), "fill");
     check(fill_i32(F1n, -1, nObjNew, s), "fill");
@@ -643,18 +637,8 @@ int Engine::strash_core(Batch &b, int64_t M, const int *L0, const int *L1, const
                                                                                                              O);
     launches_ += 1;
     check(cudaMemcpyAsync(b.dg, ng.data(), sizeof(DevGraph) * G, cudaMemcpyHostToDevice, s), "h2d");
-    if (sync()) {
-        cudaFree(F0n);
-        cudaFree(F1n);
-        cudaFree(POn);
-        return -1;
-    }
-    cudaFree(b.F0);
-    cudaFree(b.F1);
-    cudaFree(b.PO);
-    b.F0 = F0n;
-    b.F1 = F1n;
-    b.PO = POn;
+    if (sync()) return -1;
+    b.swap_spare();
     b.hg = ng;
     b.nObj = nObjNew;
     ar_.reset();
