@@ -112,15 +112,18 @@ __device__ __forceinline__ void load_rcut(const EnumArgs &A, int64_t idx, int2 m
     rc_unpack_aux((uint32_t)x.x, (uint32_t)x.y, c);
 }
 
+// Warps claim 32 consecutive positions at a time.  A lane publishes its node
+// before it next waits on its warp, and fanins lie at lower positions, so a
+// lane never waits on a warp-mate that waits on it.
 __global__ void __launch_bounds__(kEnumBlock, 4) k_enumerate(EnumArgs A) {
-    __shared__ int s_chunk;
+    const int lane = threadIdx.x & 31;
     while (true) {
-        if (threadIdx.x == 0) s_chunk = atomicAdd(A.counter, 1);
-        __syncthreads();
-        const int64_t start = A.nL0 + (int64_t)s_chunk * kEnumBlock;
-        __syncthreads();
+        int chunk = 0;
+        if (lane == 0) chunk = atomicAdd(A.counter, 1);
+        chunk = __shfl_sync(0xffffffffu, chunk, 0);
+        const int64_t start = A.nL0 + (int64_t)chunk * 32;
         if (start >= A.N) break;
-        const int64_t q = start + threadIdx.x;
+        const int64_t q = start + lane;
         if (q >= A.N) continue;
         Slot S[8];
 #pragma unroll
@@ -146,20 +149,37 @@ __global__ void __launch_bounds__(kEnumBlock, 4) k_enumerate(EnumArgs A) {
         bool ok = wait_ge(&A.done[u0], 1, A.status) && wait_ge(&A.done[u1], 1, A.status);
         if (ok) {
             const int2 *M0 = A.cutM + (int64_t)u0 * 8, *M1 = A.cutM + (int64_t)u1 * 8;
-            bool stop = false;
-#pragma unroll 1
-            for (int i = 0; i < 8 && !stop; i++) {
-                const int2 mi = M0[i];
-                if (!packed_used((uint32_t)mi.y)) continue;
-                RCut a;
-                load_rcut(A, (int64_t)u0 * 8 + i, mi, a);
-#pragma unroll 1
-                for (int j = 0; j < 8 && !stop; j++) {
+            // the pairs CutEnumerate tries (both slots used, at most 4 leaves
+            // by signature), bit i * 8 + j: visiting the set bits in order is
+            // the reference's i-major loop, and every lane takes its k-th pair
+            // in the same iteration
+            uint64_t pairs = 0;
+            {
+                uint32_t s1[8], used1 = 0;
+#pragma unroll
+                for (int j = 0; j < 8; j++) {
                     const int2 mj = M1[j];
-                    if (!packed_used((uint32_t)mj.y)) continue;
-                    if (popc32((uint32_t)mi.x | (uint32_t)mj.x) > 4) continue;
-                    RCut b;
-                    load_rcut(A, (int64_t)u1 * 8 + j, mj, b);
+                    s1[j] = (uint32_t)mj.x;
+                    used1 |= packed_used((uint32_t)mj.y) << j;
+                }
+#pragma unroll
+                for (int i = 0; i < 8; i++) {
+                    const int2 mi = M0[i];
+                    if (!packed_used((uint32_t)mi.y)) continue;
+#pragma unroll
+                    for (int j = 0; j < 8; j++)
+                        if (((used1 >> j) & 1u) && popc32((uint32_t)mi.x | s1[j]) <= 4)
+                            pairs |= 1ull << (i * 8 + j);
+                }
+            }
+            while (pairs) {
+                const int p = __ffsll((long long)pairs) - 1;
+                pairs &= pairs - 1;
+                const int i = p >> 3, j = p & 7;
+                {
+                    RCut a, b;
+                    load_rcut(A, (int64_t)u0 * 8 + i, M0[i], a);
+                    load_rcut(A, (int64_t)u1 * 8 + j, M1[j], b);
                     // FindCut: first unused slot, else lowest value among
                     // >2-leaf, then 2-leaf, then smaller cuts (rewrite.cu:84-109)
                     int id = -1;
@@ -211,7 +231,7 @@ __global__ void __launch_bounds__(kEnumBlock, 4) k_enumerate(EnumArgs A) {
 #pragma unroll
                     for (int k = 0; k < 8; k++)
                         if (k == id) S[k].pk = cut_pack(pc);
-                    if (m.n < 2) stop = true;  // rewrite.cu:291
+                    if (m.n < 2) pairs = 0;  // enumeration of this node stops (rewrite.cu:291)
                 }
             }
         }
