@@ -58,6 +58,7 @@ _lib.culs_graph_free.argtypes = [_vp]
 _lib.culs_graph_count.argtypes = [_vp]
 _lib.culs_graph_stats.argtypes = [_vp, ctypes.c_int, _ip, _ip, _ip, _ip]
 _lib.culs_batch_download.argtypes = [_vp, _vp, ctypes.POINTER(_HostGraph)]
+_lib.culs_batch_download_into.argtypes = [_vp, _vp, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
 _lib.culs_graph_download.argtypes = [_vp, _vp, ctypes.c_int, _ip, _ip, _ip]
 _lib.culs_rw.argtypes = [_vp, _vp, ctypes.c_uint32]
 _lib.culs_st.argtypes = [_vp, _vp, ctypes.c_uint32]
@@ -274,15 +275,17 @@ class DeviceGraphs:
         return dict(zip(["nPIs", "nPOs", "nAnds", "nLevels"], [x.value for x in v]))
 
     def download_all(self):
+        """Every graph of the handle as an Aig, in one transfer."""
         n = len(self)
-        arr = (_HostGraph * n)()
-        self.ctx._err(_lib.culs_batch_download(self.ctx.h, self.h, arr), "batch download")
-        out = []
-        for i in range(n):
-            a = _take(arr[i])
-            a.nLevels = self.stats(i)["nLevels"]
-            out.append(a)
-        return out
+        st = [self.stats(i) for i in range(n)]
+        f0 = [np.empty(1 + s["nPIs"] + s["nAnds"], np.int32) for s in st]
+        f1 = [np.empty(1 + s["nPIs"] + s["nAnds"], np.int32) for s in st]
+        po = [np.empty(max(s["nPOs"], 1), np.int32) for s in st]
+        P = ctypes.POINTER(ctypes.c_int32) * n
+        ptrs = [P(*[_p(a) for a in arrs]) for arrs in (f0, f1, po)]
+        self.ctx._err(_lib.culs_batch_download_into(self.ctx.h, self.h, *[ctypes.cast(x, ctypes.c_void_p) for x in ptrs]),
+                      "batch download")
+        return [Aig(s["nPIs"], f0[i], f1[i], po[i][:s["nPOs"]], s["nLevels"]) for i, s in enumerate(st)]
 
     def download(self, i=0) -> Aig:
         s = self.stats(i)

@@ -122,13 +122,8 @@ int culs_batch_download(culs_ctx *ctx, const culs_graph *g, culs_host_graph *out
     if (!ctx || !g || !outs) return CULS_E_INVALID;
     std::lock_guard<std::mutex> lk(ctx->mu);
     const culs::Batch &b = g->b;
-    std::vector<int32_t> f0(b.nObj), f1(b.nObj), po(b.nPO > 0 ? b.nPO : 1);
-    cudaStream_t s = ctx->eng.stream();
-    cudaMemcpyAsync(f0.data(), b.F0, sizeof(int32_t) * b.nObj, cudaMemcpyDeviceToHost, s);
-    cudaMemcpyAsync(f1.data(), b.F1, sizeof(int32_t) * b.nObj, cudaMemcpyDeviceToHost, s);
-    if (b.nPO) cudaMemcpyAsync(po.data(), b.PO, sizeof(int32_t) * b.nPO, cudaMemcpyDeviceToHost, s);
-    int rc = ctx->eng.sync();
-    if (rc != CULS_OK) return set_err(ctx, rc);
+    std::vector<int32_t *> f0(b.G), f1(b.G), po(b.G);
+    bool oom = false;
     for (int i = 0; i < b.G; i++) {
         const culs::DevGraph &d = b.hg[i];
         const size_t n = 1 + (size_t)d.nPIs + d.nAnds;
@@ -136,15 +131,20 @@ int culs_batch_download(culs_ctx *ctx, const culs_graph *g, culs_host_graph *out
         o.nPIs = d.nPIs;
         o.nPOs = d.nPOs;
         o.nAnds = d.nAnds;
-        o.fanin0 = (int32_t *)malloc(sizeof(int32_t) * n);
-        o.fanin1 = (int32_t *)malloc(sizeof(int32_t) * n);
-        o.outs = (int32_t *)malloc(sizeof(int32_t) * (d.nPOs > 0 ? d.nPOs : 1));
-        if (!o.fanin0 || !o.fanin1 || !o.outs) return CULS_E_OOM;
-        memcpy(o.fanin0, f0.data() + d.base, sizeof(int32_t) * n);
-        memcpy(o.fanin1, f1.data() + d.base, sizeof(int32_t) * n);
-        if (d.nPOs) memcpy(o.outs, po.data() + d.poOff, sizeof(int32_t) * d.nPOs);
+        o.fanin0 = f0[i] = (int32_t *)malloc(sizeof(int32_t) * n);
+        o.fanin1 = f1[i] = (int32_t *)malloc(sizeof(int32_t) * n);
+        o.outs = po[i] = (int32_t *)malloc(sizeof(int32_t) * (d.nPOs > 0 ? d.nPOs : 1));
+        oom |= !o.fanin0 || !o.fanin1 || !o.outs;
     }
-    return CULS_OK;
+    if (oom) return CULS_E_OOM;
+    return set_err(ctx, ctx->eng.download_all(b, f0.data(), f1.data(), po.data()));
+}
+
+int culs_batch_download_into(culs_ctx *ctx, const culs_graph *g, int32_t *const *fanin0, int32_t *const *fanin1,
+                             int32_t *const *outs) {
+    if (!ctx || !g) return CULS_E_INVALID;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    return set_err(ctx, ctx->eng.download_all(g->b, fanin0, fanin1, outs));
 }
 
 int culs_rw(culs_ctx *ctx, culs_graph *g, uint32_t flags) {

@@ -103,6 +103,9 @@ class Engine {
     int upload(Batch &b, int count, const int32_t *const *f0, const int32_t *const *f1, const int32_t *const *outs,
                const int32_t *nPIs, const int32_t *nPOs, const int32_t *nAnds);
     int download(const Batch &b, int g, int32_t *f0, int32_t *f1, int32_t *outs);
+    // Whole-batch download into caller arrays (graph i's fanins into f0[i],
+    // f1[i], its POs into outs[i]); a null array pointer skips that part.
+    int download_all(const Batch &b, int32_t *const *f0, int32_t *const *f1, int32_t *const *outs);
     int rw(Batch &b, bool useZeros, bool gpuDedup, RwStats *stats, RwDump *dump);
     int st(Batch &b, bool cpuOrder);
     int sync();
@@ -122,6 +125,7 @@ class Engine {
     int check(cudaError_t e, const char *what);
     int check_status(const char *what);
     int ensure_arena(size_t bytes);
+    int ensure_stage(size_t ints);  // pinned host staging of at least `ints` int32
     ExecCtx ctx();
 
     // stage helpers
@@ -139,6 +143,8 @@ class Engine {
     int *status_ = nullptr;     // device status word
     int *counters_ = nullptr;   // device scratch counters
     int *hostSmall_ = nullptr;  // pinned host scratch
+    int32_t *stage_ = nullptr;  // pinned staging for uploads and downloads
+    size_t stageCap_ = 0;       // in int32
     size_t budget_ = 0;
     Arena ar_;
     int launches_ = 0;

@@ -133,6 +133,7 @@ Engine::~Engine() {
     cudaFree(status_);
     cudaFree(counters_);
     if (hostSmall_) cudaFreeHost(hostSmall_);
+    if (stage_) cudaFreeHost(stage_);
     for (auto &e : ev_)
         if (e) cudaEventDestroy(e);
     if (s_) cudaStreamDestroy(s_);
@@ -239,62 +240,6 @@ int Engine::clone(const Batch &src, Batch &dst) {
     return check(cudaGetLastError(), "clone");
 }
 
-// ------------------------------------------------------------ upload
-int Engine::upload(Batch &b, int count, const int32_t *const *f0, const int32_t *const *f1,
-                   const int32_t *const *outs, const int32_t *nPIs, const int32_t *nPOs, const int32_t *nAnds) {
-    if (count < 1) return fail(CULS_E_INVALID, "upload: no graphs");
-    std::vector<DevGraph> hg(count);
-    int64_t nObj = 0, nPO = 0;
-    for (int g = 0; g < count; g++) {
-        if (nPIs[g] < 0 || nPOs[g] < 0 || nAnds[g] < 0) return fail(CULS_E_INVALID, "upload: negative size");
-        hg[g] = DevGraph{nPIs[g], nPOs[g], nAnds[g], 0, (int)nObj, (int)nPO, (int)nObj, 0};
-        nObj += 1 + (int64_t)nPIs[g] + nAnds[g];
-        nPO += nPOs[g];
-        if (nObj >= (1ll << 29)) return fail(CULS_E_INVALID, "upload: batch too large for 30-bit node positions");
-    }
-    // validate: fanins precede their node, literals in range
-    for (int g = 0; g < count; g++) {
-        const int n = 1 + nPIs[g] + nAnds[g];
-        for (int i = nPIs[g] + 1; i < n; i++) {
-            int a = f0[g][i], c = f1[g][i];
-            if (a < 0 || c < 0 || (a >> 1) >= i || (c >> 1) >= i)
-                return fail(CULS_E_INVALID, "upload: fanin literal out of range or not topological");
-        }
-        for (int k = 0; k < nPOs[g]; k++)
-            if (outs[g][k] < 0 || (outs[g][k] >> 1) >= n) return fail(CULS_E_INVALID, "upload: PO literal out of range");
-    }
-    // depth (AIGMan::readFromMemory's nLevels) on the host while staging
-    std::vector<int32_t> hF0(nObj), hF1(nObj), hPO(std::max<int64_t>(nPO, 1));
-    for (int g = 0; g < count; g++) {
-        const int n = 1 + nPIs[g] + nAnds[g];
-        int64_t base = hg[g].base;
-        std::vector<int> d(n, 0);
-        int mx = 0;
-        for (int i = 0; i < n; i++) {
-            if (i <= nPIs[g]) {
-                hF0[base + i] = hF1[base + i] = -1;
-                continue;
-            }
-            hF0[base + i] = f0[g][i];
-            hF1[base + i] = f1[g][i];
-            d[i] = 1 + std::max(d[f0[g][i] >> 1], d[f1[g][i] >> 1]);
-            mx = std::max(mx, d[i]);
-        }
-        hg[g].nLevels = mx;
-        if (nPOs[g]) memcpy(&hPO[hg[g].poOff], outs[g], sizeof(int32_t) * nPOs[g]);
-    }
-    int rc;
-    if ((rc = check(b.reserve(nObj, nPO, count), "cudaMalloc"))) return rc;
-    cudaMemcpyAsync(b.F0, hF0.data(), sizeof(int) * nObj, cudaMemcpyHostToDevice, s_);
-    cudaMemcpyAsync(b.F1, hF1.data(), sizeof(int) * nObj, cudaMemcpyHostToDevice, s_);
-    if (nPO) cudaMemcpyAsync(b.PO, hPO.data(), sizeof(int) * nPO, cudaMemcpyHostToDevice, s_);
-    cudaMemcpyAsync(b.dg, hg.data(), sizeof(DevGraph) * count, cudaMemcpyHostToDevice, s_);
-    b.G = count;
-    b.nObj = nObj;
-    b.nPO = nPO;
-    b.hg = hg;
-    return sync();
-}
 
 int Engine::download(const Batch &b, int g, int32_t *f0, int32_t *f1, int32_t *outs) {
     if (g < 0 || g >= b.G) return fail(CULS_E_INVALID, "download: graph index out of range");

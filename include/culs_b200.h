@@ -104,6 +104,14 @@ int culs_graph_download(culs_ctx *ctx, const culs_graph *g, int index, int32_t *
  * allocated by the library; free each with culs_host_graph_free). */
 int culs_batch_download(culs_ctx *ctx, const culs_graph *g, culs_host_graph *outs);
 
+/* The batch form of culs_graph_download (AIGMan::toHost for every graph of
+ * the handle at once): graph i's fanins go to fanin0[i] / fanin1[i] (1 +
+ * nPIs + nAnds entries each) and its POs to outs[i] (nPOs entries), arrays
+ * the caller owns; a null outer pointer or a null entry skips that part.
+ * One device-to-host transfer for the whole batch. */
+int culs_batch_download_into(culs_ctx *ctx, const culs_graph *g, int32_t *const *fanin0, int32_t *const *fanin1,
+                             int32_t *const *outs);
+
 /* `rw` on every graph of the handle: AIGMan::rewrite(fUseZeros,
  * fGPUDeduplicate) (CULS src/aig_manager.cu:632-672, command handler
  * src/command_manager.cpp:81-95). */

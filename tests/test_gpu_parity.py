@@ -180,6 +180,35 @@ def test_batch_of_generated_graphs_matches_oracle(ctx):
         assert same_graph(db.download(i), oracle_rw_st(g).graph()), i
 
 
+def _host_depth(g):
+    lev = np.zeros(g.nObjs, np.int64)
+    for v in range(g.nPIs + 1, g.nObjs):
+        lev[v] = 1 + max(lev[int(g.fanin0[v]) >> 1], lev[int(g.fanin1[v]) >> 1])
+    return int(lev.max()) if g.nObjs else 0
+
+
+def test_batch_transfers_agree(ctx):
+    """Upload computes every graph's depth on several host threads; the three
+    download paths (per graph, into caller arrays, library-allocated) return
+    the same arrays."""
+    gs = C.gen_batch(4, 100, 40, 1000, 60000, 16, 512, threads=8)
+    db = ctx.upload_batch(gs)
+    for i, g in enumerate(gs):
+        assert db.stats(i)["nLevels"] == _host_depth(g), i
+    ctx.rw_st(db)
+    whole = db.download_all()
+    arr = (C._HostGraph * len(db))()
+    assert C._lib.culs_batch_download(ctx.h, db.h, arr) == 0
+    for i in range(len(db)):
+        one = db.download(i)
+        lib = C._take(arr[i])
+        for got in (whole[i], lib):
+            np.testing.assert_array_equal(got.fanin0, one.fanin0)
+            np.testing.assert_array_equal(got.fanin1, one.fanin1)
+            np.testing.assert_array_equal(got.outs, one.outs)
+        assert whole[i].nLevels == one.nLevels
+
+
 def test_rewrite_preserves_function(ctx):
     for g in [GRAPHS["mult12"], GRAPHS["c1"], GRAPHS["unstrashed5"], C.gen_multiplier(32)]:
         out = gpu_run(ctx, g, FLOWS["rw;st"][0])
