@@ -355,9 +355,13 @@ CULS_HD TabRegion table_region(const RegionTable &t, int g) {
     return TabRegion{t.slots + a, (uint32_t)(b - a)};
 }
 
-// Home slot: the hash scaled onto [0, size) (multiply-high range reduction).
+// Home slot: a multiplicative hash of the key's two 32-bit halves (odd
+// constants from the golden ratio and MurmurHash3), its high bits scaled
+// onto [0, size) by a multiply-high.  Two 32-bit multiplies keep the probe
+// short; linear probing at load <= 1/2 tolerates its weaker mixing.
 CULS_HD uint32_t region_home(unsigned long long key, uint32_t size) {
-    return (uint32_t)(((unsigned long long)(uint32_t)mix64(key) * size) >> 32);
+    const uint32_t h = (uint32_t)(key >> 32) * 0x9E3779B1u + (uint32_t)key * 0x85EBCA6Bu;
+    return (uint32_t)(((unsigned long long)(h ^ (h >> 15)) * size) >> 32);
 }
 
 CULS_HD int region_insert(const TabRegion &t, unsigned long long key, int val, int lvl, int *status) {
