@@ -10,6 +10,10 @@ A step is one `rw; st` over the workload's graphs:
   c3  one 10M-AND layered AIG, 4,096 PIs/POs, 2,000 layers, 80% window-3 /
       20% far fanins
   c2  64x64 array multiplier; c1  5,000-AND 40-layer AIG (parity cases)
+  c5  served mode: Poisson arrivals (--load x measured capacity) of jobs
+      drawn from 64 c4-family graphs of 500-2M ANDs and 64 n x n
+      multipliers (n 8-128), submitted one by one through culs_submit;
+      reports throughput and p50/p99 submit-to-done latency
 `value` times device-resident steps (a device clone of the input, rw, st);
 `e2e` times the public C-ABI path from host arrays: upload, rw, st,
 download.  With --gpus N (under torchrun) every rank rewrites its own
@@ -50,6 +54,8 @@ def make_workload(name, rank):
     threads = os.cpu_count() or 8
     if name == "c4":
         return C.gen_batch(4, rank * 4096, 4096, 1000, 200000, 16, 512, threads=threads)
+    if name == "c5":  # the served workload's job pool
+        return served_pool()
     if name == "c4m":  # profiling case: the first 256 graphs of the c4 family
         return C.gen_batch(4, rank * 4096, 256, 1000, 200000, 16, 512, threads=threads)
     if name == "c3":
@@ -63,7 +69,7 @@ def make_workload(name, rank):
     raise SystemExit(f"unknown workload {name}")
 
 
-WORKLOAD_DESC = {"c4": "c4_batched_4096_layered_1k-200k", "c4m": "c4_family_batched_256_layered_1k-200k", "c3": "c3_single_10M_layered_2000",
+WORKLOAD_DESC = {"c5": "c5_served_poisson_500-2M_and_multipliers_8-128", "c4": "c4_batched_4096_layered_1k-200k", "c4m": "c4_family_batched_256_layered_1k-200k", "c3": "c3_single_10M_layered_2000",
                  "c3m": "c3_family_1M_layered_200", "c2": "c2_mult64x64", "c1": "c1_layered5k_40"}
 
 
@@ -191,6 +197,91 @@ def reference_arm(args, group):
     return 0
 
 
+def served_pool(seed=5, count=128):
+    """Job pool of the served workload: half seeded c4-family graphs with AND
+    counts log-uniform in 500-2M, half n x n array multipliers, n uniform in
+    8-128."""
+    import culs_b200 as C
+    rng = np.random.default_rng(seed)
+    pool = C.gen_batch(seed, 0, count // 2, 500, 2_000_000, 16, 512, threads=os.cpu_count() or 8)
+    pool += [C.gen_multiplier(int(n)) for n in rng.integers(8, 129, count - count // 2)]
+    return pool
+
+
+def served_arm(args, group):
+    """Served mode: jobs drawn from the pool arrive as a Poisson process at a
+    fraction of the measured batch capacity; each is submitted through the C
+    ABI (culs_submit), waited for and fetched on another thread.  Reports
+    throughput and submit-to-done latency percentiles (wall clock, the
+    latency a caller sees)."""
+    import threading
+    import culs_b200 as C
+    ctx = C.Context(device=group.local)
+    pool = served_pool()
+    rng = np.random.default_rng(5)
+    # capacity: one batch of the whole pool through the served path
+    ctx.serve_start()
+    t0 = time.perf_counter()
+    ids = [ctx.submit(g) for g in pool]
+    for j in ids:
+        ctx.wait(j)
+        ctx.fetch(j)
+    cap_jobs_s = len(pool) / (time.perf_counter() - t0)
+    njobs = max(args.steps, 1) * 400
+    rate = args.load * cap_jobs_s
+    picks = rng.integers(0, len(pool), njobs)
+    gaps = rng.exponential(1.0 / rate, njobs)
+    lat, nodes, done_t = [], 0, [0.0]
+    q = []
+    cv = threading.Condition()
+
+    def collector():
+        nonlocal nodes
+        for k in range(njobs):
+            with cv:
+                while len(q) <= k:
+                    cv.wait()
+                j = q[k]
+            ctx.wait(j)
+            out, ms = ctx.fetch(j)
+            lat.append(ms)
+            nodes += pool[picks[k]].nAnds
+        done_t[0] = time.perf_counter()
+
+    th = threading.Thread(target=collector)
+    th.start()
+    t0 = time.perf_counter()
+    due = t0
+    for k in range(njobs):
+        due += gaps[k]
+        d = due - time.perf_counter()
+        if d > 0:
+            time.sleep(d)
+        j = ctx.submit(pool[picks[k]])
+        with cv:
+            q.append(j)
+            cv.notify()
+    th.join()
+    ctx.serve_stop()
+    wall = done_t[0] - t0
+    lat = np.sort(np.array(lat))
+    line = {"metric": METRIC, "value": nodes / wall, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * wall / max(args.steps, 1), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+            "data": "synthetic (seeded generators; CULS ships no benchmark inputs)",
+            "config": {"workload": WORKLOAD_DESC["c5"], "jobs": njobs, "pool_graphs": len(pool),
+                       "offered_jobs_per_s": rate, "load_vs_capacity": args.load,
+                       "capacity_jobs_per_s": cap_jobs_s, "timing": "wall clock, submit to fetch",
+                       "parallelism": "single GPU, dynamic batching"},
+            "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                           "mean": float(lat.mean()), "max": float(lat[-1])},
+            "e2e": {"value": nodes / wall, "unit": UNIT,
+                    "h2d_bytes_per_step": None, "d2h_bytes_per_step": None},
+            "gpu_launches": ctx.kernel_launches()}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def our_arm(args, group):
     import culs_b200 as C
     ctx = C.Context(device=group.local)
@@ -277,14 +368,20 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--workload", default="c4", choices=["c4", "c4m", "c3", "c3m", "c2", "c1"])
+    ap.add_argument("--workload", default="c4", choices=["c4", "c4m", "c3", "c3m", "c2", "c1", "c5"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--load", type=float, default=0.75, help="c5: offered load as a fraction of measured capacity")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     group = Group()
     try:
-        rc = reference_arm(args, group) if args.impl == "reference" else our_arm(args, group)
+        if args.impl == "reference":
+            rc = reference_arm(args, group)
+        elif args.workload == "c5":
+            rc = served_arm(args, group) if group.rank == 0 else 0
+        else:
+            rc = our_arm(args, group)
     finally:
         group.close()
     return rc

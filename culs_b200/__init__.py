@@ -21,9 +21,12 @@ if not LIB_PATH.exists():
 _lib = ctypes.CDLL(str(LIB_PATH))
 
 CULS_OK = 0
+CULS_E_BUSY = -7
+CULS_E_NOTFOUND = -8
 ERRORS = {-1: "CULS_E_INVALID", -2: "CULS_E_OOM", -3: "CULS_E_BUDGET", -4: "CULS_E_PROBE", -5: "CULS_E_DEVICE",
           -6: "CULS_E_IO", -7: "CULS_E_BUSY", -8: "CULS_E_NOTFOUND"}
 RW_ZEROS, RW_GPU_DEDUP, RW_DUMP = 1, 2, 4
+SERVE_BYTES_PER_OBJ = 720  # device bytes the served mode's admission charges per object
 ST_CPU = 1
 STAT_NAMES = ["replaced", "replaced_pos", "replaced_zero", "reverted", "compromised", "pre_eval", "small_cut",
               "new_idx", "expected", "new_nodes", "candidates"]
@@ -59,6 +62,14 @@ _lib.culs_graph_count.argtypes = [_vp]
 _lib.culs_graph_stats.argtypes = [_vp, ctypes.c_int, _ip, _ip, _ip, _ip]
 _lib.culs_batch_download.argtypes = [_vp, _vp, ctypes.POINTER(_HostGraph)]
 _lib.culs_batch_download_into.argtypes = [_vp, _vp, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+_lib.culs_rw_st_batch.argtypes = [_vp, ctypes.c_void_p, ctypes.c_int, ctypes.c_uint32, ctypes.c_uint32]
+_lib.culs_serve_start.argtypes = [_vp, ctypes.c_size_t, ctypes.c_int]
+_lib.culs_serve_stop.argtypes = [_vp]
+_lib.culs_submit.argtypes = [_vp, _ip, _ip, _ip, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_uint32,
+                             ctypes.c_uint32, ctypes.POINTER(ctypes.c_int64)]
+_lib.culs_poll.argtypes = [_vp, ctypes.c_int64, _ip, _ip, _ip, _ip]
+_lib.culs_wait.argtypes = [_vp, ctypes.c_int64, ctypes.c_int]
+_lib.culs_fetch.argtypes = [_vp, ctypes.c_int64, _ip, _ip, _ip, ctypes.POINTER(ctypes.c_double)]
 _lib.culs_graph_download.argtypes = [_vp, _vp, ctypes.c_int, _ip, _ip, _ip]
 _lib.culs_rw.argtypes = [_vp, _vp, ctypes.c_uint32]
 _lib.culs_st.argtypes = [_vp, _vp, ctypes.c_uint32]
@@ -206,6 +217,56 @@ class Context:
     def rw_st(self, d, zeros=False, gpu_dedup=True, cpu_st=False):
         f = (RW_ZEROS if zeros else 0) | (RW_GPU_DEDUP if gpu_dedup else 0)
         self._err(_lib.culs_rw_st(self.h, d.h, f, ST_CPU if cpu_st else 0), "rw;st")
+
+    def rw_st_batch(self, handles, zeros=False, gpu_dedup=True, cpu_st=False):
+        """`rw; st` over several device handles in one pass."""
+        f = (RW_ZEROS if zeros else 0) | (RW_GPU_DEDUP if gpu_dedup else 0)
+        arr = (_vp * len(handles))(*[d.h for d in handles])
+        self._err(_lib.culs_rw_st_batch(self.h, ctypes.cast(arr, ctypes.c_void_p), len(handles), f,
+                                        ST_CPU if cpu_st else 0), "rw;st batch")
+
+    # ---- served mode
+    def serve_start(self, admit_bytes=0, max_batch=0):
+        self._err(_lib.culs_serve_start(self.h, admit_bytes, max_batch), "serve start")
+
+    def serve_stop(self):
+        self._err(_lib.culs_serve_stop(self.h), "serve stop")
+
+    def submit(self, g: Aig, zeros=False, gpu_dedup=True, cpu_st=False) -> int:
+        f = (RW_ZEROS if zeros else 0) | (RW_GPU_DEDUP if gpu_dedup else 0)
+        h = g.host()
+        job = ctypes.c_int64()
+        self._err(_lib.culs_submit(self.h, h.fanin0, h.fanin1, h.outs, h.nPIs, h.nPOs, h.nAnds, f,
+                                   ST_CPU if cpu_st else 0, ctypes.byref(job)), "submit")
+        return job.value
+
+    def poll(self, job):
+        """None while the job runs, else its result sizes."""
+        v = [ctypes.c_int32() for _ in range(4)]
+        rc = _lib.culs_poll(self.h, job, *[ctypes.byref(x) for x in v])
+        if rc == CULS_E_BUSY:
+            return None
+        self._err(rc, "poll")
+        return dict(zip(["nPIs", "nPOs", "nAnds", "nLevels"], [x.value for x in v]))
+
+    def wait(self, job, timeout_ms=-1):
+        rc = _lib.culs_wait(self.h, job, timeout_ms)
+        if rc == CULS_E_BUSY:
+            return False
+        self._err(rc, "wait")
+        return True
+
+    def fetch(self, job):
+        """The finished job's result and its submit-to-done latency in ms."""
+        st = self.poll(job)
+        if st is None:
+            raise CulsError(CULS_E_BUSY, "fetch: job still running")
+        n = 1 + st["nPIs"] + st["nAnds"]
+        f0, f1 = np.empty(n, np.int32), np.empty(n, np.int32)
+        outs = np.empty(max(st["nPOs"], 1), np.int32)
+        lat = ctypes.c_double()
+        self._err(_lib.culs_fetch(self.h, job, _p(f0), _p(f1), _p(outs), ctypes.byref(lat)), "fetch")
+        return Aig(st["nPIs"], f0, f1, outs[:st["nPOs"]], st["nLevels"]), lat.value
 
     def rw_stats(self):
         out = (ctypes.c_int64 * 11)()

@@ -1,11 +1,13 @@
 // C ABI (include/culs_b200.h) over the batch engine.
 #include <cstring>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <vector>
 
 #include "culs_b200.h"
 #include "engine.cuh"
+#include "serve.cuh"
 
 struct culs_ctx {
     culs::Engine eng;
@@ -13,6 +15,10 @@ struct culs_ctx {
     culs::RwStats last{};
     culs::RwDump dump;
     std::string err;
+    // served mode; its worker takes `mu` for every batch, so the pointer has
+    // a lock of its own, and callers hold a reference while they use it
+    std::mutex srvMu;
+    std::shared_ptr<culs::Server> srv;  // destroyed first: finishes queued jobs
 };
 
 struct culs_graph {
@@ -165,6 +171,88 @@ int culs_rw_st(culs_ctx *ctx, culs_graph *g, uint32_t rwFlags, uint32_t stFlags)
     int rc = culs_rw(ctx, g, rwFlags);
     if (rc != CULS_OK) return rc;
     return culs_st(ctx, g, stFlags);
+}
+
+int culs_rw_st_batch(culs_ctx *ctx, culs_graph *const *gs, int count, uint32_t rwFlags, uint32_t stFlags) {
+    if (!ctx || !gs || count < 1) return CULS_E_INVALID;
+    std::vector<const culs::Batch *> in;
+    std::vector<culs::Batch *> out;
+    for (int i = 0; i < count; i++) {
+        if (!gs[i]) return CULS_E_INVALID;
+        for (int k = 0; k < i; k++)
+            if (gs[k] == gs[i]) return CULS_E_INVALID;  // a handle listed twice
+        in.push_back(&gs[i]->b);
+        out.push_back(&gs[i]->b);
+    }
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    culs::Batch all;
+    int rc = ctx->eng.concat(in, all);
+    if (rc == CULS_OK)
+        rc = ctx->eng.rw(all, (rwFlags & CULS_RW_ZEROS) != 0, (rwFlags & CULS_RW_GPU_DEDUP) != 0, &ctx->last,
+                         nullptr);
+    if (rc == CULS_OK) rc = ctx->eng.st(all, (stFlags & CULS_ST_CPU) != 0);
+    if (rc == CULS_OK) rc = ctx->eng.split(all, out);
+    return set_err(ctx, rc);
+}
+
+namespace {
+std::shared_ptr<culs::Server> server_of(culs_ctx *ctx) {
+    std::lock_guard<std::mutex> lk(ctx->srvMu);
+    return ctx->srv;
+}
+}  // namespace
+
+int culs_serve_start(culs_ctx *ctx, size_t admitBytes, int maxBatch) {
+    if (!ctx) return CULS_E_INVALID;
+    std::lock_guard<std::mutex> lk(ctx->srvMu);
+    if (ctx->srv) return CULS_E_INVALID;
+    if (admitBytes == 0) admitBytes = ctx->eng.budget();
+    ctx->srv = std::make_shared<culs::Server>(ctx->eng, ctx->mu, admitBytes, maxBatch);
+    return CULS_OK;
+}
+
+int culs_serve_stop(culs_ctx *ctx) {
+    if (!ctx) return CULS_E_INVALID;
+    std::shared_ptr<culs::Server> s;
+    {
+        std::lock_guard<std::mutex> lk(ctx->srvMu);
+        s.swap(ctx->srv);
+    }
+    return s ? CULS_OK : CULS_E_INVALID;  // the last reference finishes the queue
+}
+
+int culs_submit(culs_ctx *ctx, const int32_t *fanin0, const int32_t *fanin1, const int32_t *outs, int32_t nPIs,
+                int32_t nPOs, int32_t nAnds, uint32_t rwFlags, uint32_t stFlags, int64_t *job) {
+    if (!ctx) return CULS_E_INVALID;
+    auto s = server_of(ctx);
+    if (!s) return CULS_E_INVALID;
+    return s->submit(fanin0, fanin1, outs, nPIs, nPOs, nAnds, rwFlags, stFlags, job);
+}
+
+int culs_poll(culs_ctx *ctx, int64_t job, int32_t *nPIs, int32_t *nPOs, int32_t *nAnds, int32_t *nLevels) {
+    if (!ctx) return CULS_E_INVALID;
+    auto s = server_of(ctx);
+    if (!s) return CULS_E_NOTFOUND;
+    return s->poll(job, nPIs, nPOs, nAnds, nLevels);
+}
+
+int culs_wait(culs_ctx *ctx, int64_t job, int timeoutMs) {
+    if (!ctx) return CULS_E_INVALID;
+    auto s = server_of(ctx);
+    if (!s) return CULS_E_NOTFOUND;
+    return s->wait(job, timeoutMs);
+}
+
+int culs_fetch(culs_ctx *ctx, int64_t job, int32_t *fanin0, int32_t *fanin1, int32_t *outs, double *latencyMs) {
+    if (!ctx) return CULS_E_INVALID;
+    auto s = server_of(ctx);
+    if (!s) return CULS_E_NOTFOUND;
+    int rc = s->fetch(job, fanin0, fanin1, outs, latencyMs);
+    if (rc < 0 && rc != CULS_E_BUSY && rc != CULS_E_NOTFOUND) {
+        std::lock_guard<std::mutex> lk(ctx->mu);
+        ctx->err = s->lastError();
+    }
+    return rc;
 }
 
 int culs_rw_stats(culs_ctx *ctx, int64_t *out, int n) {

@@ -118,6 +118,10 @@ class Engine {
     void mark(int m);
     float elapsed(int a, int b);  // ms between two recorded marks (-1 if missing)
     int clone(const Batch &src, Batch &dst);
+    // dst = the graphs of parts[0], parts[1], ... in order (device copies).
+    int concat(const std::vector<const Batch *> &parts, Batch &dst);
+    // Inverse of concat: parts[i] receives its graphs back from src.
+    int split(const Batch &src, const std::vector<Batch *> &parts);
     void resetLaunchCount() { launches_ = 0; }
 
   private:

@@ -159,3 +159,77 @@ int Engine::download_all(const Batch &b, int32_t *const *f0, int32_t *const *f1,
 }
 
 }  // namespace culs
+
+namespace culs {
+
+// Literals are graph-local, so joining batches moves arrays as they are and
+// only the graph table's bases and PO offsets shift.
+int Engine::concat(const std::vector<const Batch *> &parts, Batch &dst) {
+    int64_t nObj = 0, nPO = 0;
+    int G = 0;
+    for (const Batch *p : parts) {
+        nObj += p->nObj;
+        nPO += p->nPO;
+        G += p->G;
+    }
+    if (G < 1) return fail(CULS_E_INVALID, "concat: no graphs");
+    if (nObj >= (1ll << 29)) return fail(CULS_E_INVALID, "concat: batch too large for 30-bit node positions");
+    int rc;
+    if ((rc = check(dst.reserve(nObj, nPO, G), "cudaMalloc"))) return rc;
+    std::vector<DevGraph> hg;
+    hg.reserve(G);
+    int64_t o = 0, po = 0;
+    for (const Batch *p : parts) {
+        if (p->nObj) {
+            cudaMemcpyAsync(dst.F0 + o, p->F0, sizeof(int) * p->nObj, cudaMemcpyDeviceToDevice, s_);
+            cudaMemcpyAsync(dst.F1 + o, p->F1, sizeof(int) * p->nObj, cudaMemcpyDeviceToDevice, s_);
+        }
+        if (p->nPO) cudaMemcpyAsync(dst.PO + po, p->PO, sizeof(int) * p->nPO, cudaMemcpyDeviceToDevice, s_);
+        for (DevGraph d : p->hg) {
+            d.base += (int)o;
+            d.poOff += (int)po;
+            d.cpos = d.base;
+            hg.push_back(d);
+        }
+        o += p->nObj;
+        po += p->nPO;
+    }
+    cudaMemcpyAsync(dst.dg, hg.data(), sizeof(DevGraph) * G, cudaMemcpyHostToDevice, s_);
+    dst.G = G;
+    dst.nObj = nObj;
+    dst.nPO = nPO;
+    dst.hg = hg;
+    if ((rc = check(cudaGetLastError(), "concat"))) return rc;
+    return sync();  // hg's host copy feeds the table copy above
+}
+
+int Engine::split(const Batch &src, const std::vector<Batch *> &parts) {
+    int first = 0, rc;
+    for (Batch *p : parts) {
+        const int G = p->G;
+        if (first + G > src.G) return fail(CULS_E_INVALID, "split: graph counts do not add up");
+        const DevGraph &a = src.hg[first];
+        const DevGraph &z = src.hg[first + G - 1];
+        const int64_t objEnd = (int64_t)z.base + 1 + z.nPIs + z.nAnds;
+        const int64_t nObj = objEnd - a.base, nPO = (int64_t)z.poOff + z.nPOs - a.poOff;
+        if ((rc = check(p->reserve(nObj, nPO, G), "cudaMalloc"))) return rc;
+        cudaMemcpyAsync(p->F0, src.F0 + a.base, sizeof(int) * nObj, cudaMemcpyDeviceToDevice, s_);
+        cudaMemcpyAsync(p->F1, src.F1 + a.base, sizeof(int) * nObj, cudaMemcpyDeviceToDevice, s_);
+        if (nPO) cudaMemcpyAsync(p->PO, src.PO + a.poOff, sizeof(int) * nPO, cudaMemcpyDeviceToDevice, s_);
+        std::vector<DevGraph> hg(src.hg.begin() + first, src.hg.begin() + first + G);
+        for (DevGraph &d : hg) {
+            d.base -= a.base;
+            d.poOff -= a.poOff;
+            d.cpos = d.base;
+        }
+        cudaMemcpyAsync(p->dg, hg.data(), sizeof(DevGraph) * G, cudaMemcpyHostToDevice, s_);
+        p->nObj = nObj;
+        p->nPO = nPO;
+        p->hg = hg;
+        if ((rc = sync())) return rc;  // before hg goes out of scope
+        first += G;
+    }
+    return check(cudaGetLastError(), "split");
+}
+
+}  // namespace culs

@@ -1,0 +1,75 @@
+// Served mode: AIGs submitted one by one are rewritten in dynamic batches.
+//
+// The reference runs one AIG per process invocation.  A server takes jobs
+// (copied at submission, so the caller may free its arrays), and a worker
+// thread repeatedly takes the queued jobs in arrival order -- those with the
+// head job's flags, as long as their estimated device footprint stays within
+// the admission budget -- and runs them as one batch through the engine
+// (upload, rw, st, download) under the context's lock, so served jobs and
+// direct calls on the same context never overlap on the device.  Each job
+// records its submit-to-done latency.
+#pragma once
+
+#include <chrono>
+#include <condition_variable>
+#include <cstdint>
+#include <deque>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "engine.cuh"
+
+namespace culs {
+
+struct ServeJob {
+    int64_t id = 0;
+    uint32_t rwFlags = 0, stFlags = 0;  // CULS_RW_* / CULS_ST_*
+    int32_t nPIs = 0, nPOs = 0, nAnds = 0, nLevels = 0;
+    std::vector<int32_t> f0, f1, outs;  // the input, replaced by the result
+    int state = 0;                      // kQueued, kRunning, kDone, or a CULS_E_* code
+    std::chrono::steady_clock::time_point tSubmit, tDone;
+};
+
+class Server {
+  public:
+    static constexpr int kQueued = 1, kRunning = 2, kDone = 0;
+    // Device bytes the admission rule charges per object of a batch (arena
+    // of rw plus the graph arrays and their spares).
+    static constexpr size_t kBytesPerObj = 720;
+
+    Server(Engine &eng, std::mutex &engMu, size_t admitBytes, int maxBatch);
+    ~Server();  // finishes every queued job, then stops the worker
+
+    int submit(const int32_t *f0, const int32_t *f1, const int32_t *outs, int32_t nPIs, int32_t nPOs, int32_t nAnds,
+               uint32_t rwFlags, uint32_t stFlags, int64_t *id);
+    // CULS_OK with the result's sizes when done, CULS_E_BUSY while queued or
+    // running, CULS_E_NOTFOUND for an unknown id, or the job's error code.
+    int poll(int64_t id, int32_t *nPIs, int32_t *nPOs, int32_t *nAnds, int32_t *nLevels);
+    // Waits up to timeoutMs (< 0: without limit) for the job to finish.
+    int wait(int64_t id, int timeoutMs);
+    // Copies a finished job's result out and forgets the job.
+    int fetch(int64_t id, int32_t *f0, int32_t *f1, int32_t *outs, double *latencyMs);
+    const std::string &lastError() const { return err_; }
+
+  private:
+    void worker();
+    void run_batch(std::vector<ServeJob *> &batch);
+
+    Engine &eng_;
+    std::mutex &engMu_;
+    size_t admit_;
+    int maxBatch_;
+    std::mutex mu_;
+    std::condition_variable cvWork_, cvDone_;
+    std::deque<int64_t> queue_;
+    std::unordered_map<int64_t, std::unique_ptr<ServeJob>> jobs_;
+    int64_t nextId_ = 1;
+    bool stop_ = false;
+    std::string err_;
+    std::thread th_;
+};
+
+}  // namespace culs

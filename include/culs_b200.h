@@ -123,6 +123,39 @@ int culs_st(culs_ctx *ctx, culs_graph *g, uint32_t flags);
  * scripts), on one graph or a whole batch. */
 int culs_rw_st(culs_ctx *ctx, culs_graph *g, uint32_t rwFlags, uint32_t stFlags);
 
+/* `rw; st` over several handles at once (each may hold one graph or a
+ * batch): the handles are joined on the device, rewritten as one batch and
+ * split back, each handle receiving its own graphs' results.  The batch
+ * entry point of the served path; no counterpart in the reference, which
+ * rewrites one AIG per process. */
+int culs_rw_st_batch(culs_ctx *ctx, culs_graph *const *gs, int count, uint32_t rwFlags, uint32_t stFlags);
+
+/* ------------------------------------------------------------ served mode
+ * AIGs submitted one by one are rewritten (`rw; st`) in dynamic batches by a
+ * worker thread of the context: it takes queued jobs in arrival order (those
+ * with the first job's flags) while their estimated device footprint stays
+ * within admitBytes (0: the context's HBM budget) and maxBatch (<= 0: no
+ * limit), runs them as one batch, and holds every result until fetched.
+ * Jobs and direct calls on the same context never overlap on the device.
+ * No counterpart in the reference (one AIG per process invocation).
+ *
+ * culs_submit copies the graph (the caller may free its arrays) and returns
+ * a job id.  culs_poll returns CULS_OK with the result's sizes once the job
+ * is done, CULS_E_BUSY before, CULS_E_NOTFOUND for an unknown id, or the
+ * job's error code.  culs_wait blocks up to timeoutMs (< 0: no limit) and
+ * returns like culs_poll.  culs_fetch copies a finished result (fanin
+ * arrays of 1 + nPIs + nAnds entries, nPOs outputs), reports the
+ * submit-to-done latency in ms, and forgets the job.  culs_serve_stop
+ * finishes every queued job, then ends the worker; results not fetched by
+ * then are discarded.  Admission charges 720 device bytes per object. */
+int culs_serve_start(culs_ctx *ctx, size_t admitBytes, int maxBatch);
+int culs_serve_stop(culs_ctx *ctx);
+int culs_submit(culs_ctx *ctx, const int32_t *fanin0, const int32_t *fanin1, const int32_t *outs, int32_t nPIs,
+                int32_t nPOs, int32_t nAnds, uint32_t rwFlags, uint32_t stFlags, int64_t *job);
+int culs_poll(culs_ctx *ctx, int64_t job, int32_t *nPIs, int32_t *nPOs, int32_t *nAnds, int32_t *nLevels);
+int culs_wait(culs_ctx *ctx, int64_t job, int timeoutMs);
+int culs_fetch(culs_ctx *ctx, int64_t job, int32_t *fanin0, int32_t *fanin1, int32_t *outs, double *latencyMs);
+
 /* Counters of the last culs_rw (the summary CPUSolver::Rewrite prints,
  * src/algorithms/rewrite.cu:896-897,926): replaced, replaced with positive
  * gain, replaced with zero gain, reverted, compromised, without a cut, small

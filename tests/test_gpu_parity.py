@@ -209,6 +209,22 @@ def test_batch_transfers_agree(ctx):
         assert whole[i].nLevels == one.nLevels
 
 
+def test_cli_script_matches_library(ctx, tmp_path):
+    """gpuls -c "read; rw; st; ps; write" gives the oracle's rw;st result."""
+    import subprocess
+    exe = Path(__file__).resolve().parents[1] / "culs_b200" / "gpuls"
+    g = C.gen_layered(11, 48, 24, 6000, 40, 4, 0.0, True)
+    src, dst = tmp_path / "in.aig", tmp_path / "out.aig"
+    C.write_aiger(src, g)
+    r = subprocess.run([str(exe), "-c", f"read {src}; rw; st; ps; write {dst}"], capture_output=True, text=True,
+                       timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    out = C.read_aiger(dst)
+    ref = oracle_rw_st(g).graph()
+    assert same_graph(out, ref)
+    assert f"AIG stats: i/o = {g.nPIs}/{len(g.outs)} and = {ref.nAnds} level = {ref.nLevels}" in r.stdout
+
+
 def test_rewrite_preserves_function(ctx):
     for g in [GRAPHS["mult12"], GRAPHS["c1"], GRAPHS["unstrashed5"], C.gen_multiplier(32)]:
         out = gpu_run(ctx, g, FLOWS["rw;st"][0])

@@ -113,3 +113,24 @@ def test_context_fails_loudly_without_gpu():
     with pytest.raises(C.CulsError) as e:
         C.Context()
     assert e.value.code == -5
+
+
+def _gpuls():
+    exe = ROOT / "culs_b200" / "gpuls"
+    if not exe.exists():
+        pytest.skip("gpuls not built (python culs_b200/build.py)")
+    return exe
+
+
+def test_cli_command_surface_without_graph():
+    """The gpuls-compatible CLI parses the reference's script syntax and
+    answers the commands that need no device the way gpuls does."""
+    import subprocess
+    out = subprocess.run([str(_gpuls()), "-c", "ps; time; b; foo; rw -q; write x.txt"], capture_output=True,
+                         text=True, timeout=60).stdout.splitlines()
+    assert out[0] == 'Running in script mode: "ps; time; b; foo; rw -q; write x.txt".'
+    assert "AIG stats: i/o = 0/0 and = 0 level = 0" in out
+    assert any(l.startswith("{time} prev cmd: alg 0.00 s, full 0.00 s;") for l in out)
+    assert "Command foo not registered, ignored." in out
+    assert "Command rw not recognized or in wrong format!" in out
+    assert "write: only support .aig format!" in out

@@ -1,0 +1,79 @@
+"""Batch and served entry points (culs_rw_st_batch, culs_submit / culs_poll /
+culs_wait / culs_fetch): every result equals the oracle's `rw; st` of the
+same graph, exactly, whichever batch a graph or job ends up in."""
+import pytest
+
+import culs_b200 as C
+from util import oracle_rw_st, same_graph
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = C.Context()
+    yield c
+    c.close()
+
+
+def graphs():
+    return [C.gen_multiplier(8), C.gen_layered(21, 32, 16, 3000, 30, 4, 0.0, True), C.gen_multiplier(12),
+            C.gen_layered(22, 64, 32, 9000, 60, 3, 0.2, False), C.gen_layered(23, 16, 8, 700, 20, 4, 0.0, True)]
+
+
+def test_rw_st_batch_over_handles(ctx):
+    gs = graphs()
+    hs = [ctx.upload(gs[0]), ctx.upload_batch(gs[1:3]), ctx.upload(gs[3]), ctx.upload_batch(gs[4:])]
+    ctx.rw_st_batch(hs)
+    got = [hs[0].download()] + hs[1].download_all() + [hs[2].download()] + hs[3].download_all()
+    assert len(got) == len(gs)
+    for i, (a, g) in enumerate(zip(got, gs)):
+        ref = oracle_rw_st(g).graph()
+        assert same_graph(a, ref), i
+        assert a.nLevels == ref.nLevels, i
+
+
+def test_rw_st_batch_rejects_repeated_handle(ctx):
+    h = ctx.upload(C.gen_multiplier(6))
+    with pytest.raises(C.CulsError) as e:
+        ctx.rw_st_batch([h, h])
+    assert e.value.code == -1
+
+
+def test_served_jobs_match_oracle(ctx):
+    gs = graphs()
+    # a small admission budget and batch cap, so the jobs run as several batches
+    ctx.serve_start(admit_bytes=C.SERVE_BYTES_PER_OBJ * 12000, max_batch=3)
+    try:
+        jobs = [(ctx.submit(g, zeros=(i == 2)), g, i == 2) for i, g in enumerate(gs * 2)]
+        for job, g, zeros in jobs:
+            assert ctx.wait(job, 60000)
+            out, lat = ctx.fetch(job)
+            ref = oracle_rw_st(g, zeros=zeros).graph()
+            assert same_graph(out, ref), job
+            assert out.nLevels == ref.nLevels
+            assert lat >= 0.0
+            with pytest.raises(C.CulsError) as e:  # a fetched job is forgotten
+                ctx.poll(job)
+            assert e.value.code == C.CULS_E_NOTFOUND
+        with pytest.raises(C.CulsError) as e:
+            ctx.poll(10 ** 9)
+        assert e.value.code == C.CULS_E_NOTFOUND
+    finally:
+        ctx.serve_stop()
+
+
+def test_served_job_error_is_reported():
+    small = C.Context(hbm_budget=1 << 20)
+    small.serve_start()
+    try:
+        job = small.submit(C.gen_multiplier(16))
+        with pytest.raises(C.CulsError) as e:  # wait returns the job's outcome
+            small.wait(job, 60000)
+        assert e.value.code == -3  # CULS_E_BUDGET, carried to the job
+        with pytest.raises(C.CulsError) as e:
+            small.fetch(job)
+        assert e.value.code == -3
+    finally:
+        small.serve_stop()
+        small.close()
