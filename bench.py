@@ -197,6 +197,39 @@ def reference_arm(args, group):
     return 0
 
 
+def plain_path(ctx, graphs, budget_s=8.0, e2e=False):
+    """The plain single-graph path: the workload's graphs one at a time, each
+    its own handle (device-resident clone + rw;st, or with e2e the whole
+    upload + rw;st + download), for about budget_s seconds of graphs in
+    workload order.  Returns AND nodes per second and the sample."""
+    nodes, t_total, k = 0, 0.0, 0
+    t_end = time.perf_counter() + budget_s
+    while k < len(graphs) and time.perf_counter() < t_end:
+        g = graphs[k]
+        if e2e:
+            t0 = time.perf_counter()
+            d = ctx.upload(g)
+            ctx.rw_st(d)
+            d.download()
+            t_total += time.perf_counter() - t0
+        else:
+            d0 = ctx.upload(g)
+            d = ctx.clone(d0)
+            ctx.sync()
+            ctx.mark(0)
+            ctx.rw_st(d)
+            ctx.mark(1)
+            ctx.sync()
+            t_total += ctx.profile_read()["user"] / 1e3
+            d0.free()
+        d.free()
+        nodes += g.nAnds
+        k += 1
+    return {"value": nodes / t_total if t_total > 0 else None, "unit": UNIT,
+            "sample": f"first {k} graphs one at a time ({nodes} AND nodes)" +
+                      (", upload + rw;st + download, wall clock" if e2e else ", device-resident, CUDA events")}
+
+
 def served_pool(seed=5, count=128):
     """Job pool of the served workload: half seeded c4-family graphs with AND
     counts log-uniform in 500-2M, half n x n array multipliers, n uniform in
@@ -264,6 +297,7 @@ def served_arm(args, group):
     th.join()
     ctx.serve_stop()
     wall = done_t[0] - t0
+    plain = plain_path(ctx, [pool[i] for i in picks], budget_s=8.0, e2e=True)
     lat = np.sort(np.array(lat))
     line = {"metric": METRIC, "value": nodes / wall, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * wall / max(args.steps, 1), "higher_is_better": True,
@@ -275,6 +309,8 @@ def served_arm(args, group):
                        "parallelism": "single GPU, dynamic batching"},
             "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                            "mean": float(lat.mean()), "max": float(lat[-1])},
+            "plain_single_graph_path": plain,
+            "served_vs_plain": (nodes / wall) / plain["value"] if plain["value"] else None,
             "e2e": {"value": nodes / wall, "unit": UNIT,
                     "h2d_bytes_per_step": None, "d2h_bytes_per_step": None},
             "gpu_launches": ctx.kernel_launches()}
@@ -355,6 +391,10 @@ def our_arm(args, group):
             "clocks": clk.summary(), "gpu_launches": launches,
             "stages_ms_last_step": {k: round(v, 3) for k, v in prof.items() if k not in ("user",)}}
     if group.rank == 0:
+        if group.world == 1 and len(graphs) > 1:
+            plain = plain_path(ctx, graphs)
+            line["plain_single_graph_path"] = plain
+            line["batched_vs_plain"] = value / plain["value"] if plain["value"] else None
         line["cpu_baseline"] = cpu_baseline(args.workload, graphs) if group.world == 1 else None
         print(json.dumps(line), flush=True)
     dw.free()

@@ -18,9 +18,17 @@ namespace culs {
 namespace {
 
 constexpr int kEnumBlock = 128;
+// Levels with at least this many AND nodes run one node per thread, narrower
+// ones one node per warp.
+constexpr int kEnumWideMin = 16384;
 
 struct EnumArgs {
     int64_t nL0, N;
+    const int *lvlCnt;      // AND nodes per level (level 0: none)
+    const int *lvlStart;    // first W position of each level
+    const int *chunkStart;  // first chunk of each level; maxLevel + 2 entries
+    int maxLevel;
+    int wideMin;            // levels at least this wide run thread-per-node
     const int *w0, *w1;
     const int *ref;
     const uint8_t *lidLow;
@@ -112,136 +120,386 @@ __device__ __forceinline__ void load_rcut(const EnumArgs &A, int64_t idx, int2 m
     rc_unpack_aux((uint32_t)x.x, (uint32_t)x.y, c);
 }
 
-// Warps claim 32 consecutive positions at a time.  A lane publishes its node
-// before it next waits on its warp, and fanins lie at lower positions, so a
-// lane never waits on a warp-mate that waits on it.
-__global__ void __launch_bounds__(kEnumBlock, 4) k_enumerate(EnumArgs A) {
-    const int lane = threadIdx.x & 31;
-    while (true) {
-        int chunk = 0;
-        if (lane == 0) chunk = atomicAdd(A.counter, 1);
-        chunk = __shfl_sync(0xffffffffu, chunk, 0);
-        const int64_t start = A.nL0 + (int64_t)chunk * 32;
-        if (start >= A.N) break;
-        const int64_t q = start + lane;
-        if (q >= A.N) continue;
-        Slot S[8];
-#pragma unroll
-        for (int k = 0; k < 8; k++) {
-            S[k].pk = 0;
-            S[k].sign = 0;
-            S[k].l[0] = S[k].l[1] = S[k].l[2] = S[k].l[3] = 0;
+// ------------------------------------------------- warp-per-node variant
+// One candidate of a node's enumeration: the pair's merged cut (the first
+// CutFilter sees it) and its final form after the truth table and
+// MinimizeCutSupport, with value and aux.
+struct Cand {
+    int x0, x1, x2, x3;  // merged leaves
+    uint32_t xs, xn;     // merged signature, leaf count
+    int y0, y1, y2, y3;  // final leaves
+    uint32_t ys, yn, ytt, yval, a0, a1;
+    uint32_t ok, mini;   // merge succeeded; minimisation removed leaves
+};
+
+__device__ __forceinline__ void make_cand(const RCut &a, const RCut &b, int c0, int c1, Cand &c) {
+    RCut m;
+    c.ok = rc_merge(a, b, m) ? 1u : 0u;
+    c.x0 = m.l[0];
+    c.x1 = m.l[1];
+    c.x2 = m.l[2];
+    c.x3 = m.l[3];
+    c.xs = m.sign;
+    c.xn = m.n;
+    m.tt = rc_truth(m, a, b, c0, c1);
+    c.mini = rc_minimize(m) ? 1u : 0u;
+    c.y0 = m.l[0];
+    c.y1 = m.l[1];
+    c.y2 = m.l[2];
+    c.y3 = m.l[3];
+    c.ys = m.sign;
+    c.yn = m.n;
+    c.ytt = m.tt;
+    c.yval = rc_value(m);
+    rc_pack_aux(m, c.a0, c.a1);
+}
+
+// Candidate `hi ? c1 : c0` of lane src, broadcast to the warp.
+__device__ __forceinline__ void fetch_cand(const Cand &c0, const Cand &c1, bool hi, int src, Cand &o) {
+    const unsigned F = 0xffffffffu;
+#define CULS_PICK(f) o.f = __shfl_sync(F, hi ? c1.f : c0.f, src)
+    CULS_PICK(x0);
+    CULS_PICK(x1);
+    CULS_PICK(x2);
+    CULS_PICK(x3);
+    CULS_PICK(xs);
+    CULS_PICK(xn);
+    CULS_PICK(y0);
+    CULS_PICK(y1);
+    CULS_PICK(y2);
+    CULS_PICK(y3);
+    CULS_PICK(ys);
+    CULS_PICK(yn);
+    CULS_PICK(ytt);
+    CULS_PICK(yval);
+    CULS_PICK(a0);
+    CULS_PICK(a1);
+    CULS_PICK(ok);
+    CULS_PICK(mini);
+#undef CULS_PICK
+}
+
+// CutFilter (rewrite.cu:178-193) with slot k on lane k (k < 8): visiting the
+// slots in index order, a larger slot containing X is dropped and the first
+// slot contained in X drops X and ends the visit.  So every slot lane tests
+// its own slot, one ballot finds the first containing slot, and only the
+// supersets before it are dropped.  Returns true when X is dropped.
+__device__ __forceinline__ bool warp_filter(int lane, int id, const int (&sl)[4], uint32_t ssign, uint32_t &spk,
+                                            const int (&xl)[4], uint32_t xn, uint32_t xs) {
+    bool clr = false, inX = false;
+    if (lane < 8 && lane != id && packed_used(spk)) {
+        const uint32_t kn = packed_nleaves(spk);
+        if (kn > xn)
+            clr = (ssign & xs) == xs && leaves_subset(xl, xn, sl, kn);
+        else
+            inX = (ssign & xs) == ssign && leaves_subset(sl, kn, xl, xn);
+    }
+    const unsigned C = __ballot_sync(0xffffffffu, clr), D = __ballot_sync(0xffffffffu, inX);
+    const unsigned drop = D ? (C & ((1u << (__ffs(D) - 1)) - 1u)) : C;
+    if ((drop >> lane) & 1u) spk &= ~(1u << 30);
+    return D != 0;
+}
+
+// Fanin slot `lane` of the warp's node, read from the lane holding it.
+__device__ __forceinline__ void fetch_slot(int src, int4 L, int2 M, int2 X, RCut &c, uint32_t &used) {
+    const unsigned F = 0xffffffffu;
+    c.l[0] = __shfl_sync(F, L.x, src);
+    c.l[1] = __shfl_sync(F, L.y, src);
+    c.l[2] = __shfl_sync(F, L.z, src);
+    c.l[3] = __shfl_sync(F, L.w, src);
+    const uint32_t sign = (uint32_t)__shfl_sync(F, M.x, src), pk = (uint32_t)__shfl_sync(F, M.y, src);
+    const uint32_t x0 = (uint32_t)__shfl_sync(F, X.x, src), x1 = (uint32_t)__shfl_sync(F, X.y, src);
+    c.sign = sign;
+    c.tt = pk & 0xFFFFu;
+    c.n = packed_nleaves(pk);
+    c.used = 1;
+    used = packed_used(pk);
+    rc_unpack_aux(x0, x1, c);
+}
+
+// A warp enumerates one node at a time: lanes 0-7 hold u0's cut slots and
+// lanes 8-15 u1's; every lane builds the candidates of pairs lane and
+// lane + 32 (pair bit i * 8 + j, the reference's i-major order); then the
+// warp replays CutEnumerate's slot policy over the admissible pairs in order
+// with the node's 8 slots on lanes 0-7 -- FindCut is a min over those lanes,
+// CutFilter two ballots -- and lanes 0-7 write the slots.  Same results as
+// the per-thread replay, with a node's latency cut to its sequential core.
+__device__ __forceinline__ void enum_node_warp(const EnumArgs &A, int64_t q, int lane) {
+    const unsigned F = 0xffffffffu;
+    const int f0 = A.w0[q], f1 = A.w1[q];
+    const int u0 = f0 >> 1, u1 = f1 >> 1, c0 = f0 & 1, c1 = f1 & 1;
+    int ok = 1;
+    if (lane == 0) ok = wait_ge(&A.done[u0], 1, A.status) && wait_ge(&A.done[u1], 1, A.status);
+    ok = __shfl_sync(F, ok, 0);
+    __syncwarp();
+    // the node's slots: slot 0 the trivial cut
+    int sl[4] = {0, 0, 0, 0};
+    uint32_t ssign = 0, spk = 0, sa0 = 0, sa1 = 0;
+    if (lane == 0) {
+        Cut c;
+        c.sign = 1u << A.lidLow[q];
+        c.tt = 0xAAAAu;
+        c.nLeaves = 1;
+        c.used = 1;
+        c.value = 1001u;
+        sl[0] = (int)q;
+        ssign = c.sign;
+        spk = cut_pack(c);
+        sa0 = clamp_ref(A.ref[q]);
+        sa1 = (uint32_t)A.lidLow[q] << 12;
+    }
+    if (ok) {
+        int4 L = make_int4(0, 0, 0, 0);
+        int2 M = make_int2(0, 0), X = make_int2(0, 0);
+        if (lane < 16) {
+            const int64_t idx = (int64_t)(lane < 8 ? u0 : u1) * 8 + (lane & 7);
+            L = __ldcg(&A.cutL[idx]);
+            M = __ldcg(&A.cutM[idx]);
+            X = __ldcg(&A.cutA[idx]);
         }
-        {
-            Cut c;
-            c.sign = 1u << A.lidLow[q];
-            c.tt = 0xAAAAu;
-            c.nLeaves = 1;
-            c.used = 1;
-            c.value = 1001u;
-            S[0].l[0] = (int)q;
-            S[0].sign = c.sign;
-            S[0].pk = cut_pack(c);
-            A.cutA[q * 8] = make_int2((int)clamp_ref(A.ref[q]), (int)((uint32_t)A.lidLow[q] << 12));
-        }
-        const int f0 = A.w0[q], f1 = A.w1[q];
-        const int u0 = f0 >> 1, u1 = f1 >> 1, c0 = f0 & 1, c1 = f1 & 1;
-        bool ok = wait_ge(&A.done[u0], 1, A.status) && wait_ge(&A.done[u1], 1, A.status);
-        if (ok) {
-            const int2 *M0 = A.cutM + (int64_t)u0 * 8, *M1 = A.cutM + (int64_t)u1 * 8;
-            // the pairs CutEnumerate tries (both slots used, at most 4 leaves
-            // by signature), bit i * 8 + j: visiting the set bits in order is
-            // the reference's i-major loop, and every lane takes its k-th pair
-            // in the same iteration
-            uint64_t pairs = 0;
-            {
-                uint32_t s1[8], used1 = 0;
-#pragma unroll
-                for (int j = 0; j < 8; j++) {
-                    const int2 mj = M1[j];
-                    s1[j] = (uint32_t)mj.x;
-                    used1 |= packed_used((uint32_t)mj.y) << j;
+        // candidates of pairs lane (i = lane / 8) and lane + 32
+        RCut a, b;
+        uint32_t ua, ub;
+        Cand k0, k1;
+        fetch_slot(lane >> 3, L, M, X, a, ua);
+        fetch_slot(8 + (lane & 7), L, M, X, b, ub);
+        const bool adm0 = ua && ub && popc32(a.sign | b.sign) <= 4;
+        if (adm0) make_cand(a, b, c0, c1, k0);
+        fetch_slot(4 + (lane >> 3), L, M, X, a, ua);
+        const bool adm1 = ua && ub && popc32(a.sign | b.sign) <= 4;
+        if (adm1) make_cand(a, b, c0, c1, k1);
+        uint64_t pairs = (uint64_t)__ballot_sync(F, adm0) | ((uint64_t)__ballot_sync(F, adm1) << 32);
+        while (pairs) {
+            const int p = __ffsll((long long)pairs) - 1;
+            pairs &= pairs - 1;
+            Cand m;
+            fetch_cand(k0, k1, p >= 32, p & 31, m);
+            // FindCut (rewrite.cu:84-109)
+            const unsigned freeSlots = __ballot_sync(F, lane < 8 && !packed_used(spk)) & 0xFFu;
+            int id;
+            if (freeSlots) {
+                id = __ffs(freeSlots) - 1;
+            } else {
+                uint32_t key = 0xFFFFFFFFu;
+                if (lane < 8) {
+                    const uint32_t n = packed_nleaves(spk);
+                    const uint32_t cls = n > 2 ? 0u : (n == 2 ? 1u : 2u);
+                    key = (cls << 20) | (((spk >> 16) & 0x7FFu) << 3) | (uint32_t)lane;
                 }
 #pragma unroll
-                for (int i = 0; i < 8; i++) {
-                    const int2 mi = M0[i];
-                    if (!packed_used((uint32_t)mi.y)) continue;
-#pragma unroll
-                    for (int j = 0; j < 8; j++)
-                        if (((used1 >> j) & 1u) && popc32((uint32_t)mi.x | s1[j]) <= 4)
-                            pairs |= 1ull << (i * 8 + j);
+                for (int o = 4; o; o >>= 1) {
+                    const uint32_t y = __shfl_xor_sync(F, key, o);
+                    key = y < key ? y : key;
                 }
+                id = (int)(__shfl_sync(F, key, 0) & 7u);
             }
-            while (pairs) {
-                const int p = __ffsll((long long)pairs) - 1;
-                pairs &= pairs - 1;
-                const int i = p >> 3, j = p & 7;
-                {
-                    RCut a, b;
-                    load_rcut(A, (int64_t)u0 * 8 + i, M0[i], a);
-                    load_rcut(A, (int64_t)u1 * 8 + j, M1[j], b);
-                    // FindCut: first unused slot, else lowest value among
-                    // >2-leaf, then 2-leaf, then smaller cuts (rewrite.cu:84-109)
-                    int id = -1;
-#pragma unroll
-                    for (int k = 0; k < 8; k++)
-                        if (id < 0 && !sl_used(S[k])) id = k;
-                    if (id < 0) {
-                        uint32_t best = 0xFFFFFFFFu;
-#pragma unroll
-                        for (int k = 0; k < 8; k++) {
-                            uint32_t n = sl_n(S[k]);
-                            uint32_t cls = n > 2 ? 0u : (n == 2 ? 1u : 2u);
-                            uint32_t key = (cls << 20) | (sl_value(S[k]) << 3) | (uint32_t)k;
-                            best = key < best ? key : best;
-                        }
-                        id = (int)(best & 7u);
-                    }
-#pragma unroll
-                    for (int k = 0; k < 8; k++)
-                        if (k == id) sl_clear_used(S[k]);
-                    RCut m;
-                    if (!rc_merge(a, b, m)) continue;
-                    if (filter_slots(S, id, m.l, m.n, m.sign)) continue;  // dropped: slot stays free
-                    m.tt = rc_truth(m, a, b, c0, c1);
-                    const bool mini = rc_minimize(m);
-                    m.value = 0;
-                    Cut pc;
-                    pc.tt = m.tt;
-                    pc.nLeaves = m.n;
-                    pc.used = 1;
-                    pc.value = 0;
-                    uint32_t a0, a1;
-                    rc_pack_aux(m, a0, a1);
-                    A.cutA[q * 8 + id] = make_int2((int)a0, (int)a1);
-#pragma unroll
-                    for (int k = 0; k < 8; k++)
-                        if (k == id) {
-                            S[k].l[0] = m.l[0];
-                            S[k].l[1] = m.l[1];
-                            S[k].l[2] = m.l[2];
-                            S[k].l[3] = m.l[3];
-                            S[k].sign = m.sign;
-                            S[k].pk = cut_pack(pc);
-                        }
-                    bool keep = true;
-                    if (mini) keep = !filter_slots(S, id, m.l, m.n, m.sign);
-                    pc.value = rc_value(m);
-                    pc.used = keep ? 1u : 0u;
-#pragma unroll
-                    for (int k = 0; k < 8; k++)
-                        if (k == id) S[k].pk = cut_pack(pc);
-                    if (m.n < 2) pairs = 0;  // enumeration of this node stops (rewrite.cu:291)
-                }
+            if (lane == id) spk &= ~(1u << 30);
+            if (!m.ok) continue;
+            const int xl[4] = {m.x0, m.x1, m.x2, m.x3};
+            if (warp_filter(lane, id, sl, ssign, spk, xl, m.xn, m.xs)) continue;  // slot stays free
+            Cut pc;
+            pc.tt = m.ytt;
+            pc.nLeaves = m.yn;
+            pc.used = 1;
+            pc.value = 0;
+            if (lane == id) {
+                sl[0] = m.y0;
+                sl[1] = m.y1;
+                sl[2] = m.y2;
+                sl[3] = m.y3;
+                ssign = m.ys;
+                spk = cut_pack(pc);
+                sa0 = m.a0;
+                sa1 = m.a1;
             }
+            bool keep = true;
+            if (m.mini) {
+                const int yl[4] = {m.y0, m.y1, m.y2, m.y3};
+                keep = !warp_filter(lane, id, sl, ssign, spk, yl, m.yn, m.ys);
+            }
+            pc.value = m.yval;
+            pc.used = keep ? 1u : 0u;
+            if (lane == id) spk = cut_pack(pc);
+            if (m.yn < 2) break;  // enumeration of this node stops (rewrite.cu:291)
         }
-#pragma unroll
-        for (int k = 0; k < 8; k++) {
-            A.cutL[q * 8 + k] = make_int4(S[k].l[0], S[k].l[1], S[k].l[2], S[k].l[3]);
-            A.cutM[q * 8 + k] = make_int2((int)S[k].sign, (int)S[k].pk);
-        }
+    }
+    if (lane < 8) {
+        A.cutL[q * 8 + lane] = make_int4(sl[0], sl[1], sl[2], sl[3]);
+        A.cutM[q * 8 + lane] = make_int2((int)ssign, (int)spk);
+        A.cutA[q * 8 + lane] = make_int2((int)sa0, (int)sa1);
         __threadfence();
-        st_release(&A.done[q], 1);
+    }
+    __syncwarp();
+    if (lane == 0) st_release(&A.done[q], 1);
+}
+
+// One node on one thread (wide levels): the slots in registers, the
+// admissible pairs visited in order.
+__device__ __forceinline__ void enum_node_thread(const EnumArgs &A, int64_t q) {
+    Slot S[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        S[k].pk = 0;
+        S[k].sign = 0;
+        S[k].l[0] = S[k].l[1] = S[k].l[2] = S[k].l[3] = 0;
+    }
+    {
+        Cut c;
+        c.sign = 1u << A.lidLow[q];
+        c.tt = 0xAAAAu;
+        c.nLeaves = 1;
+        c.used = 1;
+        c.value = 1001u;
+        S[0].l[0] = (int)q;
+        S[0].sign = c.sign;
+        S[0].pk = cut_pack(c);
+        A.cutA[q * 8] = make_int2((int)clamp_ref(A.ref[q]), (int)((uint32_t)A.lidLow[q] << 12));
+    }
+    const int f0 = A.w0[q], f1 = A.w1[q];
+    const int u0 = f0 >> 1, u1 = f1 >> 1, c0 = f0 & 1, c1 = f1 & 1;
+    bool ok = wait_ge(&A.done[u0], 1, A.status) && wait_ge(&A.done[u1], 1, A.status);
+    if (ok) {
+        const int2 *M0 = A.cutM + (int64_t)u0 * 8, *M1 = A.cutM + (int64_t)u1 * 8;
+        // the pairs CutEnumerate tries (both slots used, at most 4 leaves
+        // by signature), bit i * 8 + j: visiting the set bits in order is
+        // the reference's i-major loop, and every lane takes its k-th pair
+        // in the same iteration
+        uint64_t pairs = 0;
+        {
+            uint32_t s1[8], used1 = 0;
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+                const int2 mj = M1[j];
+                s1[j] = (uint32_t)mj.x;
+                used1 |= packed_used((uint32_t)mj.y) << j;
+            }
+#pragma unroll
+            for (int i = 0; i < 8; i++) {
+                const int2 mi = M0[i];
+                if (!packed_used((uint32_t)mi.y)) continue;
+#pragma unroll
+                for (int j = 0; j < 8; j++)
+                    if (((used1 >> j) & 1u) && popc32((uint32_t)mi.x | s1[j]) <= 4)
+                        pairs |= 1ull << (i * 8 + j);
+            }
+        }
+        while (pairs) {
+            const int p = __ffsll((long long)pairs) - 1;
+            pairs &= pairs - 1;
+            const int i = p >> 3, j = p & 7;
+            {
+                RCut a, b;
+                load_rcut(A, (int64_t)u0 * 8 + i, M0[i], a);
+                load_rcut(A, (int64_t)u1 * 8 + j, M1[j], b);
+                // FindCut: first unused slot, else lowest value among
+                // >2-leaf, then 2-leaf, then smaller cuts (rewrite.cu:84-109)
+                int id = -1;
+#pragma unroll
+                for (int k = 0; k < 8; k++)
+                    if (id < 0 && !sl_used(S[k])) id = k;
+                if (id < 0) {
+                    uint32_t best = 0xFFFFFFFFu;
+#pragma unroll
+                    for (int k = 0; k < 8; k++) {
+                        uint32_t n = sl_n(S[k]);
+                        uint32_t cls = n > 2 ? 0u : (n == 2 ? 1u : 2u);
+                        uint32_t key = (cls << 20) | (sl_value(S[k]) << 3) | (uint32_t)k;
+                        best = key < best ? key : best;
+                    }
+                    id = (int)(best & 7u);
+                }
+#pragma unroll
+                for (int k = 0; k < 8; k++)
+                    if (k == id) sl_clear_used(S[k]);
+                RCut m;
+                if (!rc_merge(a, b, m)) continue;
+                if (filter_slots(S, id, m.l, m.n, m.sign)) continue;  // dropped: slot stays free
+                m.tt = rc_truth(m, a, b, c0, c1);
+                const bool mini = rc_minimize(m);
+                m.value = 0;
+                Cut pc;
+                pc.tt = m.tt;
+                pc.nLeaves = m.n;
+                pc.used = 1;
+                pc.value = 0;
+                uint32_t a0, a1;
+                rc_pack_aux(m, a0, a1);
+                A.cutA[q * 8 + id] = make_int2((int)a0, (int)a1);
+#pragma unroll
+                for (int k = 0; k < 8; k++)
+                    if (k == id) {
+                        S[k].l[0] = m.l[0];
+                        S[k].l[1] = m.l[1];
+                        S[k].l[2] = m.l[2];
+                        S[k].l[3] = m.l[3];
+                        S[k].sign = m.sign;
+                        S[k].pk = cut_pack(pc);
+                    }
+                bool keep = true;
+                if (mini) keep = !filter_slots(S, id, m.l, m.n, m.sign);
+                pc.value = rc_value(m);
+                pc.used = keep ? 1u : 0u;
+#pragma unroll
+                for (int k = 0; k < 8; k++)
+                    if (k == id) S[k].pk = cut_pack(pc);
+                if (m.n < 2) pairs = 0;  // enumeration of this node stops (rewrite.cu:291)
+            }
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        A.cutL[q * 8 + k] = make_int4(S[k].l[0], S[k].l[1], S[k].l[2], S[k].l[3]);
+        A.cutM[q * 8 + k] = make_int2((int)S[k].sign, (int)S[k].pk);
+    }
+    __threadfence();
+    st_release(&A.done[q], 1);
+}
+
+// Levels are cut into chunks that never cross a level: a wide level into
+// 32-node chunks, each node on one thread (throughput), a narrow level into
+// one-node chunks, each node on a whole warp (latency: a narrow level's
+// time is the time of its slowest node).  Warps claim chunks in level
+// order, so every fanin of a claimed node lies in an earlier, claimed chunk.
+__global__ void __launch_bounds__(kEnumBlock, 3) k_enumerate(EnumArgs A) {
+    const unsigned F = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int total = A.chunkStart[A.maxLevel + 1];
+    while (true) {
+        int c = 0;
+        if (lane == 0) c = atomicAdd(A.counter, 1);
+        c = __shfl_sync(F, c, 0);
+        if (c >= total) break;
+        int lo = 1, hi = A.maxLevel;
+        while (lo < hi) {  // last level whose first chunk is <= c
+            const int mid = (lo + hi + 1) >> 1;
+            if (A.chunkStart[mid] <= c)
+                lo = mid;
+            else
+                hi = mid - 1;
+        }
+        const int w = A.lvlCnt[lo];
+        const int64_t base = A.nL0 + A.lvlStart[lo];
+        const int64_t k = c - A.chunkStart[lo];
+        if (w >= A.wideMin) {
+            const int64_t q = base + k * 32 + lane;
+            if (q < base + w) enum_node_thread(A, q);
+        } else {
+            enum_node_warp(A, base + k, lane);
+        }
+    }
+}
+
+__global__ void k_level_count(int64_t nL0, int64_t N, const int *wlev, int *lvlCnt) {
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t q = nL0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < N; q += stride)
+        agg_add(lvlCnt, wlev[q], 1);
+}
+
+__global__ void k_level_chunks(int n, const int *lvlCnt, int wideMin, int *cc) {
+    int stride = gridDim.x * blockDim.x;
+    for (int l = blockIdx.x * blockDim.x + threadIdx.x; l < n; l += stride) {
+        const int w = lvlCnt[l];
+        cc[l] = w >= wideMin ? (w + 31) / 32 : w;
     }
 }
 
@@ -258,12 +516,24 @@ int rw_enumerate(ExecCtx &X, RwWork &w) {
     int rc;
     if ((rc = X.check(cudaMemsetAsync(w.cutM, 0, sizeof(int2) * N * 8, s), "memset"))) return rc;
     if ((rc = X.check(cudaMemsetAsync(X.counters, 0, sizeof(int) * 4, s), "memset"))) return rc;
+    // per-level widths, starts and chunk offsets
+    const int L = w.maxLevel + 2;
+    int *lvlCnt = X.ar->get<int>(L), *lvlStart = X.ar->get<int>(L), *cc = X.ar->get<int>(L),
+        *chunkStart = X.ar->get<int>(L);
+    if (!lvlCnt || !lvlStart || !cc || !chunkStart) return X.fail(CULS_E_OOM, "rw: scratch arena exhausted (levels)");
+    if ((rc = X.check(cudaMemsetAsync(lvlCnt, 0, sizeof(int) * L, s), "memset"))) return rc;
+    k_level_count<<<X.grid(N - w.nL0), kBlock, 0, s>>>(w.nL0, N, w.wlev, lvlCnt);
+    k_level_chunks<<<grid_1d(L, kBlock, X.sms * 16), kBlock, 0, s>>>(L - 1, lvlCnt, kEnumWideMin, cc);
+    if ((rc = X.check(scan_exclusive(lvlCnt, lvlStart, L - 1, nullptr, *X.ar, s), "scan"))) return rc;
+    if ((rc = X.check(scan_exclusive(cc, chunkStart, L - 1, chunkStart + L - 1, *X.ar, s), "scan"))) return rc;
     k_enum_init<<<X.grid(N), kBlock, 0, s>>>(N, w.wlev, w.wl, w.lidLow, w.ref, w.cutL, w.cutM, cutA, done);
-    EnumArgs A{w.nL0, N, w.w0, w.w1, w.ref, w.lidLow, w.cutL, w.cutM, cutA, done, X.counters, X.status};
+    // lvlStart counts AND nodes only: the AND positions of W start at nL0
+    EnumArgs A{w.nL0, N,       lvlCnt, lvlStart, chunkStart, w.maxLevel, kEnumWideMin, w.w0, w.w1,
+               w.ref, w.lidLow, w.cutL, w.cutM, cutA,       done,       X.counters, X.status};
     X.mark(kMkEnumK0);
     k_enumerate<<<(unsigned)(X.sms * 8), kEnumBlock, 0, s>>>(A);
     X.mark(kMkEnumK1);
-    X.launched(2);
+    X.launched(6);
     if ((rc = X.check(cudaGetLastError(), "enumerate launch"))) return rc;
     return 0;
 }
