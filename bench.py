@@ -325,6 +325,9 @@ def our_arm(args, group):
     n_and = sum(g.nAnds for g in graphs)
     in_bytes = sum(4 * (2 * g.nObjs + g.nPOs) for g in graphs)
     d0 = ctx.upload_batch(graphs)
+    # the enumeration schedule, chosen by the autotuner on the workload
+    # itself (clones; outside the timed region)
+    tuned = ctx.autotune(d0)
     dw = ctx.clone(d0)
     ctx.profile(True)
     for _ in range(args.warmup):
@@ -384,6 +387,7 @@ def our_arm(args, group):
             "config": {"workload": WORKLOAD_DESC[args.workload], "graphs_per_gpu": len(graphs),
                        "and_nodes_per_gpu": n_and, "and_nodes_out_per_gpu": out_and,
                        "input_bytes_per_gpu": in_bytes, "l2": "inputs and working set larger than L2",
+                       "tuned": tuned,
                        "parallelism": f"graph-sharded x{group.world}" if group.world > 1 else "single GPU"},
             "roofline": roof,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": in_bytes,

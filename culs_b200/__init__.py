@@ -62,6 +62,9 @@ _lib.culs_graph_count.argtypes = [_vp]
 _lib.culs_graph_stats.argtypes = [_vp, ctypes.c_int, _ip, _ip, _ip, _ip]
 _lib.culs_batch_download.argtypes = [_vp, _vp, ctypes.POINTER(_HostGraph)]
 _lib.culs_batch_download_into.argtypes = [_vp, _vp, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+_lib.culs_set_param.argtypes = [_vp, ctypes.c_int, ctypes.c_int64]
+_lib.culs_get_param.argtypes = [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int64)]
+_lib.culs_autotune.argtypes = [_vp, _vp, ctypes.c_int]
 _lib.culs_rw_st_batch.argtypes = [_vp, ctypes.c_void_p, ctypes.c_int, ctypes.c_uint32, ctypes.c_uint32]
 _lib.culs_serve_start.argtypes = [_vp, ctypes.c_size_t, ctypes.c_int]
 _lib.culs_serve_stop.argtypes = [_vp]
@@ -224,6 +227,23 @@ class Context:
         arr = (_vp * len(handles))(*[d.h for d in handles])
         self._err(_lib.culs_rw_st_batch(self.h, ctypes.cast(arr, ctypes.c_void_p), len(handles), f,
                                         ST_CPU if cpu_st else 0), "rw;st batch")
+
+    # ---- tuning (speed only; results never change)
+    PARAMS = {"enum_wide_min": 1, "enum_blocks_per_sm": 2}
+
+    def set_param(self, name, value):
+        self._err(_lib.culs_set_param(self.h, self.PARAMS[name], value), f"set_param {name}")
+
+    def get_param(self, name):
+        v = ctypes.c_int64()
+        self._err(_lib.culs_get_param(self.h, self.PARAMS[name], ctypes.byref(v)), f"get_param {name}")
+        return v.value
+
+    def autotune(self, sample, rounds=1):
+        """Chooses the enumeration schedule by timing it on clones of the
+        device handle `sample`; returns the chosen parameters."""
+        self._err(_lib.culs_autotune(self.h, sample.h, rounds), "autotune")
+        return {k: self.get_param(k) for k in self.PARAMS}
 
     # ---- served mode
     def serve_start(self, admit_bytes=0, max_batch=0):

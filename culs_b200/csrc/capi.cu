@@ -255,6 +255,41 @@ int culs_fetch(culs_ctx *ctx, int64_t job, int32_t *fanin0, int32_t *fanin1, int
     return rc;
 }
 
+int culs_set_param(culs_ctx *ctx, int which, int64_t value) {
+    if (!ctx) return CULS_E_INVALID;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    culs::Tune &t = ctx->eng.tune();
+    switch (which) {
+        case CULS_PARAM_ENUM_WIDE_MIN:
+            if (value < 1 || value > (1ll << 30)) return CULS_E_INVALID;
+            t.enumWideMin = (int)value;
+            return CULS_OK;
+        case CULS_PARAM_ENUM_BLOCKS_PER_SM:
+            if (value < 1 || value > 64) return CULS_E_INVALID;
+            t.enumBlocksPerSm = (int)value;
+            return CULS_OK;
+        default:
+            return CULS_E_INVALID;
+    }
+}
+
+int culs_get_param(culs_ctx *ctx, int which, int64_t *value) {
+    if (!ctx || !value) return CULS_E_INVALID;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    const culs::Tune &t = ctx->eng.tune();
+    switch (which) {
+        case CULS_PARAM_ENUM_WIDE_MIN: *value = t.enumWideMin; return CULS_OK;
+        case CULS_PARAM_ENUM_BLOCKS_PER_SM: *value = t.enumBlocksPerSm; return CULS_OK;
+        default: return CULS_E_INVALID;
+    }
+}
+
+int culs_autotune(culs_ctx *ctx, const culs_graph *sample, int rounds) {
+    if (!ctx || !sample) return CULS_E_INVALID;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    return set_err(ctx, ctx->eng.autotune(sample->b, rounds));
+}
+
 int culs_rw_stats(culs_ctx *ctx, int64_t *out, int n) {
     if (!ctx || !out) return CULS_E_INVALID;
     const culs::RwStats &s = ctx->last;

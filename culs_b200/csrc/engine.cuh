@@ -22,6 +22,13 @@ namespace culs {
 
 struct ExecCtx;
 
+// Launch and schedule parameters that do not change results, only speed
+// (set by culs_set_param or culs_autotune).
+struct Tune {
+    int enumWideMin = 16384;   // levels this wide run one node per thread, narrower one per warp
+    int enumBlocksPerSm = 8;   // persistent enumeration blocks per SM
+};
+
 struct DevGraph {
     int nPIs, nPOs, nAnds, nLevels;
     int base;   // first position of this graph in graph-major arrays
@@ -123,6 +130,10 @@ class Engine {
     // Inverse of concat: parts[i] receives its graphs back from src.
     int split(const Batch &src, const std::vector<Batch *> &parts);
     void resetLaunchCount() { launches_ = 0; }
+    Tune &tune() { return tune_; }
+    // Times rw's enumeration on clones of `sample` for each candidate
+    // schedule and keeps the fastest; `rounds` timings per candidate.
+    int autotune(const Batch &sample, int rounds);
 
   private:
     int fail(int code, const std::string &msg);
@@ -154,6 +165,7 @@ class Engine {
     int launches_ = 0;
     int sms_ = 148;
     bool prof_ = false;
+    Tune tune_;
     cudaEvent_t ev_[kNumMarks] = {};
     bool evSet_[kNumMarks] = {};
 };

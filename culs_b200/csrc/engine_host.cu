@@ -170,6 +170,7 @@ ExecCtx Engine::ctx() {
     X.err = &err_;
     X.ev = prof_ ? ev_ : nullptr;
     X.evSet = evSet_;
+    X.tune = &tune_;
     return X;
 }
 

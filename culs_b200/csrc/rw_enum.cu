@@ -18,9 +18,6 @@ namespace culs {
 namespace {
 
 constexpr int kEnumBlock = 128;
-// Levels with at least this many AND nodes run one node per thread, narrower
-// ones one node per warp.
-constexpr int kEnumWideMin = 16384;
 
 struct EnumArgs {
     int64_t nL0, N;
@@ -523,15 +520,15 @@ int rw_enumerate(ExecCtx &X, RwWork &w) {
     if (!lvlCnt || !lvlStart || !cc || !chunkStart) return X.fail(CULS_E_OOM, "rw: scratch arena exhausted (levels)");
     if ((rc = X.check(cudaMemsetAsync(lvlCnt, 0, sizeof(int) * L, s), "memset"))) return rc;
     k_level_count<<<X.grid(N - w.nL0), kBlock, 0, s>>>(w.nL0, N, w.wlev, lvlCnt);
-    k_level_chunks<<<grid_1d(L, kBlock, X.sms * 16), kBlock, 0, s>>>(L - 1, lvlCnt, kEnumWideMin, cc);
+    k_level_chunks<<<grid_1d(L, kBlock, X.sms * 16), kBlock, 0, s>>>(L - 1, lvlCnt, X.tune->enumWideMin, cc);
     if ((rc = X.check(scan_exclusive(lvlCnt, lvlStart, L - 1, nullptr, *X.ar, s), "scan"))) return rc;
     if ((rc = X.check(scan_exclusive(cc, chunkStart, L - 1, chunkStart + L - 1, *X.ar, s), "scan"))) return rc;
     k_enum_init<<<X.grid(N), kBlock, 0, s>>>(N, w.wlev, w.wl, w.lidLow, w.ref, w.cutL, w.cutM, cutA, done);
     // lvlStart counts AND nodes only: the AND positions of W start at nL0
-    EnumArgs A{w.nL0, N,       lvlCnt, lvlStart, chunkStart, w.maxLevel, kEnumWideMin, w.w0, w.w1,
+    EnumArgs A{w.nL0, N,       lvlCnt, lvlStart, chunkStart, w.maxLevel, X.tune->enumWideMin, w.w0, w.w1,
                w.ref, w.lidLow, w.cutL, w.cutM, cutA,       done,       X.counters, X.status};
     X.mark(kMkEnumK0);
-    k_enumerate<<<(unsigned)(X.sms * 8), kEnumBlock, 0, s>>>(A);
+    k_enumerate<<<(unsigned)(X.sms * X.tune->enumBlocksPerSm), kEnumBlock, 0, s>>>(A);
     X.mark(kMkEnumK1);
     X.launched(6);
     if ((rc = X.check(cudaGetLastError(), "enumerate launch"))) return rc;

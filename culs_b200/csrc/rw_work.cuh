@@ -22,6 +22,7 @@ struct ExecCtx {
     int sms = 148;
     int *launches = nullptr;
     std::string *err = nullptr;
+    const Tune *tune = nullptr;  // launch and schedule parameters
     cudaEvent_t *ev = nullptr;  // profiling marks (null when profiling is off)
     bool *evSet = nullptr;
     void mark(int m) {

@@ -156,6 +156,20 @@ int culs_poll(culs_ctx *ctx, int64_t job, int32_t *nPIs, int32_t *nPOs, int32_t 
 int culs_wait(culs_ctx *ctx, int64_t job, int timeoutMs);
 int culs_fetch(culs_ctx *ctx, int64_t job, int32_t *fanin0, int32_t *fanin1, int32_t *outs, double *latencyMs);
 
+/* --------------------------------------------------------------- tuning
+ * Launch and schedule parameters: they change speed only, never results.
+ * CULS_PARAM_ENUM_WIDE_MIN: cut-enumeration levels with at least this many
+ * AND nodes run one node per thread, narrower ones one node per warp
+ * (default 16384).  CULS_PARAM_ENUM_BLOCKS_PER_SM: persistent enumeration
+ * blocks per SM (default 8).  culs_autotune times rw's enumeration on
+ * clones of `sample` (left unchanged) for candidate values, `rounds` times
+ * each, and keeps the fastest in the context.  No reference counterpart. */
+#define CULS_PARAM_ENUM_WIDE_MIN 1
+#define CULS_PARAM_ENUM_BLOCKS_PER_SM 2
+int culs_set_param(culs_ctx *ctx, int which, int64_t value);
+int culs_get_param(culs_ctx *ctx, int which, int64_t *value);
+int culs_autotune(culs_ctx *ctx, const culs_graph *sample, int rounds);
+
 /* Counters of the last culs_rw (the summary CPUSolver::Rewrite prints,
  * src/algorithms/rewrite.cu:896-897,926): replaced, replaced with positive
  * gain, replaced with zero gain, reverted, compromised, without a cut, small

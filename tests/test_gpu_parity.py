@@ -246,3 +246,45 @@ def test_invalid_graph_rejected(ctx):
     with pytest.raises(C.CulsError) as e:
         ctx.upload(bad)
     assert e.value.code == -1
+
+
+@pytest.mark.parametrize("wide_min", [1, 1 << 30])
+def test_both_enumeration_schedules_match_oracle(wide_min):
+    """Every level on one thread per node (1), or every level on one warp per
+    node (2^30): the enumeration schedule changes speed, never results."""
+    c = C.Context()
+    try:
+        c.set_param("enum_wide_min", wide_min)
+        for name in ["mult12", "c1", "unstrashed3", "far20k"]:
+            g = GRAPHS[name]
+            d = c.upload(g)
+            c.rw(d, dump=True)
+            D = c.dump()
+            o = Oracle()
+            o.set_graph(to_oracle(g))
+            o.rw()
+            np.testing.assert_array_equal(D["cuts"].reshape(-1, 8, 9), o.dump_cuts())
+            c.st(d)
+            assert same_graph(d.download(), oracle_rw_st(g).graph()), name
+        gs = C.gen_batch(4, 300, 12, 1000, 30000, 16, 512, threads=8)
+        db = c.upload_batch(gs)
+        c.rw_st(db)
+        for i, g in enumerate(gs):
+            assert same_graph(db.download(i), oracle_rw_st(g).graph()), i
+    finally:
+        c.close()
+
+
+def test_autotune_keeps_results():
+    c = C.Context()
+    try:
+        gs = C.gen_batch(4, 400, 16, 1000, 30000, 16, 512, threads=8)
+        sample = c.upload_batch(gs)
+        chosen = c.autotune(sample)
+        assert chosen["enum_wide_min"] in (2048, 4096, 8192, 16384, 32768, 65536, 1 << 30)
+        assert chosen["enum_blocks_per_sm"] in (4, 6, 8, 12, 16)
+        c.rw_st(sample)  # the sample itself is left unchanged by the tuner
+        for i, g in enumerate(gs):
+            assert same_graph(sample.download(i), oracle_rw_st(g).graph()), i
+    finally:
+        c.close()
