@@ -149,8 +149,10 @@ class Engine {
     // position's graph and local id (lid is read for the constant and PIs
     // only), po the PO literals over positions.  b.dg[g].cpos must hold each
     // graph's constant position.  Replaces b's arrays with the result.
+    // topo: positions are topological and b's graph-major layout (levels by
+    // an in-order dataflow instead of a worklist).
     int strash_core(Batch &b, int64_t M, const int *L0, const int *L1, const int *gid, const int *lid, const int *po,
-                    bool idOrder, bool removeDangling, bool foldTrivial);
+                    bool idOrder, bool removeDangling, bool foldTrivial, bool topo);
 
     std::string err_;
     cudaStream_t s_ = nullptr;

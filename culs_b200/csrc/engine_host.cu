@@ -304,7 +304,7 @@ int Engine::st(Batch &b, bool cpuOrder) {
     launches_ += 2;
     // `st` = GPU strash (frontier order, trivial folding); `st -c` = CPU strash
     // (id order, no folding), both with dangling removal
-    rc = strash_core(b, N, L0, L1, gid, lid, po, cpuOrder, true, !cpuOrder);
+    rc = strash_core(b, N, L0, L1, gid, lid, po, cpuOrder, true, !cpuOrder, true);
     if (prof_) mark(kMkStEnd);
     return rc;
 }

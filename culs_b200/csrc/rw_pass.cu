@@ -137,7 +137,7 @@ int Engine::rw(Batch &b, bool useZeros, bool gpuDedup, RwStats *stats, RwDump *d
                                                                            o1, b.nPO, w.wpo, opo);
     launches_ += 1;
     // updateFromRewriteManager(2) -> GPU strash; (1) -> CPU deduplicate
-    rc = strash_core(b, M, o0, o1, w.gidAll, w.wl, opo, false, gpuDedup, gpuDedup);
+    rc = strash_core(b, M, o0, o1, w.gidAll, w.wl, opo, false, gpuDedup, gpuDedup, false);
     X.mark(kMkRwEnd);
     return rc;
 }

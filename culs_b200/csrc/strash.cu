@@ -26,6 +26,8 @@
 #include <vector>
 
 #include "kernels.cuh"
+#include "rw_work.cuh"
+#include "sched.cuh"
 
 namespace culs {
 
@@ -208,6 +210,66 @@ __global__ void __launch_bounds__(kBlock) k_level_queue(unsigned long long *item
     }
     myMax = __reduce_max_sync(0xffffffffu, myMax);
     if (lane == 0 && myMax > 0) atomicMax(maxLevel, myMax);
+}
+
+__global__ void k_live_flags(int64_t M, const int *L0, const uint8_t *dead, uint8_t *liveFlag, int *done) {
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < M; v += stride) {
+        const bool isAnd = L0[v] >= 0;
+        liveFlag[v] = isAnd && !dead[v];
+        done[v] = isAnd ? 0 : 1;
+    }
+}
+
+// Levels of a graph-major batch whose positions are topological (`st`):
+// the in-order dataflow of the rw front over the interleaved chunk schedule
+// (sched.cuh), instead of a worklist over a fanout CSR.  Every AND node gets
+// its ASAP level; only live nodes count towards a graph's depth.
+__global__ void __launch_bounds__(kBlock) k_st_levelize(ChunkSched S, const int *L0, const int *L1,
+                                                         const uint8_t *liveFlag, const int *gid, int *level,
+                                                         int *done, int *graphLevels, int *counter, int *maxLevel,
+                                                         int *status) {
+    __shared__ int64_t s_begin, s_end;
+    int myMax = 0;
+    while (true) {
+        if (threadIdx.x == 0) {
+            const int64_t c = atomicAdd(counter, 1);
+            if (c < S.total) {
+                sched_chunk(S, c, s_begin, s_end);
+            } else {
+                s_begin = s_end = -1;
+            }
+        }
+        __syncthreads();
+        const int64_t begin = s_begin, end = s_end;
+        __syncthreads();
+        if (begin < 0) break;
+        const int64_t p = begin + threadIdx.x;
+        if (p >= end) continue;
+        const int a = L0[p];
+        if (a < 0) continue;  // constant or PI: level 0, done preset
+        const int u0 = a >> 1, u1 = L1[p] >> 1;
+        int l0 = 0, l1 = 0;
+        if (L0[u0] >= 0) {
+            if (!wait_ge(&done[u0], 1, status)) continue;
+            l0 = __ldcg(&level[u0]);
+        }
+        if (L0[u1] >= 0) {
+            if (!wait_ge(&done[u1], 1, status)) continue;
+            l1 = __ldcg(&level[u1]);
+        }
+        const int lv = 1 + (l0 > l1 ? l0 : l1);
+        __stcg(&level[p], lv);
+        if (liveFlag[p]) {
+            agg_max(graphLevels, gid[p], lv);
+            myMax = lv > myMax ? lv : myMax;
+        }
+        __threadfence();
+        st_release(&done[p], 1);
+    }
+    // every thread of the block leaves the loop at the same claim
+    myMax = __reduce_max_sync(0xffffffffu, myMax);
+    if ((threadIdx.x & 31) == 0 && myMax > 0) atomicMax(maxLevel, myMax);
 }
 
 __global__ void k_gather_levels(int64_t n, const int *idx, const int *level, uint32_t *keys, int *lvlCnt) {
@@ -440,7 +502,7 @@ __global__ void k_strash_out(int64_t nW, const int *wl, OutArgs A) {
 }  // namespace
 
 int Engine::strash_core(Batch &b, int64_t M, const int *L0, const int *L1, const int *gidA, const int *lidIn,
-                        const int *po, bool idOrder, bool removeDangling, bool foldTrivial) {
+                        const int *po, bool idOrder, bool removeDangling, bool foldTrivial, bool topo) {
     const int G = b.G;
     const int64_t nPO = b.nPO;
     cudaStream_t s = s_;
@@ -474,6 +536,27 @@ int Engine::strash_core(Batch &b, int64_t M, const int *L0, const int *L1, const
         launches_ += 4;
     }
     // 2. levels of live AND nodes
+    unsigned long long *items64 = nullptr;
+    int *liveIdx = nullptr;
+    if (topo) {
+        liveIdx = ar_.get<int>(M + 1);
+        int *done = pending;  // reuse
+        if (!liveIdx) return fail(CULS_E_OOM, "strash: scratch arena exhausted");
+        ExecCtx X = ctx();
+        ChunkSched sched;
+        int rc;
+        if ((rc = build_chunk_sched(X, b, kBlock, sched))) return rc;
+        check(cudaMemsetAsync(qc, 0, sizeof(int) * 8, s), "memset");
+        check(cudaMemsetAsync(graphLevels, 0, sizeof(int) * (G + 1), s), "memset");
+        check(cudaMemsetAsync(level, 0, sizeof(int) * (M + 1), s), "memset");
+        k_live_flags<<<gridM, kBlock, 0, s>>>(M, L0, dead, liveFlag, done);
+        check(compact_flags(liveFlag, M, liveIdx, qc + 3, ar_, s), "compact");  // live list and count
+        if (prof_) this->mark(kMkLevelK0);
+        k_st_levelize<<<gridQ, kBlock, 0, s>>>(sched, L0, L1, liveFlag, gidA, level, done, graphLevels, qc + 5,
+                                               qc + 4, status_);
+        if (prof_) this->mark(kMkLevelK1);
+        launches_ += 2;
+    } else {
     check(cudaMemsetAsync(off, 0, sizeof(int) * (M + 2), s), "memset");
     k_live_degrees<<<gridM, kBlock, 0, s>>>(M, L0, L1, dead, pending, off, liveFlag, flags);
     check(scan_exclusive(off, off, M + 1, nullptr, ar_, s), "scan");
@@ -486,8 +569,8 @@ int Engine::strash_core(Batch &b, int64_t M, const int *L0, const int *L1, const
     int *adj = ar_.get<int>(nEdges + 1);
     if (!adj) return fail(CULS_E_OOM, "strash: scratch arena exhausted");
     k_csr_fill<<<gridM, kBlock, 0, s>>>(M, L0, L1, liveFlag, cursor, adj);
-    unsigned long long *items64 = ar_.get<unsigned long long>(M + 1);
-    int *liveIdx = ar_.get<int>(M + 1);
+    items64 = ar_.get<unsigned long long>(M + 1);
+    liveIdx = ar_.get<int>(M + 1);
     if (!items64 || !liveIdx) return fail(CULS_E_OOM, "strash: scratch arena exhausted");
     check(cudaMemsetAsync(qc, 0, sizeof(int) * 8, s), "memset");
     check(cudaMemsetAsync(graphLevels, 0, sizeof(int) * (G + 1), s), "memset");
@@ -500,13 +583,14 @@ int Engine::strash_core(Batch &b, int64_t M, const int *L0, const int *L1, const
                                            graphLevels, qc + 4, status_);
     if (prof_) this->mark(kMkLevelK1);
     launches_ += 4;
+    }
     // 3. processing order (level, position) and tentative ranks
     check(cudaMemcpyAsync(hostSmall_, qc, sizeof(int) * 8, cudaMemcpyDeviceToHost, s), "d2h");
     if (sync()) return -1;
     if (check_status("strash levels")) return -1;
     int64_t nLive = hostSmall_[3];
     int maxLevel = hostSmall_[4];
-    if (hostSmall_[1] != nLive) return fail(CULS_E_INVALID, "strash: the AIG has a cycle");
+    if (!topo && hostSmall_[1] != nLive) return fail(CULS_E_INVALID, "strash: the AIG has a cycle");
     int *srt = ar_.get<int>(nLive + 1);
     uint32_t *keys = ar_.get<uint32_t>(nLive + 1);
     uint32_t *keys2 = ar_.get<uint32_t>(nLive + 1);
