@@ -174,6 +174,43 @@ def cpu_baseline(name, graphs, budget_s=12.0, threads=None):
             "sample": f"{desc}: {done} AND nodes in {dt:.1f} s"}
 
 
+def reference_gpu_path(graphs, max_nodes=4_000_000, timeout_s=600):
+    """The reference's own rw;st on the GPU, one graph at a time: its rewrite
+    and strash compiled from the CULS sources (oracle/_ref/rw_harness, built
+    by oracle/build_ref.sh), timed per graph with device synchronisation,
+    best of 2 runs after a warm-up.  None when the harness or a GPU is
+    missing."""
+    import tempfile
+    import culs_b200 as C
+    exe = ROOT / "oracle" / "_ref" / "rw_harness"
+    if not exe.exists():
+        return None
+    try:
+        import torch
+        if not torch.cuda.is_available():
+            return None
+    except Exception:
+        return None
+    with tempfile.TemporaryDirectory() as d:
+        files, nodes = [], 0
+        for i, g in enumerate(graphs):
+            if nodes >= max_nodes:
+                break
+            f = Path(d) / f"g{i}.aig"
+            C.write_aiger(f, g)
+            files.append(str(f))
+            nodes += g.nAnds
+        r = subprocess.run([str(exe), "time", "2"] + files, capture_output=True, text=True, timeout=timeout_s)
+        line = [l for l in r.stdout.splitlines() if l.startswith("HARNESS time")]
+        if r.returncode != 0 or not line:
+            return {"unavailable": f"reference harness exited {r.returncode}"}
+        kv = dict(x.split("=") for x in line[0].split()[2:])
+        ms = float(kv["ms"])
+        return {"value": int(kv["and_nodes"]) / (ms / 1e3), "unit": UNIT, "kind": "reference GPU rw;st",
+                "sample": f"{kv['files']} graphs one at a time, {kv['and_nodes']} AND nodes, "
+                          "AIGMan::rewrite + strash per graph, best of 2"}
+
+
 def reference_arm(args, group):
     """`--impl reference`: the reference's rw;st restated on the CPU (oracle
     port; the reference's own rw needs a GPU for cut enumeration, so it has no
@@ -193,6 +230,8 @@ def reference_arm(args, group):
             "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded generators)",
             "config": {"workload": WORKLOAD_DESC[args.workload]}, "cpu_baseline": cb,
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if args.workload in ("c1", "c2", "c3m", "c4", "c4m"):
+        line["reference_gpu_path"] = reference_gpu_path(graphs)
     print(json.dumps(line), flush=True)
     return 0
 
