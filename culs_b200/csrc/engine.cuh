@@ -11,6 +11,9 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <map>
+#include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -43,6 +46,26 @@ struct RwStats {
         newNodes, candidates;
 };
 
+// Device blocks freed by batches, kept for the next batch of a context (a
+// served loop or a benchmark uploads batches of similar size again and
+// again).  Shared by the engine and every batch it filled, so it outlives
+// whichever goes first; cached bytes are bounded.
+class DevPool {
+  public:
+    explicit DevPool(size_t limitBytes) : limit_(limitBytes) {}
+    ~DevPool();
+    // A block of at least `bytes` (the smallest cached one up to twice that
+    // size, else a new allocation); *got receives its size.
+    void *take(size_t bytes, size_t *got);
+    void give(void *p, size_t bytes);  // caches the block, or frees it beyond the limit
+    void flush();                      // frees every cached block
+
+  private:
+    std::mutex mu_;
+    std::multimap<size_t, void *> free_;
+    size_t cached_ = 0, limit_;
+};
+
 struct Batch {
     int G = 0;
     int64_t nObj = 0, nPO = 0;
@@ -54,6 +77,7 @@ struct Batch {
     // spare fanin/PO buffers: strash writes its output there and swaps
     int *F0s = nullptr, *F1s = nullptr, *POs = nullptr;
     int64_t capObjS = 0, capPOS = 0;
+    std::shared_ptr<DevPool> pool;  // where the buffers come from and go back to (null: cudaMalloc)
     ~Batch();
     void release();
     // Grows the buffers to hold nObj objects, nPO POs and G graphs (their
@@ -168,6 +192,7 @@ class Engine {
     int sms_ = 148;
     bool prof_ = false;
     Tune tune_;
+    std::shared_ptr<DevPool> pool_;
     cudaEvent_t ev_[kNumMarks] = {};
     bool evSet_[kNumMarks] = {};
 };

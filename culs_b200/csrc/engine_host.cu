@@ -25,41 +25,121 @@ int ExecCtx::status_check(const char *what) {
 
 Batch::~Batch() { release(); }
 
-static cudaError_t grow(int **p, int64_t &cap, int64_t need) {
+DevPool::~DevPool() { flush(); }
+
+void *DevPool::take(size_t bytes, size_t *got) {
+    {
+        std::lock_guard<std::mutex> lk(mu_);
+        auto it = free_.lower_bound(bytes);
+        if (it != free_.end() && it->first <= 2 * bytes) {
+            void *p = it->second;
+            *got = it->first;
+            cached_ -= it->first;
+            free_.erase(it);
+            return p;
+        }
+    }
+    void *p = nullptr;
+    if (cudaMalloc(&p, bytes) != cudaSuccess) {
+        flush();  // cached blocks may be what stands in the way
+        if (cudaMalloc(&p, bytes) != cudaSuccess) return nullptr;
+    }
+    *got = bytes;
+    return p;
+}
+
+void DevPool::give(void *p, size_t bytes) {
+    if (!p) return;
+    {
+        std::lock_guard<std::mutex> lk(mu_);
+        if (cached_ + bytes <= limit_) {
+            free_.emplace(bytes, p);
+            cached_ += bytes;
+            return;
+        }
+    }
+    cudaFree(p);
+}
+
+void DevPool::flush() {
+    std::multimap<size_t, void *> all;
+    {
+        std::lock_guard<std::mutex> lk(mu_);
+        all.swap(free_);
+        cached_ = 0;
+    }
+    for (auto &kv : all) cudaFree(kv.second);
+}
+
+namespace {
+
+template <class T>
+void drop(const std::shared_ptr<DevPool> &pool, T *&p, size_t bytes) {
+    if (p) {
+        if (pool)
+            pool->give(p, bytes);
+        else
+            cudaFree(p);
+    }
+    p = nullptr;
+}
+
+// Grows *p to at least `need` elements (contents not kept); cap is the
+// block's real element count.
+template <class T>
+cudaError_t grow(const std::shared_ptr<DevPool> &pool, T *&p, int64_t &cap, int64_t need) {
     need = std::max<int64_t>(need, 1);
-    if (*p && cap >= need) return cudaSuccess;
-    cudaFree(*p);
-    *p = nullptr;
+    if (p && cap >= need) return cudaSuccess;
+    drop(pool, p, sizeof(T) * (size_t)cap);
     cap = 0;
-    cudaError_t e = cudaMalloc(p, sizeof(int) * need);
+    if (pool) {
+        size_t got = 0;
+        p = static_cast<T *>(pool->take(sizeof(T) * (size_t)need, &got));
+        if (!p) return cudaErrorMemoryAllocation;
+        cap = (int64_t)(got / sizeof(T));
+        return cudaSuccess;
+    }
+    cudaError_t e = cudaMalloc(&p, sizeof(T) * (size_t)need);
     if (e == cudaSuccess) cap = need;
     return e;
 }
 
+}  // namespace
+
+void Batch::release() {
+    drop(pool, F0, sizeof(int) * (size_t)capObj);
+    drop(pool, F1, sizeof(int) * (size_t)capObj);
+    drop(pool, PO, sizeof(int) * (size_t)capPO);
+    drop(pool, dg, sizeof(DevGraph) * (size_t)capG);
+    drop(pool, F0s, sizeof(int) * (size_t)capObjS);
+    drop(pool, F1s, sizeof(int) * (size_t)capObjS);
+    drop(pool, POs, sizeof(int) * (size_t)capPOS);
+    capObj = capPO = capObjS = capPOS = 0;
+    capG = 0;
+    G = 0;
+    nObj = nPO = 0;
+    hg.clear();
+}
+
 cudaError_t Batch::reserve(int64_t n, int64_t np, int g) {
-    int64_t c0 = capObj, c1 = capObj;
+    int64_t c0 = capObj, c1 = capObj, cg = capG;
     cudaError_t e;
-    if ((e = grow(&F0, c0, n)) != cudaSuccess) return e;
-    if ((e = grow(&F1, c1, n)) != cudaSuccess) return e;
+    if ((e = grow(pool, F0, c0, n)) != cudaSuccess) return e;
+    if ((e = grow(pool, F1, c1, n)) != cudaSuccess) return e;
     capObj = std::min(c0, c1);
-    if ((e = grow(&PO, capPO, np)) != cudaSuccess) return e;
-    if (!dg || capG < std::max(g, 1)) {
-        cudaFree(dg);
-        dg = nullptr;
-        capG = 0;
-        if ((e = cudaMalloc(&dg, sizeof(DevGraph) * std::max(g, 1))) != cudaSuccess) return e;
-        capG = std::max(g, 1);
-    }
+    if ((e = grow(pool, PO, capPO, np)) != cudaSuccess) return e;
+    if ((e = grow(pool, dg, cg, g)) != cudaSuccess) return e;
+    capG = (int)cg;
     return cudaSuccess;
 }
 
 cudaError_t Batch::reserve_spare(int64_t n, int64_t np) {
     int64_t c0 = capObjS, c1 = capObjS;
     cudaError_t e;
-    if ((e = grow(&F0s, c0, n)) != cudaSuccess) return e;
-    if ((e = grow(&F1s, c1, n)) != cudaSuccess) return e;
+    if ((e = grow(pool, F0s, c0, n)) != cudaSuccess) return e;
+    if ((e = grow(pool, F1s, c1, n)) != cudaSuccess) return e;
     capObjS = std::min(c0, c1);
-    return grow(&POs, capPOS, np);
+    return grow(pool, POs, capPOS, np);
 }
 
 void Batch::swap_spare() {
@@ -68,24 +148,6 @@ void Batch::swap_spare() {
     std::swap(PO, POs);
     std::swap(capObj, capObjS);
     std::swap(capPO, capPOS);
-}
-
-void Batch::release() {
-    cudaFree(F0);
-    cudaFree(F1);
-    cudaFree(PO);
-    cudaFree(dg);
-    cudaFree(F0s);
-    cudaFree(F1s);
-    cudaFree(POs);
-    F0 = F1 = PO = nullptr;
-    F0s = F1s = POs = nullptr;
-    dg = nullptr;
-    capObj = capPO = capObjS = capPOS = 0;
-    capG = 0;
-    G = 0;
-    nObj = nPO = 0;
-    hg.clear();
 }
 
 // Decodes the embedded rwlib.bin (culs_b200/data/make_rwlib.py layout).
@@ -199,6 +261,7 @@ int Engine::init(size_t hbmBudget) {
     size_t freeB = 0, totalB = 0;
     cudaMemGetInfo(&freeB, &totalB);
     budget_ = hbmBudget ? hbmBudget : totalB;
+    pool_ = std::make_shared<DevPool>(budget_ / 4);  // freed batch buffers kept for reuse
     return 0;
 }
 
@@ -208,6 +271,11 @@ int Engine::ensure_arena(size_t bytes) {
     if (bytes > budget_) return fail(CULS_E_BUDGET, "request exceeds the HBM budget");
     ar_.reset();
     cudaError_t e = ar_.reserve(bytes);
+    if (e != cudaSuccess && pool_) {  // cached batch buffers may be in the way
+        cudaGetLastError();
+        pool_->flush();
+        e = ar_.reserve(bytes);
+    }
     if (e != cudaSuccess) return fail(CULS_E_OOM, std::string("device arena: ") + cudaGetErrorString(e));
     return 0;
 }
@@ -229,6 +297,7 @@ float Engine::elapsed(int a, int b) {
 int Engine::clone(const Batch &src, Batch &dst) {
     if (&src == &dst) return 0;
     int rc;
+    if (!dst.pool) dst.pool = pool_;
     if ((rc = check(dst.reserve(src.nObj, src.nPO, src.G), "cudaMalloc"))) return rc;
     cudaMemcpyAsync(dst.F0, src.F0, sizeof(int) * src.nObj, cudaMemcpyDeviceToDevice, s_);
     cudaMemcpyAsync(dst.F1, src.F1, sizeof(int) * src.nObj, cudaMemcpyDeviceToDevice, s_);

@@ -79,6 +79,8 @@ int Engine::upload(Batch &b, int count, const int32_t *const *f0, const int32_t 
     }
     int rc;
     if ((rc = ensure_stage((size_t)2 * nObj + nPO))) return rc;
+    if (!b.pool) b.pool = pool_;
+    if ((rc = check(b.reserve(nObj, nPO, count), "cudaMalloc"))) return rc;
     int32_t *sF0 = stage_, *sF1 = stage_ + nObj, *sPO = stage_ + 2 * nObj;
     const std::vector<int> runs = split_runs(hg, nObj, host_threads(nObj, count));
     std::atomic<int> bad{0};
@@ -116,13 +118,19 @@ int Engine::upload(Batch &b, int count, const int32_t *const *f0, const int32_t 
             }
             hg[g].nLevels = mx;  // AIGMan::readFromMemory's nLevels
         }
+        // this run is staged: its copies overlap the other runs' staging
+        const DevGraph &a = hg[runs[r]], &z = hg[runs[r + 1] - 1];
+        const int64_t o0 = a.base, o1 = (int64_t)z.base + 1 + z.nPIs + z.nAnds;
+        const int64_t p0 = a.poOff, p1 = (int64_t)z.poOff + z.nPOs;
+        cudaMemcpyAsync(b.F0 + o0, sF0 + o0, sizeof(int) * (o1 - o0), cudaMemcpyHostToDevice, s_);
+        cudaMemcpyAsync(b.F1 + o0, sF1 + o0, sizeof(int) * (o1 - o0), cudaMemcpyHostToDevice, s_);
+        if (p1 > p0) cudaMemcpyAsync(b.PO + p0, sPO + p0, sizeof(int) * (p1 - p0), cudaMemcpyHostToDevice, s_);
     };
     run_parallel((int)runs.size() - 1, work);
-    if (bad.load()) return fail(CULS_E_INVALID, why);
-    if ((rc = check(b.reserve(nObj, nPO, count), "cudaMalloc"))) return rc;
-    cudaMemcpyAsync(b.F0, sF0, sizeof(int) * nObj, cudaMemcpyHostToDevice, s_);
-    cudaMemcpyAsync(b.F1, sF1, sizeof(int) * nObj, cudaMemcpyHostToDevice, s_);
-    if (nPO) cudaMemcpyAsync(b.PO, sPO, sizeof(int) * nPO, cudaMemcpyHostToDevice, s_);
+    if (bad.load()) {
+        sync();  // copies already issued read the staging buffer
+        return fail(CULS_E_INVALID, why);
+    }
     cudaMemcpyAsync(b.dg, hg.data(), sizeof(DevGraph) * count, cudaMemcpyHostToDevice, s_);
     b.G = count;
     b.nObj = nObj;
@@ -137,16 +145,35 @@ int Engine::download_all(const Batch &b, int32_t *const *f0, int32_t *const *f1,
     int rc;
     if ((rc = ensure_stage((size_t)2 * b.nObj + b.nPO))) return rc;
     int32_t *sF0 = stage_, *sF1 = stage_ + b.nObj, *sPO = stage_ + 2 * b.nObj;
-    if (f0 && (rc = check(cudaMemcpyAsync(sF0, b.F0, sizeof(int) * b.nObj, cudaMemcpyDeviceToHost, s_), "d2h")))
-        return rc;
-    if (f1 && (rc = check(cudaMemcpyAsync(sF1, b.F1, sizeof(int) * b.nObj, cudaMemcpyDeviceToHost, s_), "d2h")))
-        return rc;
-    if (outs && b.nPO &&
-        (rc = check(cudaMemcpyAsync(sPO, b.PO, sizeof(int) * b.nPO, cudaMemcpyDeviceToHost, s_), "d2h")))
-        return rc;
-    if ((rc = sync())) return rc;
     const std::vector<int> runs = split_runs(b.hg, b.nObj, host_threads(b.nObj, b.G));
-    run_parallel((int)runs.size() - 1, [&](int r) {
+    const int nr = (int)runs.size() - 1;
+    // one event per run: a thread scatters its run as soon as it has landed
+    std::vector<cudaEvent_t> ev(nr, nullptr);
+    for (int r = 0; r < nr && rc == 0; r++) {
+        const DevGraph &a = b.hg[runs[r]], &z = b.hg[runs[r + 1] - 1];
+        const int64_t o0 = a.base, o1 = (int64_t)z.base + 1 + z.nPIs + z.nAnds;
+        const int64_t p0 = a.poOff, p1 = (int64_t)z.poOff + z.nPOs;
+        if (f0) rc = check(cudaMemcpyAsync(sF0 + o0, b.F0 + o0, sizeof(int) * (o1 - o0), cudaMemcpyDeviceToHost, s_),
+                           "d2h");
+        if (!rc && f1)
+            rc = check(cudaMemcpyAsync(sF1 + o0, b.F1 + o0, sizeof(int) * (o1 - o0), cudaMemcpyDeviceToHost, s_), "d2h");
+        if (!rc && outs && p1 > p0)
+            rc = check(cudaMemcpyAsync(sPO + p0, b.PO + p0, sizeof(int) * (p1 - p0), cudaMemcpyDeviceToHost, s_), "d2h");
+        if (!rc) rc = check(cudaEventCreateWithFlags(&ev[r], cudaEventDisableTiming), "event");
+        if (!rc) rc = check(cudaEventRecord(ev[r], s_), "event");
+    }
+    if (rc) {
+        sync();
+        for (cudaEvent_t e : ev)
+            if (e) cudaEventDestroy(e);
+        return rc;
+    }
+    std::atomic<int> bad{0};
+    run_parallel(nr, [&](int r) {
+        if (cudaEventSynchronize(ev[r]) != cudaSuccess) {
+            bad.store(1);
+            return;
+        }
         for (int g = runs[r]; g < runs[r + 1]; g++) {
             const DevGraph &d = b.hg[g];
             const size_t n = 1 + (size_t)d.nPIs + d.nAnds;
@@ -155,6 +182,8 @@ int Engine::download_all(const Batch &b, int32_t *const *f0, int32_t *const *f1,
             if (outs && outs[g] && d.nPOs) memcpy(outs[g], sPO + d.poOff, sizeof(int32_t) * d.nPOs);
         }
     });
+    for (cudaEvent_t e : ev) cudaEventDestroy(e);
+    if (bad.load()) return check(cudaErrorUnknown, "d2h");
     return 0;
 }
 
@@ -175,6 +204,7 @@ int Engine::concat(const std::vector<const Batch *> &parts, Batch &dst) {
     if (G < 1) return fail(CULS_E_INVALID, "concat: no graphs");
     if (nObj >= (1ll << 29)) return fail(CULS_E_INVALID, "concat: batch too large for 30-bit node positions");
     int rc;
+    if (!dst.pool) dst.pool = pool_;
     if ((rc = check(dst.reserve(nObj, nPO, G), "cudaMalloc"))) return rc;
     std::vector<DevGraph> hg;
     hg.reserve(G);
@@ -212,6 +242,7 @@ int Engine::split(const Batch &src, const std::vector<Batch *> &parts) {
         const DevGraph &z = src.hg[first + G - 1];
         const int64_t objEnd = (int64_t)z.base + 1 + z.nPIs + z.nAnds;
         const int64_t nObj = objEnd - a.base, nPO = (int64_t)z.poOff + z.nPOs - a.poOff;
+        if (!p->pool) p->pool = pool_;
         if ((rc = check(p->reserve(nObj, nPO, G), "cudaMalloc"))) return rc;
         cudaMemcpyAsync(p->F0, src.F0 + a.base, sizeof(int) * nObj, cudaMemcpyDeviceToDevice, s_);
         cudaMemcpyAsync(p->F1, src.F1 + a.base, sizeof(int) * nObj, cudaMemcpyDeviceToDevice, s_);

@@ -706,6 +706,7 @@ int Engine::strash_core(Batch &b, int64_t M, const int *L0, const int *L1, const
     DevGraph *dgNew = reinterpret_cast<DevGraph *>(ar_.get<char>(sizeof(DevGraph) * (G + 1)));
     if (!dgNew) return fail(CULS_E_OOM, "strash: arena");
     // the output goes to the batch's spare buffers, swapped in at the end
+    if (!b.pool) b.pool = pool_;
     if (check(b.reserve_spare(nObjNew + 1, nPO + 1), "cudaMalloc")) return -1;
     int *F0n = b.F0s, *F1n = b.F1s, *POn = b.POs;
     check(cudaMemcpyAsync(dgNew, ng.data(), sizeof(DevGraph) * G, cudaMemcpyHostToDevice, s), "h2d");
