@@ -366,7 +366,7 @@ def our_arm(args, group):
     d0 = ctx.upload_batch(graphs)
     # the enumeration schedule, chosen by the autotuner on the workload
     # itself (clones; outside the timed region)
-    tuned = ctx.autotune(d0)
+    tuned = ctx.autotune(d0, rounds=2)
     dw = ctx.clone(d0)
     ctx.profile(True)
     for _ in range(args.warmup):

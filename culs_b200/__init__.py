@@ -66,7 +66,7 @@ _lib.culs_set_param.argtypes = [_vp, ctypes.c_int, ctypes.c_int64]
 _lib.culs_get_param.argtypes = [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int64)]
 _lib.culs_autotune.argtypes = [_vp, _vp, ctypes.c_int]
 _lib.culs_rw_st_batch.argtypes = [_vp, ctypes.c_void_p, ctypes.c_int, ctypes.c_uint32, ctypes.c_uint32]
-_lib.culs_serve_start.argtypes = [_vp, ctypes.c_size_t, ctypes.c_int]
+_lib.culs_serve_start.argtypes = [_vp, ctypes.c_size_t, ctypes.c_int, ctypes.c_int]
 _lib.culs_serve_stop.argtypes = [_vp]
 _lib.culs_submit.argtypes = [_vp, _ip, _ip, _ip, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_uint32,
                              ctypes.c_uint32, ctypes.POINTER(ctypes.c_int64)]
@@ -246,8 +246,8 @@ class Context:
         return {k: self.get_param(k) for k in self.PARAMS}
 
     # ---- served mode
-    def serve_start(self, admit_bytes=0, max_batch=0):
-        self._err(_lib.culs_serve_start(self.h, admit_bytes, max_batch), "serve start")
+    def serve_start(self, admit_bytes=0, max_batch=0, workers=0):
+        self._err(_lib.culs_serve_start(self.h, admit_bytes, max_batch, workers), "serve start")
 
     def serve_stop(self):
         self._err(_lib.culs_serve_stop(self.h), "serve stop")

@@ -202,12 +202,17 @@ std::shared_ptr<culs::Server> server_of(culs_ctx *ctx) {
 }
 }  // namespace
 
-int culs_serve_start(culs_ctx *ctx, size_t admitBytes, int maxBatch) {
+int culs_serve_start(culs_ctx *ctx, size_t admitBytes, int maxBatch, int workers) {
     if (!ctx) return CULS_E_INVALID;
     std::lock_guard<std::mutex> lk(ctx->srvMu);
     if (ctx->srv) return CULS_E_INVALID;
     if (admitBytes == 0) admitBytes = ctx->eng.budget();
-    ctx->srv = std::make_shared<culs::Server>(ctx->eng, ctx->mu, admitBytes, maxBatch);
+    if (workers <= 0) workers = 2;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaSetDevice(ctx->eng.device());  // the server's own engines live beside the context's
+    ctx->srv = std::make_shared<culs::Server>(ctx->eng, ctx->mu, admitBytes, maxBatch, workers);
+    cudaSetDevice(dev);
     return CULS_OK;
 }
 

@@ -143,6 +143,7 @@ class Engine {
 
     cudaStream_t stream() const { return s_; }
     size_t budget() const { return budget_; }
+    int device() const { return device_; }  // the CUDA device the engine lives on
     size_t arenaHighWater() const { return ar_.high_water(); }
     int kernelLaunches() const { return launches_; }
     void setProfile(bool on) { prof_ = on; }
@@ -187,6 +188,7 @@ class Engine {
     int32_t *stage_ = nullptr;  // pinned staging for uploads and downloads
     size_t stageCap_ = 0;       // in int32
     size_t budget_ = 0;
+    int device_ = 0;
     Arena ar_;
     int launches_ = 0;
     int sms_ = 148;

@@ -240,6 +240,7 @@ int Engine::init(size_t hbmBudget) {
     int n = 0;
     if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) return fail(CULS_E_DEVICE, "no CUDA device");
     int rc;
+    if ((rc = check(cudaGetDevice(&device_), "device"))) return rc;
     if ((rc = check(cudaStreamCreateWithFlags(&s_, cudaStreamNonBlocking), "stream"))) return rc;
     sms_ = num_sms();
     RwLib *h = new RwLib;

@@ -5,9 +5,22 @@
 
 namespace culs {
 
-Server::Server(Engine &eng, std::mutex &engMu, size_t admitBytes, int maxBatch)
-    : eng_(eng), engMu_(engMu), admit_(admitBytes), maxBatch_(maxBatch > 0 ? maxBatch : 1 << 20) {
-    th_ = std::thread([this] { worker(); });
+Server::Server(Engine &eng, std::mutex &engMu, size_t admitBytes, int maxBatch, int workers)
+    : eng_(eng), engMu_(engMu), maxBatch_(maxBatch > 0 ? maxBatch : 1 << 20) {
+    workers = workers < 1 ? 1 : workers;
+    admit_ = admitBytes / (size_t)workers;  // every worker's batch within its share
+    for (int w = 1; w < workers; w++) {
+        auto e = std::make_unique<Engine>();
+        if (e->init(eng.budget() / (size_t)workers) != CULS_OK) break;  // fewer workers
+        own_.push_back(std::move(e));
+        ownMu_.push_back(std::make_unique<std::mutex>());
+    }
+    th_ = std::thread([this] { worker(eng_, engMu_); });
+    for (size_t i = 0; i < own_.size(); i++) {
+        Engine *e = own_[i].get();
+        std::mutex *m = ownMu_[i].get();
+        extra_.emplace_back([this, e, m] { worker(*e, *m); });
+    }
 }
 
 Server::~Server() {
@@ -17,6 +30,8 @@ Server::~Server() {
     }
     cvWork_.notify_all();
     if (th_.joinable()) th_.join();
+    for (auto &t : extra_)
+        if (t.joinable()) t.join();
 }
 
 int Server::submit(const int32_t *f0, const int32_t *f1, const int32_t *outs, int32_t nPIs, int32_t nPOs,
@@ -99,7 +114,8 @@ int Server::fetch(int64_t id, int32_t *f0, int32_t *f1, int32_t *outs, double *l
     return CULS_OK;
 }
 
-void Server::worker() {
+void Server::worker(Engine &eng, std::mutex &engMu) {
+    cudaSetDevice(eng.device());  // the current device is per thread
     while (true) {
         std::vector<ServeJob *> batch;
         {
@@ -132,12 +148,12 @@ void Server::worker() {
                 rest.pop_back();
             }
         }
-        run_batch(batch);
+        run_batch(eng, engMu, batch);
         cvDone_.notify_all();
     }
 }
 
-void Server::run_batch(std::vector<ServeJob *> &batch) {
+void Server::run_batch(Engine &eng, std::mutex &engMu, std::vector<ServeJob *> &batch) {
     const int n = (int)batch.size();
     std::vector<const int32_t *> f0(n), f1(n), po(n);
     std::vector<int32_t> nPIs(n), nPOs(n), nAnds(n);
@@ -153,14 +169,14 @@ void Server::run_batch(std::vector<ServeJob *> &batch) {
     int rc;
     std::string why;
     {
-        std::lock_guard<std::mutex> lk(engMu_);
+        std::lock_guard<std::mutex> lk(engMu);
         Batch b;
-        rc = eng_.upload(b, n, f0.data(), f1.data(), po.data(), nPIs.data(), nPOs.data(), nAnds.data());
+        rc = eng.upload(b, n, f0.data(), f1.data(), po.data(), nPIs.data(), nPOs.data(), nAnds.data());
         if (rc == CULS_OK) {
             RwStats st{};
-            rc = eng_.rw(b, (rwf & CULS_RW_ZEROS) != 0, (rwf & CULS_RW_GPU_DEDUP) != 0, &st, nullptr);
+            rc = eng.rw(b, (rwf & CULS_RW_ZEROS) != 0, (rwf & CULS_RW_GPU_DEDUP) != 0, &st, nullptr);
         }
-        if (rc == CULS_OK) rc = eng_.st(b, (stf & CULS_ST_CPU) != 0);
+        if (rc == CULS_OK) rc = eng.st(b, (stf & CULS_ST_CPU) != 0);
         if (rc == CULS_OK) {
             std::vector<int32_t *> o0(n), o1(n), oo(n);
             for (int i = 0; i < n; i++) {
@@ -175,9 +191,9 @@ void Server::run_batch(std::vector<ServeJob *> &batch) {
                 o1[i] = batch[i]->f1.data();
                 oo[i] = batch[i]->outs.data();
             }
-            rc = eng_.download_all(b, o0.data(), o1.data(), oo.data());
+            rc = eng.download_all(b, o0.data(), o1.data(), oo.data());
         }
-        if (rc != CULS_OK) why = eng_.error();
+        if (rc != CULS_OK) why = eng.error();
     }
     const auto now = std::chrono::steady_clock::now();
     std::lock_guard<std::mutex> lk(mu_);

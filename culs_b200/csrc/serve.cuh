@@ -40,7 +40,10 @@ class Server {
     // of rw plus the graph arrays and their spares).
     static constexpr size_t kBytesPerObj = 720;
 
-    Server(Engine &eng, std::mutex &engMu, size_t admitBytes, int maxBatch);
+    // workers > 1 adds engines of the server's own (stream, arena, staging)
+    // on the same device, so batches overlap on the GPU: a batch waits on its
+    // deepest graph's critical path, during which most SMs would sit idle.
+    Server(Engine &eng, std::mutex &engMu, size_t admitBytes, int maxBatch, int workers = 1);
     ~Server();  // finishes every queued job, then stops the worker
 
     int submit(const int32_t *f0, const int32_t *f1, const int32_t *outs, int32_t nPIs, int32_t nPOs, int32_t nAnds,
@@ -55,11 +58,14 @@ class Server {
     const std::string &lastError() const { return err_; }
 
   private:
-    void worker();
-    void run_batch(std::vector<ServeJob *> &batch);
+    void worker(Engine &eng, std::mutex &engMu);
+    void run_batch(Engine &eng, std::mutex &engMu, std::vector<ServeJob *> &batch);
 
     Engine &eng_;
     std::mutex &engMu_;
+    std::vector<std::unique_ptr<Engine>> own_;  // engines of workers 2..n
+    std::vector<std::unique_ptr<std::mutex>> ownMu_;
+    std::vector<std::thread> extra_;
     size_t admit_;
     int maxBatch_;
     std::mutex mu_;

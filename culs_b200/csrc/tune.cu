@@ -35,6 +35,14 @@ int Engine::autotune(const Batch &sample, int rounds) {
     Tune best = tune_;
     float bestMs = FLT_MAX;
     int rc = CULS_OK;
+    {  // one untimed pass first: clocks, caches and the arena settle
+        float ms;
+        if ((rc = measure(best, ms))) {
+            tune_ = best;
+            prof_ = prof;
+            return rc;
+        }
+    }
     const int wides[] = {2048, 4096, 8192, 16384, 32768, 65536, 1 << 30};
     for (int w : wides) {
         Tune t = best;

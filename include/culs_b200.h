@@ -136,7 +136,10 @@ int culs_rw_st_batch(culs_ctx *ctx, culs_graph *const *gs, int count, uint32_t r
  * with the first job's flags) while their estimated device footprint stays
  * within admitBytes (0: the context's HBM budget) and maxBatch (<= 0: no
  * limit), runs them as one batch, and holds every result until fetched.
- * Jobs and direct calls on the same context never overlap on the device.
+ * `workers` (<= 0: 2) batches run at once, each on an engine of its own
+ * (the first is the context's), splitting the admission budget: a batch
+ * waits on its deepest graph while most of the GPU would sit idle.  Jobs
+ * and direct calls on the same context never overlap on its engine.
  * No counterpart in the reference (one AIG per process invocation).
  *
  * culs_submit copies the graph (the caller may free its arrays) and returns
@@ -148,7 +151,7 @@ int culs_rw_st_batch(culs_ctx *ctx, culs_graph *const *gs, int count, uint32_t r
  * submit-to-done latency in ms, and forgets the job.  culs_serve_stop
  * finishes every queued job, then ends the worker; results not fetched by
  * then are discarded.  Admission charges 720 device bytes per object. */
-int culs_serve_start(culs_ctx *ctx, size_t admitBytes, int maxBatch);
+int culs_serve_start(culs_ctx *ctx, size_t admitBytes, int maxBatch, int workers);
 int culs_serve_stop(culs_ctx *ctx);
 int culs_submit(culs_ctx *ctx, const int32_t *fanin0, const int32_t *fanin1, const int32_t *outs, int32_t nPIs,
                 int32_t nPOs, int32_t nAnds, uint32_t rwFlags, uint32_t stFlags, int64_t *job);
