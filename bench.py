@@ -292,7 +292,7 @@ def served_arm(args, group):
     pool = served_pool()
     rng = np.random.default_rng(5)
     # capacity: one batch of the whole pool through the served path
-    ctx.serve_start()
+    ctx.serve_start(workers=args.workers)
     t0 = time.perf_counter()
     ids = [ctx.submit(g) for g in pool]
     for j in ids:
@@ -345,7 +345,7 @@ def served_arm(args, group):
             "config": {"workload": WORKLOAD_DESC["c5"], "jobs": njobs, "pool_graphs": len(pool),
                        "offered_jobs_per_s": rate, "load_vs_capacity": args.load,
                        "capacity_jobs_per_s": cap_jobs_s, "timing": "wall clock, submit to fetch",
-                       "parallelism": "single GPU, dynamic batching"},
+                       "parallelism": f"single GPU, dynamic batching, {args.workers} batches at once"},
             "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                            "mean": float(lat.mean()), "max": float(lat[-1])},
             "plain_single_graph_path": plain,
@@ -454,6 +454,7 @@ def main():
     ap.add_argument("--workload", default="c4", choices=["c4", "c4m", "c3", "c3m", "c2", "c1", "c5"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--load", type=float, default=0.75, help="c5: offered load as a fraction of measured capacity")
+    ap.add_argument("--workers", type=int, default=2, help="c5: batches the served mode runs at once")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -63,6 +63,26 @@ def test_served_jobs_match_oracle(ctx):
         ctx.serve_stop()
 
 
+def test_served_workers_match_oracle(ctx):
+    # three workers, each with an engine of its own, take their shares of a burst
+    gs = graphs()
+    ctx.serve_start(workers=3)
+    try:
+        jobs = [(ctx.submit(g), g) for g in gs * 3]
+        for job, g in jobs:
+            assert ctx.wait(job, 60000)
+            out, _ = ctx.fetch(job)
+            ref = oracle_rw_st(g).graph()
+            assert same_graph(out, ref), job
+            assert out.nLevels == ref.nLevels
+    finally:
+        ctx.serve_stop()
+    # direct calls on the context still work after the server stopped
+    h = ctx.upload(gs[0])
+    ctx.rw_st_batch([h])
+    assert same_graph(h.download(), oracle_rw_st(gs[0]).graph())
+
+
 def test_served_job_error_is_reported():
     small = C.Context(hbm_budget=1 << 20)
     small.serve_start()
