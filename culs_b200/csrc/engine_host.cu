@@ -170,6 +170,7 @@ static bool decode_lib(const unsigned char *b, size_t n, RwLib &L) {
     memcpy(L.nRoots, nr, kNumClasses);
     memset(L.node, 0, sizeof L.node);
     memset(L.roots, 0, sizeof L.roots);
+    memset(L.batch, 0xFF, sizeof L.batch);
     for (int c = 0; c < kNumClasses; c++) {
         if (L.nNodes[c] > kMaxLibNodes - 4 || L.nRoots[c] > 16) return false;
         if (!need((size_t)L.nNodes[c] * 4 + L.nRoots[c])) return false;
@@ -183,6 +184,30 @@ static bool decode_lib(const unsigned char *b, size_t n, RwLib &L) {
         cur += L.nRoots[c];
         for (int i = 0; i < L.nNodes[c]; i++)  // fanins precede their node
             if (ln_f0(L.node[c][i]) >= i + 4 || ln_f1(L.node[c][i]) >= i + 4) return false;
+        // evaluation batches: nodes by depth (inputs at depth 0), index order
+        // within a depth, at most kLibBatch per batch
+        int depth[kMaxLibNodes], maxDepth = 0;
+        for (int i = 0; i < 4; i++) depth[i] = 0;
+        for (int i = 0; i < L.nNodes[c]; i++) {
+            const int d0 = depth[ln_f0(L.node[c][i])], d1 = depth[ln_f1(L.node[c][i])];
+            depth[i + 4] = 1 + (d0 > d1 ? d0 : d1);
+            maxDepth = depth[i + 4] > maxDepth ? depth[i + 4] : maxDepth;
+        }
+        int nb = 0;
+        for (int d = 1; d <= maxDepth; d++) {
+            uint32_t ent[kLibBatch];
+            int k = 0;
+            for (int i = 0; i <= L.nNodes[c]; i++) {
+                const bool flush = k == kLibBatch || (i == L.nNodes[c] && k > 0);
+                if (flush) {
+                    for (int e = k; e < kLibBatch; e++) ent[e] = kNoLibNode;
+                    L.batch[c][nb++] = uint4{ent[0], ent[1], ent[2], ent[3]};
+                    k = 0;
+                }
+                if (i < L.nNodes[c] && depth[i + 4] == d) ent[k++] = L.node[c][i] | ((uint32_t)i << 18);
+            }
+        }
+        L.nBatches[c] = (uint8_t)nb;
     }
     return cur == n;
 }

@@ -28,7 +28,17 @@ struct RwLib {
     // fanin0 (bits 0-7) | fanin1 (bits 8-15) | compl0 (bit 16) | compl1 (bit 17)
     uint32_t node[kNumClasses][kMaxLibNodes];
     uint8_t roots[kNumClasses][16];
+    // The same internal nodes regrouped for evaluation: batches of up to
+    // kLibBatch nodes of equal depth (every fanin in an earlier batch), in
+    // order of depth.  Entry = node word | index j (bits 18-23), or
+    // kNoLibNode for an unused entry.  Nodes of one batch never read each
+    // other, so their table probes are issued together.
+    uint4 batch[kNumClasses][kMaxLibNodes];
+    uint8_t nBatches[kNumClasses];
 };
+constexpr int kLibBatch = 4;
+constexpr uint32_t kNoLibNode = 0xFFFFFFFFu;
+static_assert(kLibBatch == 4, "a batch is one uint4");
 
 CULS_HD int npn_phase(uint32_t w) { return (int)(w & 31u); }
 CULS_HD int npn_perm(uint32_t w) { return (int)((w >> 8) & 31u); }
@@ -407,11 +417,14 @@ CULS_HD int4 region_load(const TabRegion &t, uint32_t h) {
 #endif
 }
 
-// Finishes a lookup whose home slot h was already loaded into s: returns
-// {position, level} of the key, or {-1, 0} when absent.
-CULS_HD int2 region_resolve(const TabRegion &t, unsigned long long key, uint32_t h, int4 s, int *status) {
+// Finishes a lookup whose home slot was already loaded into s: returns
+// {position, level} of the key, or {-1, 0} when absent.  The home index is
+// recomputed only when the probe goes on past it.
+CULS_HD int2 region_resolve(const TabRegion &t, unsigned long long key, int4 s, int *status) {
+    uint32_t h = 0;
     for (uint32_t probe = 0; probe < t.size; probe++) {
         if (probe > 0) {
+            if (probe == 1) h = region_home(key, t.size);
             if (++h == t.size) h = 0;
             s = region_load(t, h);
         }
@@ -447,62 +460,76 @@ struct EvalIn {
 };
 
 // 8-entry reference table of CalcMFFC (src/algorithms/rewrite.cu:296-316).
-// Every access below uses a compile-time index after unrolling, so the
-// table stays in registers.
+// Every access below names its entry by a literal index (CULS_EACH8), never
+// by a loop variable left to the unroller, so the table stays in registers
+// however large the calling kernel grows.
 struct MffcTab {
     int size;
     int id[8];
     int num[8];
 };
 
+#define CULS_EACH8(X) X(0) X(1) X(2) X(3) X(4) X(5) X(6) X(7)
+
 CULS_HD int pick8(const int (&v)[8], int i) {
     int r = v[0];
-#pragma unroll
-    for (int k = 1; k < 8; k++)
-        if (k == i) r = v[k];
+#define CULS_PICK8(k) \
+    if (k == i) r = v[k];
+    CULS_EACH8(CULS_PICK8)
+#undef CULS_PICK8
     return r;
 }
 
 // Decrease, src/algorithms/rewrite.cu:296-309.  *slot receives the table
 // entry whose count was returned (unchanged for leaves and a full table).
 CULS_HD int mffc_decrease(int v, MffcTab &t, const int (&leaves)[4], const int *ref, int *slot) {
-#pragma unroll
-    for (int i = 0; i < 4; i++)
-        if (v == leaves[i]) return 1;
+    if (v == leaves[0] || v == leaves[1] || v == leaves[2] || v == leaves[3]) return 1;
     int found = -1;
-#pragma unroll
-    for (int i = 0; i < 8; i++)
-        if (found < 0 && i < t.size && t.id[i] == v) found = i;
+#define CULS_FIND8(k) \
+    if (found < 0 && k < t.size && t.id[k] == v) found = k;
+    CULS_EACH8(CULS_FIND8)
+#undef CULS_FIND8
     if (found >= 0) {
         int r = 0;
-#pragma unroll
-        for (int i = 0; i < 8; i++)
-            if (i == found) r = --t.num[i];
+#define CULS_DEC8(k) \
+    if (k == found) r = --t.num[k];
+        CULS_EACH8(CULS_DEC8)
+#undef CULS_DEC8
         *slot = found;
         return r;
     }
     if (t.size == 8) return 1;
     const int r = ref[v] - 1;
-#pragma unroll
-    for (int i = 0; i < 8; i++)
-        if (i == t.size) {
-            t.id[i] = v;
-            t.num[i] = r;
-        }
+#define CULS_ADD8(k)    \
+    if (k == t.size) {  \
+        t.id[k] = v;    \
+        t.num[k] = r;   \
+    }
+    CULS_EACH8(CULS_ADD8)
+#undef CULS_ADD8
     *slot = t.size;
     t.size++;
     return r;
 }
 
-// IsDeleted, src/algorithms/rewrite.cu:312-316
-CULS_HD int mffc_deleted(int v, const MffcTab &t) {
-    int del = 0, found = 0;
-#pragma unroll
-    for (int i = 0; i < 8; i++)
-        if (!found && i < t.size && t.id[i] == v) {
-            found = 1;
-            del = t.num[i] == 0;
-        }
+// Bit i set when table entry i exists with a zero count: the entries
+// IsDeleted (src/algorithms/rewrite.cu:312-316) reports.  Table ids are
+// distinct, so the counts are no longer needed once this mask is taken.
+CULS_HD uint32_t mffc_zero_mask(const MffcTab &t) {
+    uint32_t z = 0;
+#define CULS_ZERO8(k) \
+    if (k < t.size && t.num[k] == 0) z |= 1u << k;
+    CULS_EACH8(CULS_ZERO8)
+#undef CULS_ZERO8
+    return z;
+}
+
+// IsDeleted, src/algorithms/rewrite.cu:312-316, on the ids and zero mask
+CULS_HD int mffc_deleted(int v, const int (&id)[8], uint32_t zero) {
+    int del = 0;
+#define CULS_DEL8(k) del |= ((zero >> k) & 1u) && id[k] == v;
+    CULS_EACH8(CULS_DEL8)
+#undef CULS_DEL8
     return del;
 }
 
@@ -565,6 +592,64 @@ CULS_HD int lib_added(const RwLib *lib, int cls, int rt, uint64_t unmatched) {
     return popc64(reach);
 }
 
+// One library node of an evaluation batch (the body of EvaluateNode's node
+// loop, src/algorithms/rewrite.cu:400-428), split in two so that a batch's
+// table probes are in flight together: lib_probe_issue sets the node's level
+// from its fanins and, when both fanins are matched (and not to the root),
+// loads the home slot of its structural-hash key; lib_probe_finish resolves
+// the probe into a match or marks the node unmatched.
+struct LibProbe {
+    unsigned long long key;
+    int4 slot;  // the key's home slot
+    int num;    // library index, or -1 when no probe is pending
+};
+
+CULS_HD void lib_probe_issue(const EvalIn &E, int q, uint32_t w, int isC, int *match, int *mlev, int stride,
+                             uint64_t &unmatched, LibProbe &p) {
+    p.num = -1;
+    if (w == kNoLibNode) return;
+    const int num = (int)((w >> 18) & 63u) + 4;
+    const int in0 = ln_f0(w), in1 = ln_f1(w);
+    const int m0 = match[in0 * stride], m1 = match[in1 * stride];
+    const int lv0 = mlev[in0 * stride], lv1 = mlev[in1 * stride];
+    mlev[num * stride] = 1 + (lv0 > lv1 ? lv0 : lv1);
+    match[num * stride] = -1;
+    const bool uin0 = in0 >= 4 && ((unmatched >> in0) & 1ull);
+    const bool uin1 = in1 >= 4 && ((unmatched >> in1) & 1ull);
+    if (uin0 || uin1 || m0 == q || m1 == q) {
+        unmatched |= 1ull << num;
+        return;
+    }
+    // the reference's isC mask only has input bits (0..3)
+    int cc0 = (in0 < 4 ? ((isC >> in0) & 1) : 0) ^ ln_c0(w);
+    int cc1 = (in1 < 4 ? ((isC >> in1) & 1) : 0) ^ ln_c1(w);
+    int a = m0, b = m1;
+    if (a > b) {  // TableLookup orders the ids
+        const int x = a;
+        a = b;
+        b = x;
+        const int y = cc0;
+        cc0 = cc1;
+        cc1 = y;
+    }
+    p.key = and_key(a, b, cc0, cc1);
+    p.slot = region_load(E.tab, region_home(p.key, E.tab.size));
+    p.num = num;
+}
+
+CULS_HD void lib_probe_finish(const EvalIn &E, const LibProbe &p, const int (&mffcId)[8], uint32_t zero, int *match,
+                              int *mlev, int stride, uint64_t &unmatched) {
+    if (p.num < 0) return;
+    // the slot carries the node's level, so a hit needs no second load
+    const int2 r = region_resolve(E.tab, p.key, p.slot, E.status);
+    if (r.x != -1 && !mffc_deleted(r.x, mffcId, zero)) {
+        match[p.num * stride] = r.x;
+        mlev[p.num * stride] = r.y;
+    } else {
+        unmatched |= 1ull << p.num;
+    }
+}
+
 template <class T>
 CULS_HD T pick4v(const T (&v)[4], int i) {
     return i == 0 ? v[0] : (i == 1 ? v[1] : (i == 2 ? v[2] : v[3]));
@@ -588,6 +673,7 @@ CULS_HD CutBest eval_cut(const EvalIn &E, int q, int cpos, uint32_t pk, int4 l, 
     MffcTab tab;
     tab.size = 0;
     const int saved = mffc_size(E, q, leaves, tab);
+    const uint32_t zero = mffc_zero_mask(tab);
     const uint32_t npn = E.lib->npn[pk & 0xFFFFu];
     const int uPhase = npn_phase(npn), cls = npn_class(npn);
     const uint32_t perm = *reinterpret_cast<const uint32_t *>(E.lib->perm4[npn_perm(npn)]);
@@ -599,45 +685,23 @@ CULS_HD CutBest eval_cut(const EvalIn &E, int q, int cpos, uint32_t pk, int4 l, 
         mlev[j * stride] = E.level[m];
         if (uPhase >> j & 1) isC |= 1 << j;
     }
+    // The library nodes in the reference's index order, regrouped into
+    // batches of equal depth: every node reads only its fanins' entries, so
+    // this order yields the same match, level and unmatched bits.
     uint64_t unmatched = 0;
-    const int nn = E.lib->nNodes[cls];
-    const uint32_t *lnodes = E.lib->node[cls];
-    for (int j = 0; j < nn; j++) {
-        const int num = j + 4;
-        const uint32_t w = lnodes[j];
-        const int in0 = ln_f0(w), in1 = ln_f1(w);
-        const int m0 = match[in0 * stride], m1 = match[in1 * stride];
-        const int lv0 = mlev[in0 * stride], lv1 = mlev[in1 * stride];
-        mlev[num * stride] = 1 + (lv0 > lv1 ? lv0 : lv1);
-        match[num * stride] = -1;
-        const bool uin0 = in0 >= 4 && ((unmatched >> in0) & 1ull);
-        const bool uin1 = in1 >= 4 && ((unmatched >> in1) & 1ull);
-        if (uin0 || uin1 || m0 == q || m1 == q) {
-            unmatched |= 1ull << num;
-            continue;
-        }
-        // the reference's isC mask only has input bits (0..3)
-        int cc0 = (in0 < 4 ? ((isC >> in0) & 1) : 0) ^ ln_c0(w);
-        int cc1 = (in1 < 4 ? ((isC >> in1) & 1) : 0) ^ ln_c1(w);
-        int a = m0, b = m1;
-        if (a > b) {  // TableLookup orders the ids
-            const int x = a;
-            a = b;
-            b = x;
-            const int y = cc0;
-            cc0 = cc1;
-            cc1 = y;
-        }
-        const unsigned long long key = and_key(a, b, cc0, cc1);
-        const uint32_t home = region_home(key, E.tab.size);
-        // the slot carries the node's level, so a hit needs no second load
-        const int2 r = region_resolve(E.tab, key, home, region_load(E.tab, home), E.status);
-        if (r.x != -1 && !mffc_deleted(r.x, tab)) {
-            match[num * stride] = r.x;
-            mlev[num * stride] = r.y;
-        } else {
-            unmatched |= 1ull << num;
-        }
+    const int nb = E.lib->nBatches[cls];
+    const uint4 *lbatch = E.lib->batch[cls];
+    for (int bi = 0; bi < nb; bi++) {
+        const uint4 bw = lbatch[bi];
+        LibProbe p0, p1, p2, p3;  // the batch's probes in flight together
+        lib_probe_issue(E, q, bw.x, isC, match, mlev, stride, unmatched, p0);
+        lib_probe_issue(E, q, bw.y, isC, match, mlev, stride, unmatched, p1);
+        lib_probe_issue(E, q, bw.z, isC, match, mlev, stride, unmatched, p2);
+        lib_probe_issue(E, q, bw.w, isC, match, mlev, stride, unmatched, p3);
+        lib_probe_finish(E, p0, tab.id, zero, match, mlev, stride, unmatched);
+        lib_probe_finish(E, p1, tab.id, zero, match, mlev, stride, unmatched);
+        lib_probe_finish(E, p2, tab.id, zero, match, mlev, stride, unmatched);
+        lib_probe_finish(E, p3, tab.id, zero, match, mlev, stride, unmatched);
     }
     const int nr = E.lib->nRoots[cls];
     for (int out = 0; out < nr; out++) {
