@@ -171,6 +171,7 @@ static bool decode_lib(const unsigned char *b, size_t n, RwLib &L) {
     memset(L.node, 0, sizeof L.node);
     memset(L.roots, 0, sizeof L.roots);
     memset(L.batch, 0xFF, sizeof L.batch);
+    memset(L.rootCone, 0, sizeof L.rootCone);
     for (int c = 0; c < kNumClasses; c++) {
         if (L.nNodes[c] > kMaxLibNodes - 4 || L.nRoots[c] > 16) return false;
         if (!need((size_t)L.nNodes[c] * 4 + L.nRoots[c])) return false;
@@ -208,6 +209,14 @@ static bool decode_lib(const unsigned char *b, size_t n, RwLib &L) {
             }
         }
         L.nBatches[c] = (uint8_t)nb;
+        // root cones over the internal nodes
+        unsigned long long cone[kMaxLibNodes] = {0, 0, 0, 0};
+        for (int i = 0; i < L.nNodes[c]; i++)
+            cone[i + 4] = (1ull << (i + 4)) | cone[ln_f0(L.node[c][i])] | cone[ln_f1(L.node[c][i])];
+        for (int r = 0; r < L.nRoots[c]; r++) {
+            if (L.roots[c][r] >= 4 + L.nNodes[c]) return false;
+            L.rootCone[c][r] = cone[L.roots[c][r]];
+        }
     }
     return cur == n;
 }

@@ -35,6 +35,9 @@ struct RwLib {
     // other, so their table probes are issued together.
     uint4 batch[kNumClasses][kMaxLibNodes];
     uint8_t nBatches[kNumClasses];
+    // Per class and root: bit j set for every internal node j (j >= 4) in
+    // the root's cone, the root included.
+    unsigned long long rootCone[kNumClasses][16];
 };
 constexpr int kLibBatch = 4;
 constexpr uint32_t kNoLibNode = 0xFFFFFFFFu;
@@ -526,6 +529,7 @@ CULS_HD uint32_t mffc_zero_mask(const MffcTab &t) {
 
 // IsDeleted, src/algorithms/rewrite.cu:312-316, on the ids and zero mask
 CULS_HD int mffc_deleted(int v, const int (&id)[8], uint32_t zero) {
+    if (!zero) return 0;  // the common case: the MFFC is the root alone
     int del = 0;
 #define CULS_DEL8(k) del |= ((zero >> k) & 1u) && id[k] == v;
     CULS_EACH8(CULS_DEL8)
@@ -576,20 +580,13 @@ CULS_HD int clz64(uint64_t x) {
 
 // Number of library nodes the subgraph rooted at rt adds: unmatched nodes
 // reachable from rt through unmatched nodes (Eval, rewrite.cu:369-374).
-// unmatched has bit j set for library node j without a match.  Visits only
-// the reached nodes, highest index first.
-CULS_HD int lib_added(const RwLib *lib, int cls, int rt, uint64_t unmatched) {
-    if (!((unmatched >> rt) & 1ull)) return 0;
-    uint64_t reach = 1ull << rt, todo = reach;
-    while (todo) {
-        const int j = 63 - clz64(todo);
-        todo &= ~(1ull << j);
-        const uint32_t w = lib->node[cls][j - 4];
-        const uint64_t nf = ((1ull << ln_f0(w)) | (1ull << ln_f1(w))) & unmatched & ~reach;
-        reach |= nf;
-        todo |= nf;
-    }
-    return popc64(reach);
+// unmatched has bit j set for library node j without a match.  A node is
+// matched only when both its fanins are (inputs always are), so a matched
+// node's whole cone is matched and every unmatched node of rt's cone is
+// reached through unmatched nodes: the count is the unmatched part of the
+// cone.
+CULS_HD int lib_added(const RwLib *lib, int cls, int out, uint64_t unmatched) {
+    return popc64(lib->rootCone[cls][out] & unmatched);
 }
 
 // One library node of an evaluation batch (the body of EvaluateNode's node
@@ -707,7 +704,7 @@ CULS_HD CutBest eval_cut(const EvalIn &E, int q, int cpos, uint32_t pk, int4 l, 
     for (int out = 0; out < nr; out++) {
         const int rt = E.lib->roots[cls][out];
         if (match[rt * stride] == q) continue;
-        const int added = lib_added(E.lib, cls, rt, unmatched);
+        const int added = lib_added(E.lib, cls, out, unmatched);
         const int rtLevel = mlev[rt * stride];
         const int gain = saved - added;
         if (gain < 0 || (gain == 0 && !useZeros)) continue;
