@@ -218,6 +218,10 @@ static bool decode_lib(const unsigned char *b, size_t n, RwLib &L) {
             L.rootCone[c][r] = cone[L.roots[c][r]];
         }
     }
+    int order[kNumClasses];
+    for (int c = 0; c < kNumClasses; c++) order[c] = c;
+    std::stable_sort(order, order + kNumClasses, [&](int a, int b) { return L.nBatches[a] < L.nBatches[b]; });
+    for (int i = 0; i < kNumClasses; i++) L.classSlot[order[i]] = (uint8_t)i;
     return cur == n;
 }
 

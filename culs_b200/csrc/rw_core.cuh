@@ -38,6 +38,10 @@ struct RwLib {
     // Per class and root: bit j set for every internal node j (j >= 4) in
     // the root's cone, the root included.
     unsigned long long rootCone[kNumClasses][16];
+    // Evaluation order of the classes: by number of batches, then class, so
+    // that cut items sorted by this slot put forests of equal batch count
+    // side by side.
+    uint8_t classSlot[kNumClasses];
 };
 constexpr int kLibBatch = 4;
 constexpr uint32_t kNoLibNode = 0xFFFFFFFFu;
@@ -601,7 +605,8 @@ struct LibProbe {
     int num;    // library index, or -1 when no probe is pending
 };
 
-CULS_HD void lib_probe_issue(const EvalIn &E, int q, uint32_t w, int isC, int *match, int *mlev, int stride,
+template <class LevT>
+CULS_HD void lib_probe_issue(const EvalIn &E, int q, uint32_t w, int isC, int *match, LevT *mlev, int stride,
                              uint64_t &unmatched, LibProbe &p) {
     p.num = -1;
     if (w == kNoLibNode) return;
@@ -609,7 +614,7 @@ CULS_HD void lib_probe_issue(const EvalIn &E, int q, uint32_t w, int isC, int *m
     const int in0 = ln_f0(w), in1 = ln_f1(w);
     const int m0 = match[in0 * stride], m1 = match[in1 * stride];
     const int lv0 = mlev[in0 * stride], lv1 = mlev[in1 * stride];
-    mlev[num * stride] = 1 + (lv0 > lv1 ? lv0 : lv1);
+    mlev[num * stride] = (LevT)(1 + (lv0 > lv1 ? lv0 : lv1));
     match[num * stride] = -1;
     const bool uin0 = in0 >= 4 && ((unmatched >> in0) & 1ull);
     const bool uin1 = in1 >= 4 && ((unmatched >> in1) & 1ull);
@@ -634,14 +639,15 @@ CULS_HD void lib_probe_issue(const EvalIn &E, int q, uint32_t w, int isC, int *m
     p.num = num;
 }
 
+template <class LevT>
 CULS_HD void lib_probe_finish(const EvalIn &E, const LibProbe &p, const int (&mffcId)[8], uint32_t zero, int *match,
-                              int *mlev, int stride, uint64_t &unmatched) {
+                              LevT *mlev, int stride, uint64_t &unmatched) {
     if (p.num < 0) return;
     // the slot carries the node's level, so a hit needs no second load
     const int2 r = region_resolve(E.tab, p.key, p.slot, E.status);
     if (r.x != -1 && !mffc_deleted(r.x, mffcId, zero)) {
         match[p.num * stride] = r.x;
-        mlev[p.num * stride] = r.y;
+        mlev[p.num * stride] = (LevT)r.y;
     } else {
         unmatched |= 1ull << p.num;
     }
@@ -662,7 +668,10 @@ struct CutBest {
     int gain, level, out;
 };
 
-CULS_HD CutBest eval_cut(const EvalIn &E, int q, int cpos, uint32_t pk, int4 l, bool useZeros, int *match, int *mlev,
+// LevT holds library-node levels: int, or uint16_t when every level of the
+// graph plus the forest depth stays below 65,535.
+template <class LevT>
+CULS_HD CutBest eval_cut(const EvalIn &E, int q, int cpos, uint32_t pk, int4 l, bool useZeros, int *match, LevT *mlev,
                          int stride) {
     CutBest best{-1, 0, -1};
     const uint32_t nLeaves = packed_nleaves(pk);
@@ -679,7 +688,7 @@ CULS_HD CutBest eval_cut(const EvalIn &E, int q, int cpos, uint32_t pk, int4 l, 
     for (int j = 0; j < 4; j++) {
         const int m = pick4v(leaves, (int)((perm >> (8 * j)) & 255u));
         match[j * stride] = m;
-        mlev[j * stride] = E.level[m];
+        mlev[j * stride] = (LevT)E.level[m];
         if (uPhase >> j & 1) isC |= 1 << j;
     }
     // The library nodes in the reference's index order, regrouped into

@@ -65,60 +65,74 @@ struct EvalArgs {
     uint8_t *candFlag;
 };
 
-// Per-warp shared state of k_evaluate: the warp's 32 nodes' evaluable cuts
-// as items grouped by NPN class, and one result per (node, slot).
+// Per-warp shared state of k_evaluate: the warp's nodes' evaluable cuts as
+// items grouped by class slot, and one result per (node, cut slot).
+// Nodes per lane in a warp's window: two (about 210 cut items to sort per
+// warp instead of 105) fill rounds better but measured slower on the
+// 4,096-graph batch.
+constexpr int kNodesPerLane = 1;
+constexpr int kWarpNodes = 32 * kNodesPerLane;
 struct WarpItems {
-    int off[kClassSlots];    // class counts, then exclusive offsets
-    uint16_t item[32 * 8];   // node lane * 8 + slot, in class order
-    int2 res[32 * 8];        // {gain * 16 + root index, level} or {-1, 0}
+    int off[kClassSlots];          // class-slot counts, then exclusive offsets
+    uint16_t item[kWarpNodes * 8];  // local node * 8 + cut slot, in class-slot order
+    int2 res[kWarpNodes * 8];       // {gain * 16 + root index, level} or {-1, 0}
 };
 
-// A warp takes 32 consecutive nodes of the graph-major order, sorts their
-// evaluable cuts by NPN class and evaluates them 32 at a time, so the lanes
-// of a round mostly walk the same library forest (the forests' sizes differ
-// several-fold between classes).  Each lane then folds its own node's
-// results in slot order, the order of the reference's loop.  Warps never
-// wait for one another.
+// A warp takes 32 * kNodesPerLane consecutive nodes of the graph-major
+// order, sorts their evaluable cuts by NPN class -- classes ordered by their
+// forests' batch counts -- and evaluates them 32 at a time, so the lanes of
+// a round mostly walk the same library forest, or forests of as many
+// batches (the forests' sizes differ several-fold between classes).  Each
+// lane then folds its own nodes' results in slot order, the order of the
+// reference's loop.  Warps never wait for one another.  LevT is the type of
+// the library-node levels in the scratch (16-bit when the graph is shallow
+// enough, which halves that part of the shared memory).
+template <class LevT>
 __global__ void __launch_bounds__(kEvalBlock, 8) k_evaluate(EvalArgs A) {
     __shared__ int s_match[kLibFast * kEvalBlock];
-    __shared__ int s_mlev[kLibFast * kEvalBlock];
+    __shared__ LevT s_mlev[kLibFast * kEvalBlock];
     __shared__ WarpItems s_w[kEvalBlock / 32];
     int *match = s_match + threadIdx.x;
-    int *mlev = s_mlev + threadIdx.x;
+    LevT *mlev = s_mlev + threadIdx.x;
     const int lane = threadIdx.x & 31;
     WarpItems &W = s_w[threadIdx.x >> 5];
     const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
     const int gstride = gridDim.x * blockDim.x;
     int *gmatch = A.scratch + gtid;
-    int *gmlev = A.scratch + (int64_t)kLibSlots * gstride + gtid;
-    const int64_t nWarpChunks = (A.N + 31) / 32;
+    LevT *gmlev = reinterpret_cast<LevT *>(A.scratch + (int64_t)kLibSlots * gstride) + gtid;
+    const int64_t nWarpChunks = (A.N + kWarpNodes - 1) / kWarpNodes;
     const int64_t warpStride = (int64_t)gridDim.x * (kEvalBlock / 32);
     for (int64_t wc = (int64_t)blockIdx.x * (kEvalBlock / 32) + (threadIdx.x >> 5); wc < nWarpChunks;
          wc += warpStride) {
-        const int64_t base = wc * 32;
+        const int64_t base = wc * kWarpNodes;
         for (int c = lane; c < kClassSlots; c += 32) W.off[c] = 0;
         __syncwarp();
-        // 1. this lane's node: its evaluable cuts and their classes
-        int64_t q = -1;
-        if (base + lane < A.N) {
-            q = A.byGraph[base + lane];
-            if (q < A.nL0) q = -1;  // constant or PI
-        }
-        uint32_t clsRank[8];
+        // 1. this lane's nodes: their evaluable cuts and class slots
+        int64_t q[kNodesPerLane];
+        uint32_t clsRank[kNodesPerLane][8];
 #pragma unroll
-        for (int k = 0; k < 8; k++) {
-            clsRank[k] = 0xFFFFFFFFu;
-            W.res[lane * 8 + k] = make_int2(-1, 0);
-            if (q >= 0) {
-                const uint32_t pk = (uint32_t)A.cutM[q * 8 + k].y;
-                if (packed_used(pk) && packed_nleaves(pk) >= 3) {
-                    const int cls = npn_class(A.E.lib->npn[pk & 0xFFFFu]);
-                    clsRank[k] = ((uint32_t)cls << 16) | (uint32_t)atomicAdd(&W.off[cls], 1);
+        for (int h = 0; h < kNodesPerLane; h++) {
+            const int local = h * 32 + lane;
+            q[h] = -1;
+            if (base + local < A.N) {
+                q[h] = A.byGraph[base + local];
+                if (q[h] < A.nL0) q[h] = -1;  // constant or PI
+            }
+#pragma unroll
+            for (int k = 0; k < 8; k++) {
+                clsRank[h][k] = 0xFFFFFFFFu;
+                W.res[local * 8 + k] = make_int2(-1, 0);
+                if (q[h] >= 0) {
+                    const uint32_t pk = (uint32_t)A.cutM[q[h] * 8 + k].y;
+                    if (packed_used(pk) && packed_nleaves(pk) >= 3) {
+                        const int cs = A.E.lib->classSlot[npn_class(A.E.lib->npn[pk & 0xFFFFu])];
+                        clsRank[h][k] = ((uint32_t)cs << 16) | (uint32_t)atomicAdd(&W.off[cs], 1);
+                    }
                 }
             }
         }
         __syncwarp();
-        // 2. exclusive scan of the class counts, kClassSlots / 32 per lane
+        // 2. exclusive scan of the class-slot counts, kClassSlots / 32 per lane
         int v[kClassSlots / 32], sum = 0;
 #pragma unroll
         for (int t = 0; t < kClassSlots / 32; t++) {
@@ -141,11 +155,14 @@ __global__ void __launch_bounds__(kEvalBlock, 8) k_evaluate(EvalArgs A) {
         }
         __syncwarp();
 #pragma unroll
-        for (int k = 0; k < 8; k++)
-            if (clsRank[k] != 0xFFFFFFFFu)
-                W.item[W.off[clsRank[k] >> 16] + (clsRank[k] & 0xFFFFu)] = (uint16_t)(lane * 8 + k);
+        for (int h = 0; h < kNodesPerLane; h++)
+#pragma unroll
+            for (int k = 0; k < 8; k++)
+                if (clsRank[h][k] != 0xFFFFFFFFu)
+                    W.item[W.off[clsRank[h][k] >> 16] + (clsRank[h][k] & 0xFFFFu)] =
+                        (uint16_t)((h * 32 + lane) * 8 + k);
         __syncwarp();
-        // 3. evaluate the items, 32 per round, in class order
+        // 3. evaluate the items, 32 per round, in class-slot order
         for (int it = lane; it < nItems; it += 32) {
             const int slot = W.item[it];
             const int qq = A.byGraph[base + (slot >> 3)];
@@ -164,17 +181,20 @@ __global__ void __launch_bounds__(kEvalBlock, 8) k_evaluate(EvalArgs A) {
             if (b.out >= 0) W.res[slot] = make_int2(b.gain * 16 + b.out, b.level);
         }
         __syncwarp();
-        // 4. fold this lane's node's cuts in slot order
-        if (q >= 0) {
+        // 4. fold each of this lane's nodes' cuts in slot order
+#pragma unroll
+        for (int h = 0; h < kNodesPerLane; h++) {
+            if (q[h] < 0) continue;
+            const int local = h * 32 + lane;
             int bc = -1, bo = -1, gain = 0, level = 0;
 #pragma unroll
             for (int k = 0; k < 8; k++) {
-                const int2 r = W.res[lane * 8 + k];
+                const int2 r = W.res[local * 8 + k];
                 if (r.x >= 0) fold_cut_best(CutBest{r.x >> 4, r.y, r.x & 15}, k, bc, bo, gain, level);
             }
-            A.bestCut[q] = (int8_t)bc;
-            A.bestOut[q] = (uint8_t)(bo < 0 ? 0 : bo);
-            A.candFlag[q] = bc >= 0;
+            A.bestCut[q[h]] = (int8_t)bc;
+            A.bestOut[q[h]] = (uint8_t)(bo < 0 ? 0 : bo);
+            A.candFlag[q[h]] = bc >= 0;
         }
         __syncwarp();
     }
@@ -218,7 +238,12 @@ int rw_evaluate(ExecCtx &X, RwWork &w, const Batch &b) {
         EvalArgs A{w.nL0, N, w.byGraph, scratch, EvalIn{w.w0, w.w1, w.ref, w.wlev, X.lib, TabRegion{}, X.status}, w.tab,
                    w.cutL, w.cutM, w.wg, w.dg, w.useZeros ? 1 : 0, w.bestCut, w.bestOut, candFlag};
         X.mark(kMkEvalK0);
-        k_evaluate<<<evalGrid, kEvalBlock, 0, s>>>(A);
+        // 16-bit library levels when no level of the batch, plus a forest's
+        // depth (at most 50 nodes), can reach 65,535
+        if (w.maxLevel + 64 < 0xFFFF)
+            k_evaluate<uint16_t><<<evalGrid, kEvalBlock, 0, s>>>(A);
+        else
+            k_evaluate<int><<<evalGrid, kEvalBlock, 0, s>>>(A);
         X.mark(kMkEvalK1);
         X.launched(3);
     }

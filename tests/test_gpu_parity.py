@@ -248,6 +248,28 @@ def test_invalid_graph_rejected(ctx):
     assert e.value.code == -1
 
 
+def test_graph_deeper_than_16_bit_levels_matches_oracle():
+    """A graph over 65,535 levels deep, alone and inside a batch of shallow
+    ones: evaluation keeps library-node levels in 32 bits there (16 bits
+    otherwise), with the same results."""
+    deep = C.gen_layered(31, 8, 4, 200000, 100000, 2, 0.0, True)  # 96k ANDs, depth 70,687
+    shallow = C.gen_batch(4, 500, 3, 1000, 20000, 16, 256, threads=8)
+    c = C.Context()
+    try:
+        d = c.upload(deep)
+        c.rw_st(d)
+        ref = oracle_rw_st(deep).graph()
+        out = d.download()
+        assert same_graph(out, ref)
+        assert out.nLevels == ref.nLevels
+        db = c.upload_batch(shallow + [deep])
+        c.rw_st(db)
+        for i, g in enumerate(shallow + [deep]):
+            assert same_graph(db.download(i), oracle_rw_st(g).graph()), i
+    finally:
+        c.close()
+
+
 @pytest.mark.parametrize("wide_min", [1, 1 << 30])
 def test_both_enumeration_schedules_match_oracle(wide_min):
     """Every level on one thread per node (1), or every level on one warp per
