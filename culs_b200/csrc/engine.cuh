@@ -77,14 +77,30 @@ struct Batch {
     // spare fanin/PO buffers: strash writes its output there and swaps
     int *F0s = nullptr, *F1s = nullptr, *POs = nullptr;
     int64_t capObjS = 0, capPOS = 0;
+    // The rewrite manager's graph left by a rewrite with CPU deduplication
+    // (AIGMan::prevCmdRewrite, src/aig_manager.cu:654-662): every node of the
+    // rewritten graph in the manager's numbering, duplicates and dangling
+    // nodes included.  The next rewrite starts from it instead of from the
+    // deduplicated graph; a strash -- st, or a rewrite's GPU deduplication --
+    // drops it (src/aig/strash.cu:498).
+    bool keep = false;
+    int *F0k = nullptr, *F1k = nullptr, *POk = nullptr;
+    int64_t capObjK = 0, capPOK = 0, nObjK = 0;
+    std::vector<DevGraph> hgk;
     std::shared_ptr<DevPool> pool;  // where the buffers come from and go back to (null: cudaMalloc)
     ~Batch();
     void release();
     // Grows the buffers to hold nObj objects, nPO POs and G graphs (their
-    // contents are not kept); allocates nothing when they are large enough.
+    // contents are not kept, nor is the kept rewrite state); allocates
+    // nothing when they are large enough.
     cudaError_t reserve(int64_t nObj, int64_t nPO, int G);
     cudaError_t reserve_spare(int64_t nObj, int64_t nPO);
     void swap_spare();
+    // Copies the current graph into the kept buffers and sets keep.
+    cudaError_t keep_current(cudaStream_t s);
+    // Makes the kept graph current (the current one is discarded) and clears
+    // keep; the caller uploads hg to dg.
+    void restore_kept();
 };
 
 // Per-node dumps of the last rw (for parity checks); indexed by the graph's
@@ -176,8 +192,12 @@ class Engine {
     // graph's constant position.  Replaces b's arrays with the result.
     // topo: positions are topological and b's graph-major layout (levels by
     // an in-order dataflow instead of a worklist).
+    // unique: every node is its own representative (no duplicate merged):
+    // the output is the input graph renumbered in processing order.
     int strash_core(Batch &b, int64_t M, const int *L0, const int *L1, const int *gid, const int *lid, const int *po,
-                    bool idOrder, bool removeDangling, bool foldTrivial, bool topo);
+                    bool idOrder, bool removeDangling, bool foldTrivial, bool topo, bool unique = false);
+    // strash_core over b's own graph-major arrays (the body of st).
+    int strash_batch(Batch &b, bool idOrder, bool removeDangling, bool foldTrivial);
 
     std::string err_;
     cudaStream_t s_ = nullptr;

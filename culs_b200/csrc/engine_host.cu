@@ -114,6 +114,12 @@ void Batch::release() {
     drop(pool, F0s, sizeof(int) * (size_t)capObjS);
     drop(pool, F1s, sizeof(int) * (size_t)capObjS);
     drop(pool, POs, sizeof(int) * (size_t)capPOS);
+    drop(pool, F0k, sizeof(int) * (size_t)capObjK);
+    drop(pool, F1k, sizeof(int) * (size_t)capObjK);
+    drop(pool, POk, sizeof(int) * (size_t)capPOK);
+    capObjK = capPOK = nObjK = 0;
+    keep = false;
+    hgk.clear();
     capObj = capPO = capObjS = capPOS = 0;
     capG = 0;
     G = 0;
@@ -122,6 +128,7 @@ void Batch::release() {
 }
 
 cudaError_t Batch::reserve(int64_t n, int64_t np, int g) {
+    keep = false;  // a new graph is written: no rewrite state carries over
     int64_t c0 = capObj, c1 = capObj, cg = capG;
     cudaError_t e;
     if ((e = grow(pool, F0, c0, n)) != cudaSuccess) return e;
@@ -140,6 +147,33 @@ cudaError_t Batch::reserve_spare(int64_t n, int64_t np) {
     if ((e = grow(pool, F1s, c1, n)) != cudaSuccess) return e;
     capObjS = std::min(c0, c1);
     return grow(pool, POs, capPOS, np);
+}
+
+cudaError_t Batch::keep_current(cudaStream_t s) {
+    int64_t c0 = capObjK, c1 = capObjK;
+    cudaError_t e;
+    if ((e = grow(pool, F0k, c0, nObj)) != cudaSuccess) return e;
+    if ((e = grow(pool, F1k, c1, nObj)) != cudaSuccess) return e;
+    capObjK = std::min(c0, c1);
+    if ((e = grow(pool, POk, capPOK, nPO)) != cudaSuccess) return e;
+    if (nObj && (e = cudaMemcpyAsync(F0k, F0, sizeof(int) * nObj, cudaMemcpyDeviceToDevice, s))) return e;
+    if (nObj && (e = cudaMemcpyAsync(F1k, F1, sizeof(int) * nObj, cudaMemcpyDeviceToDevice, s))) return e;
+    if (nPO && (e = cudaMemcpyAsync(POk, PO, sizeof(int) * nPO, cudaMemcpyDeviceToDevice, s))) return e;
+    hgk = hg;
+    nObjK = nObj;
+    keep = true;
+    return cudaSuccess;
+}
+
+void Batch::restore_kept() {
+    std::swap(F0, F0k);
+    std::swap(F1, F1k);
+    std::swap(PO, POk);
+    std::swap(capObj, capObjK);
+    std::swap(capPO, capPOK);
+    hg = hgk;
+    nObj = nObjK;
+    keep = false;
 }
 
 void Batch::swap_spare() {
@@ -395,8 +429,17 @@ __global__ void k_st_po(int64_t nPO, int G, const DevGraph *dg, const int *PO, i
 }  // namespace
 
 int Engine::st(Batch &b, bool cpuOrder) {
-    const int64_t N = b.nObj;
     if (prof_) mark(kMkStStart);
+    // `st` = GPU strash (frontier order, trivial folding); `st -c` = CPU strash
+    // (id order, no folding), both with dangling removal
+    const int rc = strash_batch(b, cpuOrder, true, !cpuOrder);
+    if (prof_) mark(kMkStEnd);
+    return rc;
+}
+
+int Engine::strash_batch(Batch &b, bool idOrder, bool removeDangling, bool foldTrivial) {
+    const int64_t N = b.nObj;
+    b.keep = false;  // a strash ends the rewrite manager's state (src/aig/strash.cu:498)
     int rc;
     if ((rc = ensure_arena((size_t)N * 160 + (size_t)b.nPO * 8 + ((size_t)64 << 20)))) return rc;
     ar_.reset();
@@ -410,11 +453,7 @@ int Engine::st(Batch &b, bool cpuOrder) {
     k_st_prep<<<X.grid(N), kBlock, 0, s_>>>(N, b.G, b.dg, b.F0, b.F1, L0, L1, gid, lid);
     if (b.nPO) k_st_po<<<X.grid(b.nPO), kBlock, 0, s_>>>(b.nPO, b.G, b.dg, b.PO, po);
     launches_ += 2;
-    // `st` = GPU strash (frontier order, trivial folding); `st -c` = CPU strash
-    // (id order, no folding), both with dangling removal
-    rc = strash_core(b, N, L0, L1, gid, lid, po, cpuOrder, true, !cpuOrder, true);
-    if (prof_) mark(kMkStEnd);
-    return rc;
+    return strash_core(b, N, L0, L1, gid, lid, po, idOrder, removeDangling, foldTrivial, true);
 }
 
 }  // namespace culs

@@ -54,8 +54,14 @@ int Engine::rw(Batch &b, bool useZeros, bool gpuDedup, RwStats *stats, RwDump *d
     bool anyAnd = false;
     for (auto &g : b.hg) anyAnd |= g.nAnds > 0;
     if (!anyAnd) return 0;  // AIGMan::rewrite returns at once without AND nodes
-    const int64_t N = b.nObj;
     int rc;
+    if (b.keep) {  // the previous command was a rewrite: no Reset (src/aig_manager.cu:654-655)
+        b.restore_kept();
+        if ((rc = check(cudaMemcpyAsync(b.dg, b.hg.data(), sizeof(DevGraph) * b.G, cudaMemcpyHostToDevice, s_),
+                        "h2d")))
+            return rc;
+    }
+    const int64_t N = b.nObj;
     if ((rc = ensure_arena((size_t)N * 640 + (size_t)b.nPO * 16 + ((size_t)256 << 20)))) return rc;
     ar_.reset();
     ExecCtx X = ctx();
@@ -136,8 +142,22 @@ int Engine::rw(Batch &b, bool useZeros, bool gpuDedup, RwStats *stats, RwDump *d
     k_rw_to_aigman<<<X.grid(std::max<int64_t>(M, b.nPO)), kBlock, 0, s_>>>(N, M, w.wlev, w.gidAll, w.dg, w.L0, w.L1, o0,
                                                                            o1, b.nPO, w.wpo, opo);
     launches_ += 1;
-    // updateFromRewriteManager(2) -> GPU strash; (1) -> CPU deduplicate
-    rc = strash_core(b, M, o0, o1, w.gidAll, w.wl, opo, false, gpuDedup, gpuDedup, false);
+    if (gpuDedup) {
+        // updateFromRewriteManager(2): GPU strash, which also ends the
+        // rewrite manager's state (src/aig_manager.cu:523-546)
+        rc = strash_core(b, M, o0, o1, w.gidAll, w.wl, opo, false, true, true, false);
+        b.keep = false;
+    } else {
+        // updateFromRewriteManager(1): the manager's graph (every node, in
+        // its final Reorder numbering) is kept for a following rewrite, then
+        // deduplicated in id order (src/aig_manager.cu:454-522)
+        rc = strash_core(b, M, o0, o1, w.gidAll, w.wl, opo, false, false, false, false, true);
+        if (!rc) rc = check(b.keep_current(s_), "keep");
+        if (!rc) {
+            rc = strash_batch(b, false, false, false);
+            b.keep = rc == 0;
+        }
+    }
     X.mark(kMkRwEnd);
     return rc;
 }

@@ -304,6 +304,7 @@ struct DedupArgs {
     int *mapEnc;  // per position: mapped literal (>= 0) or -(slot+1)
     int *kl0, *kl1;
     int foldTrivial;
+    int unique;  // key each node by its position: nothing merges
     int *counter;
     int *status;
 };
@@ -407,7 +408,10 @@ __global__ void __launch_bounds__(kDedupChunk) k_dedup(DedupArgs A) {
             if (triv >= 0) {
                 A.mapEnc[v] = triv;
             } else {
-                unsigned long long key = ((unsigned long long)(uint32_t)l0 << 32) | (uint32_t)l1;
+                // literals are non-negative, so a key with the top bit set
+                // is never a real one
+                const unsigned long long key = A.unique ? (1ull << 63) | (unsigned long long)(uint32_t)v
+                                                        : ((unsigned long long)(uint32_t)l0 << 32) | (uint32_t)l1;
                 int slot = table_insert(A.tab, key, A.rankOf[v], A.status);
                 A.kl0[t] = l0;
                 A.kl1[t] = l1;
@@ -502,7 +506,8 @@ __global__ void k_strash_out(int64_t nW, const int *wl, OutArgs A) {
 }  // namespace
 
 int Engine::strash_core(Batch &b, int64_t M, const int *L0, const int *L1, const int *gidA, const int *lidIn,
-                        const int *po, bool idOrder, bool removeDangling, bool foldTrivial, bool topo) {
+                        const int *po, bool idOrder, bool removeDangling, bool foldTrivial, bool topo,
+                        bool unique) {
     const int G = b.G;
     const int64_t nPO = b.nPO;
     cudaStream_t s = s_;
@@ -640,8 +645,8 @@ int Engine::strash_core(Batch &b, int64_t M, const int *L0, const int *L1, const
                     L0,         L1,       level,   lvlCnt,
                     lvlStart,   chunkStart, maxLevel, lvlDone,
                     gidA,       b.dg,     AndTable{tk, tv, cap - 1}, mapEnc,
-                    kl0,        kl1,      foldTrivial ? 1 : 0, qc + 5,
-                    status_};
+                    kl0,        kl1,      foldTrivial ? 1 : 0, unique ? 1 : 0,
+                    qc + 5,     status_};
         if (prof_) this->mark(kMkDedupK0);
         k_dedup<<<(unsigned)(sms_ * 8), kBlock, 0, s>>>(A);
         if (prof_) this->mark(kMkDedupK1);

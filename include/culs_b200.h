@@ -114,7 +114,13 @@ int culs_batch_download_into(culs_ctx *ctx, const culs_graph *g, int32_t *const 
 
 /* `rw` on every graph of the handle: AIGMan::rewrite(fUseZeros,
  * fGPUDeduplicate) (CULS src/aig_manager.cu:632-672, command handler
- * src/command_manager.cpp:81-95). */
+ * src/command_manager.cpp:81-95).  Without CULS_RW_GPU_DEDUP (the
+ * ABC-patch `grw` default) the handle also keeps the rewrite manager's graph
+ * -- every node of the rewritten graph before deduplication -- and the next
+ * culs_rw on it starts from that graph, as the reference skips its Reset
+ * after a rewrite (src/aig_manager.cu:654-662).  culs_st, a rewrite with
+ * CULS_RW_GPU_DEDUP (whose deduplication is a strash, src/aig/strash.cu:498)
+ * and writing a new graph into the handle drop it. */
 int culs_rw(culs_ctx *ctx, culs_graph *g, uint32_t flags);
 /* `st` on every graph of the handle: AIGMan::strash(fCPU)
  * (src/aig/strash.cu:317-503, handler src/command_manager.cpp:115-128). */

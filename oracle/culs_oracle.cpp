@@ -1081,6 +1081,12 @@ struct Oracle {
     Graph g;
     Solver s;
     Graph preDedup;
+    // AIGMan::prevCmdRewrite (src/aig_manager.h:97): the solver still holds
+    // the last rewrite's graph, so the next rewrite starts from it instead
+    // of resetting from g.  Set by every rewrite (aig_manager.cu:662) and
+    // cleared by a strash (src/aig/strash.cu:498) -- the GPU deduplication
+    // of a rewrite is one -- and by reading a graph (aig_manager.cu:101).
+    bool keepRw = false;
     std::string err;
 };
 
@@ -1107,6 +1113,7 @@ void orc_destroy(void *h) { delete (Oracle *)h; }
 int orc_set_graph(void *h, int nPIs, int nPOs, int nAnds, const int *f0, const int *f1, const int *outs) {
     Oracle *o = (Oracle *)h;
     orc::Graph &g = o->g;
+    o->keepRw = false;
     g.nPIs = nPIs;
     g.nPOs = nPOs;
     g.nObjs = 1 + nPIs + nAnds;
@@ -1138,7 +1145,7 @@ int orc_rw(void *h, int fUseZeros, int dedupMode) {
     orc::Graph &g = o->g;
     if (g.nObjs - 1 - g.nPIs == 0) return 0;  // rewrite: nothing to do
     orc::Solver &s = o->s;
-    s.reset(g);
+    if (!o->keepRw) s.reset(g);  // src/aig_manager.cu:654-655
     s.rewrite(fUseZeros != 0);
     // updateFromRewriteManager, src/aig_manager.cu:432-564
     orc::Graph r;
@@ -1161,6 +1168,7 @@ int orc_rw(void *h, int fUseZeros, int dedupMode) {
         g = orc::dedup_cpu(r);
     else
         g = r;
+    o->keepRw = dedupMode != 2;
     return 0;
 }
 
@@ -1168,6 +1176,7 @@ int orc_rw(void *h, int fUseZeros, int dedupMode) {
 int orc_st(void *h, int fCPU) {
     Oracle *o = (Oracle *)h;
     o->g = fCPU ? orc::strash_cpu(o->g) : orc::strash_gpu(o->g);
+    o->keepRw = false;
     return 0;
 }
 

@@ -8,6 +8,11 @@
 //       AIGMan::readFile; AIGMan::rewrite(zeros, true); AIGMan::strash();
 //       AIGMan::saveFile -- the sequence of `read; rw [-z]; st; write`
 //       (command handlers src/command_manager.cpp:32-128).
+//   rw_harness chain <in.aig> <out.aig> <script>
+//       a command sequence on one AIGMan, script = comma-separated tokens
+//       rw | rwz | rwc | rwzc | st: AIGMan::rewrite(zeros = 'z',
+//       fGPUDeduplicate = no 'c') or AIGMan::strash(false, true), printing
+//       the AND count and level after each, then AIGMan::saveFile.
 //   rw_harness dump <in.aig> <prefix>
 //       the first half of rw::CPUSolver::Rewrite (src/algorithms/
 //       rewrite.cu:811-826) step by step, writing the reordered fanins, all
@@ -116,6 +121,29 @@ static int run_full(const char *in, const char *out, bool zeros) {
     return 0;
 }
 
+static int run_chain(const char *in, const char *out, const char *script) {
+    AIGMan man;
+    if (!man.readFile(in)) return 2;
+    std::stringstream ss(script);
+    std::string tok;
+    while (std::getline(ss, tok, ',')) {
+        if (tok == "st") {
+            man.strash(false, true);
+        } else if (tok.rfind("rw", 0) == 0) {
+            const bool zeros = tok.find('z') != std::string::npos;
+            const bool gpuDedup = tok.find('c') == std::string::npos;
+            man.rewrite(zeros, gpuDedup);
+        } else {
+            fprintf(stderr, "chain: unknown command %s\n", tok.c_str());
+            return 4;
+        }
+        printf("HARNESS after %s: and = %d level = %d\n", tok.c_str(), man.nNodes, man.nLevels);
+    }
+    man.saveFile(out);
+    fflush(stdout);
+    return 0;
+}
+
 // The reference's own rw;st timed per graph (its GPU path, one AIG at a
 // time): read each file, then time AIGMan::rewrite + AIGMan::strash with a
 // device synchronisation on both sides; best of `reps` runs per file after
@@ -149,6 +177,7 @@ int main(int argc, char **argv) {
     if (argc >= 5 && !strcmp(argv[1], "full")) return run_full(argv[2], argv[3], atoi(argv[4]) != 0);
     if (argc >= 4 && !strcmp(argv[1], "time")) return run_time(atoi(argv[2]), argc - 3, argv + 3);
     if (argc >= 4 && !strcmp(argv[1], "dump")) return run_dump(argv[2], argv[3]);
+    if (argc >= 5 && !strcmp(argv[1], "chain")) return run_chain(argv[2], argv[3], argv[4]);
     fprintf(stderr, "usage: rw_harness full <in.aig> <out.aig> <zeros> | dump <in.aig> <prefix>\n");
     return 1;
 }
