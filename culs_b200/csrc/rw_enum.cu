@@ -331,8 +331,11 @@ __device__ __forceinline__ void enum_node_warp(const EnumArgs &A, int64_t q, int
 }
 
 // One node on one thread (wide levels): the slots in registers, the
-// admissible pairs visited in order.
-__device__ __forceinline__ void enum_node_thread(const EnumArgs &A, int64_t q) {
+// admissible pairs visited in order.  All lanes of the warp call it (valid:
+// the lane has a node) and run as many rounds as the lane with the most
+// admissible pairs, one pair per round and back in step after each, so
+// lanes that finish a pair early do not drift into later pairs alone.
+__device__ __forceinline__ void enum_node_thread(const EnumArgs &A, int64_t q, bool valid) {
     Slot S[8];
 #pragma unroll
     for (int k = 0; k < 8; k++) {
@@ -340,7 +343,7 @@ __device__ __forceinline__ void enum_node_thread(const EnumArgs &A, int64_t q) {
         S[k].sign = 0;
         S[k].l[0] = S[k].l[1] = S[k].l[2] = S[k].l[3] = 0;
     }
-    {
+    if (valid) {
         Cut c;
         c.sign = 1u << A.lidLow[q];
         c.tt = 0xAAAAu;
@@ -352,16 +355,16 @@ __device__ __forceinline__ void enum_node_thread(const EnumArgs &A, int64_t q) {
         S[0].pk = cut_pack(c);
         A.cutA[q * 8] = make_int2((int)clamp_ref(A.ref[q]), (int)((uint32_t)A.lidLow[q] << 12));
     }
-    const int f0 = A.w0[q], f1 = A.w1[q];
+    const int f0 = valid ? A.w0[q] : 0, f1 = valid ? A.w1[q] : 0;
     const int u0 = f0 >> 1, u1 = f1 >> 1, c0 = f0 & 1, c1 = f1 & 1;
-    bool ok = wait_ge(&A.done[u0], 1, A.status) && wait_ge(&A.done[u1], 1, A.status);
+    bool ok = valid && wait_ge(&A.done[u0], 1, A.status) && wait_ge(&A.done[u1], 1, A.status);
+    uint64_t pairs = 0;
+    const int2 *M0 = A.cutM + (int64_t)u0 * 8, *M1 = A.cutM + (int64_t)u1 * 8;
     if (ok) {
-        const int2 *M0 = A.cutM + (int64_t)u0 * 8, *M1 = A.cutM + (int64_t)u1 * 8;
         // the pairs CutEnumerate tries (both slots used, at most 4 leaves
         // by signature), bit i * 8 + j: visiting the set bits in order is
         // the reference's i-major loop, and every lane takes its k-th pair
         // in the same iteration
-        uint64_t pairs = 0;
         {
             uint32_t s1[8], used1 = 0;
 #pragma unroll
@@ -380,11 +383,16 @@ __device__ __forceinline__ void enum_node_thread(const EnumArgs &A, int64_t q) {
                         pairs |= 1ull << (i * 8 + j);
             }
         }
-        while (pairs) {
+    }
+    // every lane runs the warp's largest number of admissible pairs, in step;
+    // `continue` in the do-while below ends the lane's current pair
+    const int rounds = __reduce_max_sync(0xffffffffu, (unsigned)popc64(pairs));
+    for (int t = 0; t < rounds; t++) {
+        if (pairs) {
             const int p = __ffsll((long long)pairs) - 1;
             pairs &= pairs - 1;
             const int i = p >> 3, j = p & 7;
-            {
+            do {
                 RCut a, b;
                 load_rcut(A, (int64_t)u0 * 8 + i, M0[i], a);
                 load_rcut(A, (int64_t)u1 * 8 + j, M1[j], b);
@@ -440,9 +448,11 @@ __device__ __forceinline__ void enum_node_thread(const EnumArgs &A, int64_t q) {
                 for (int k = 0; k < 8; k++)
                     if (k == id) S[k].pk = cut_pack(pc);
                 if (m.n < 2) pairs = 0;  // enumeration of this node stops (rewrite.cu:291)
-            }
+            } while (false);
         }
+        __syncwarp();
     }
+    if (!valid) return;
 #pragma unroll
     for (int k = 0; k < 8; k++) {
         A.cutL[q * 8 + k] = make_int4(S[k].l[0], S[k].l[1], S[k].l[2], S[k].l[3]);
@@ -479,7 +489,7 @@ __global__ void __launch_bounds__(kEnumBlock, 3) k_enumerate(EnumArgs A) {
         const int64_t k = c - A.chunkStart[lo];
         if (w >= A.wideMin) {
             const int64_t q = base + k * 32 + lane;
-            if (q < base + w) enum_node_thread(A, q);
+            enum_node_thread(A, q, q < base + w);
         } else {
             enum_node_warp(A, base + k, lane);
         }
