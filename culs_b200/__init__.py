@@ -60,6 +60,7 @@ _lib.culs_batch_upload.argtypes = [_vp, ctypes.c_int, ctypes.POINTER(_HostGraph)
 _lib.culs_graph_free.argtypes = [_vp]
 _lib.culs_graph_count.argtypes = [_vp]
 _lib.culs_graph_stats.argtypes = [_vp, ctypes.c_int, _ip, _ip, _ip, _ip]
+_lib.culs_batch_stats.argtypes = [_vp, _ip, _ip, _ip, _ip]
 _lib.culs_batch_download.argtypes = [_vp, _vp, ctypes.POINTER(_HostGraph)]
 _lib.culs_batch_download_into.argtypes = [_vp, _vp, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
 _lib.culs_set_param.argtypes = [_vp, ctypes.c_int, ctypes.c_int64]
@@ -124,11 +125,17 @@ class Aig:
         return len(self.outs)
 
     def host(self):
-        """A culs_host_graph view (keeps references to the arrays)."""
+        """A culs_host_graph view (keeps references to the arrays); built
+        once and reused while the three arrays stay the same objects."""
+        c = self.__dict__.get("_hostc")
+        if c is not None and c[0] is self.fanin0 and c[1] is self.fanin1 and c[2] is self.outs and c[3] == self.nPIs:
+            return c[4]
         self.fanin0 = np.ascontiguousarray(self.fanin0, dtype=np.int32)
         self.fanin1 = np.ascontiguousarray(self.fanin1, dtype=np.int32)
         self.outs = np.ascontiguousarray(self.outs, dtype=np.int32)
-        return _HostGraph(self.nPIs, self.nPOs, self.nAnds, _p(self.fanin0), _p(self.fanin1), _p(self.outs))
+        h = _HostGraph(self.nPIs, self.nPOs, self.nAnds, _p(self.fanin0), _p(self.fanin1), _p(self.outs))
+        self.__dict__["_hostc"] = (self.fanin0, self.fanin1, self.outs, self.nPIs, h)
+        return h
 
 
 def _take(h: _HostGraph) -> Aig:
@@ -355,18 +362,33 @@ class DeviceGraphs:
         _check(_lib.culs_graph_stats(self.h, i, *[ctypes.byref(x) for x in v]), "stats")
         return dict(zip(["nPIs", "nPOs", "nAnds", "nLevels"], [x.value for x in v]))
 
-    def download_all(self):
-        """Every graph of the handle as an Aig, in one transfer."""
+    def stats_all(self):
+        """nPIs, nPOs, nAnds, nLevels of every graph, as int32 arrays."""
         n = len(self)
-        st = [self.stats(i) for i in range(n)]
-        f0 = [np.empty(1 + s["nPIs"] + s["nAnds"], np.int32) for s in st]
-        f1 = [np.empty(1 + s["nPIs"] + s["nAnds"], np.int32) for s in st]
-        po = [np.empty(max(s["nPOs"], 1), np.int32) for s in st]
-        P = ctypes.POINTER(ctypes.c_int32) * n
-        ptrs = [P(*[_p(a) for a in arrs]) for arrs in (f0, f1, po)]
-        self.ctx._err(_lib.culs_batch_download_into(self.ctx.h, self.h, *[ctypes.cast(x, ctypes.c_void_p) for x in ptrs]),
+        v = [np.empty(max(n, 1), np.int32) for _ in range(4)]
+        _check(_lib.culs_batch_stats(self.h, *[_p(x) for x in v]), "stats")
+        return dict(zip(["nPIs", "nPOs", "nAnds", "nLevels"], [x[:n] for x in v]))
+
+    def download_all(self):
+        """Every graph of the handle as an Aig, in one transfer (the graphs'
+        arrays are views of three buffers)."""
+        n = len(self)
+        st = self.stats_all()
+        nobj = 1 + st["nPIs"].astype(np.int64) + st["nAnds"]
+        npo = st["nPOs"].astype(np.int64)
+        o0 = np.zeros(n + 1, np.int64)
+        np.cumsum(nobj, out=o0[1:])
+        p0 = np.zeros(n + 1, np.int64)
+        np.cumsum(npo, out=p0[1:])
+        F0 = np.empty(max(int(o0[-1]), 1), np.int32)
+        F1 = np.empty(max(int(o0[-1]), 1), np.int32)
+        PO = np.empty(max(int(p0[-1]), 1), np.int32)
+        ptrs = [np.ascontiguousarray(B.ctypes.data + 4 * off[:n], dtype=np.uint64) for B, off in ((F0, o0), (F1, o0), (PO, p0))]
+        self.ctx._err(_lib.culs_batch_download_into(self.ctx.h, self.h, *[x.ctypes.data_as(ctypes.c_void_p) for x in ptrs]),
                       "batch download")
-        return [Aig(s["nPIs"], f0[i], f1[i], po[i][:s["nPOs"]], s["nLevels"]) for i, s in enumerate(st)]
+        nP, nL = st["nPIs"].tolist(), st["nLevels"].tolist()
+        a, b = o0.tolist(), p0.tolist()
+        return [Aig(nP[i], F0[a[i]:a[i + 1]], F1[a[i]:a[i + 1]], PO[b[i]:b[i + 1]], nL[i]) for i in range(n)]
 
     def download(self, i=0) -> Aig:
         s = self.stats(i)

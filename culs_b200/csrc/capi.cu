@@ -117,6 +117,18 @@ int culs_graph_stats(const culs_graph *g, int index, int32_t *nPIs, int32_t *nPO
     return CULS_OK;
 }
 
+int culs_batch_stats(const culs_graph *g, int32_t *nPIs, int32_t *nPOs, int32_t *nAnds, int32_t *nLevels) {
+    if (!g) return CULS_E_INVALID;
+    for (int i = 0; i < g->b.G; i++) {
+        const culs::DevGraph &d = g->b.hg[i];
+        if (nPIs) nPIs[i] = d.nPIs;
+        if (nPOs) nPOs[i] = d.nPOs;
+        if (nAnds) nAnds[i] = d.nAnds;
+        if (nLevels) nLevels[i] = d.nLevels;
+    }
+    return CULS_OK;
+}
+
 int culs_graph_download(culs_ctx *ctx, const culs_graph *g, int index, int32_t *fanin0, int32_t *fanin1,
                         int32_t *outs) {
     if (!ctx || !g) return CULS_E_INVALID;

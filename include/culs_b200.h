@@ -95,6 +95,9 @@ void culs_graph_free(culs_graph *g);
 int culs_graph_count(const culs_graph *g);
 /* Sizes and level of graph `index` (AIGMan::printStats, src/aig_manager.cu:604-612). */
 int culs_graph_stats(const culs_graph *g, int index, int32_t *nPIs, int32_t *nPOs, int32_t *nAnds, int32_t *nLevels);
+/* culs_graph_stats for every graph of the handle at once: arrays of
+ * culs_graph_count(g) entries (a null array is skipped). */
+int culs_batch_stats(const culs_graph *g, int32_t *nPIs, int32_t *nPOs, int32_t *nAnds, int32_t *nLevels);
 /* Copies graph `index` back (AIGMan::toHost, src/aig_manager.cu:314-336);
  * fanin arrays need 1 + nPIs + nAnds entries, outs nPOs. */
 int culs_graph_download(culs_ctx *ctx, const culs_graph *g, int index, int32_t *fanin0, int32_t *fanin1,

@@ -188,14 +188,17 @@ def _host_depth(g):
 
 
 def test_batch_transfers_agree(ctx):
-    """Upload computes every graph's depth on several host threads; the three
-    download paths (per graph, into caller arrays, library-allocated) return
-    the same arrays."""
+    """Upload computes every graph's depth on several host threads; the batch
+    sizes equal the per-graph ones; the three download paths (per graph, into
+    caller arrays, library-allocated) return the same arrays."""
     gs = C.gen_batch(4, 100, 40, 1000, 60000, 16, 512, threads=8)
     db = ctx.upload_batch(gs)
     for i, g in enumerate(gs):
         assert db.stats(i)["nLevels"] == _host_depth(g), i
     ctx.rw_st(db)
+    allst = db.stats_all()  # culs_batch_stats equals culs_graph_stats per graph
+    for i in range(len(db)):
+        assert {k: int(v[i]) for k, v in allst.items()} == db.stats(i), i
     whole = db.download_all()
     arr = (C._HostGraph * len(db))()
     assert C._lib.culs_batch_download(ctx.h, db.h, arr) == 0
