@@ -109,107 +109,58 @@ __global__ void k_csr_fill(int64_t M, const int *L0, const int *L1, const uint8_
     }
 }
 
-constexpr unsigned long long kNoItem = ~0ull;
-
-__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long *p) {
-    unsigned long long v;
-    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
-    return v;
-}
-__device__ __forceinline__ void st_relaxed_u64(unsigned long long *p, unsigned long long v) {
-    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
-}
-
-// Seeds of the level worklist: live AND nodes without AND fanins, level 1.
-__global__ void k_seed_items(int64_t n, const int *seeds, const int *nSeeds, unsigned long long *items) {
-    const int ns = *nSeeds;
-    int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
-        items[i] = i < ns ? ((unsigned long long)(uint32_t)seeds[i] | (1ull << 32)) : kNoItem;
-}
-
-// Forward Kahn: ASAP level of every live AND node (PIs and constant: 0).
-// pending[v] = (highest level among v's finished AND fanins) << 2 | (AND
-// fanins not finished yet), updated by CAS.  The fanin that finishes last
-// reads v's level off its CAS and publishes the item {v, level} with one
-// 64-bit store, so a consumer needs no other thread's writes and the data
-// path has no fences.  Every live node is published exactly once, so a lane
-// whose queue index reaches the live count has nothing left to wait for.
-__global__ void __launch_bounds__(kBlock) k_level_queue(unsigned long long *items, int *head, int *tail,
-                                                         const int *nLivePtr, const int *L0, const int *L1,
-                                                         const int *off, const int *adj, int *pending, int *level,
-                                                         const int *gid, int *graphLevels, int *maxLevel,
-                                                         int *status) {
+// Level-synchronous Kahn: ASAP level of every live AND node (PIs and
+// constant: 0), one launch per level.  The queue's levels are consecutive
+// segments of `items`; launch L reads its segment's start and size from a
+// three-slot ring (written by launch L - 1, which has finished), releases
+// the fanouts of every node of level L, and appends each fanout whose last
+// pending fanin this was to level L + 1's segment.  Thread 0 of block 0
+// sets the next segment's start and clears the slot that launch L + 1 will
+// append to, which no other block of launch L touches.  No thread waits on
+// another.  ring[0..2]: segment sizes, ring[3..5]: segment starts, both by
+// level mod 3.
+__global__ void __launch_bounds__(kBlock) k_level_step(int L, int *items, int *ring, const int *off, const int *adj,
+                                                        int *pending, int *level, const int *gid, int *graphLevels,
+                                                        int *maxLevel) {
+    const int r = L % 3;
+    const int start = ring[3 + r], n = ring[r];
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        ring[3 + (L + 1) % 3] = start + n;
+        ring[(L + 2) % 3] = 0;
+        if (n > 0) atomicMax(maxLevel, L);
+    }
+    if (n == 0) return;
+    int *nextCnt = ring + (L + 1) % 3;
+    const int nextBase = start + n;
     const int lane = threadIdx.x & 31;
-    const int total = *nLivePtr;
-    int myMax = 0;
-    int h = -1;
-    bool fin = false;
-    int64_t idle = 0;
-    while (true) {
-        const unsigned need = __ballot_sync(0xffffffffu, !fin && h < 0);
-        if (need) {
-            int base = 0;
-            if (lane == 0) base = atomicAdd(head, __popc(need));
-            base = __shfl_sync(0xffffffffu, base, 0);
-            if (!fin && h < 0) h = base + __popc(need & ((1u << lane) - 1u));
-        }
-        int v = -1, lv = 0;
-        if (!fin) {
-            if (h >= total) {
-                fin = true;
-            } else {
-                const unsigned long long it = ld_relaxed_u64(&items[h]);
-                if (it != kNoItem) {
-                    v = (int)(uint32_t)it;
-                    lv = (int)(it >> 32);
-                    h = -1;
-                }
-            }
-        }
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    for (int64_t i0 = ((int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 32; i0 < n; i0 += warps * 32) {
+        const int64_t i = i0 + lane;
         int k = 0, e = 0;
-        if (v >= 0) {
-            level[v] = lv;
-            agg_max(graphLevels, gid[v], lv);
-            myMax = lv > myMax ? lv : myMax;
+        if (i < n) {
+            const int v = items[start + i];
+            level[v] = L;
+            agg_max(graphLevels, gid[v], L);
             k = off[v];
             e = off[v + 1];
         }
         // release the fanouts, one fanout per lane per round
         while (__any_sync(0xffffffffu, k < e)) {
-            unsigned long long item = kNoItem;
+            bool push = false;
+            int w = 0;
             if (k < e) {
-                const int w = adj[k++];
-                int old = __ldcg(&pending[w]), nw;
-                while (true) {  // at most two updaters per word
-                    const int m = (old >> 2) > lv ? (old >> 2) : lv;
-                    nw = (m << 2) | ((old & 3) - 1);
-                    const int prev = atomicCAS(&pending[w], old, nw);
-                    if (prev == old) break;
-                    old = prev;
-                }
-                if ((old & 3) == 1) item = (unsigned long long)(uint32_t)w | ((unsigned long long)(1 + (nw >> 2)) << 32);
+                w = adj[k++];
+                push = atomicSub(&pending[w], 1) == 1;
             }
-            const unsigned b = __ballot_sync(0xffffffffu, item != kNoItem);
+            const unsigned b = __ballot_sync(0xffffffffu, push);
             if (b) {
                 int base = 0;
-                if (lane == 0) base = atomicAdd(tail, __popc(b));
+                if (lane == 0) base = atomicAdd(nextCnt, __popc(b));
                 base = __shfl_sync(0xffffffffu, base, 0);
-                if (item != kNoItem) st_relaxed_u64(&items[base + __popc(b & ((1u << lane) - 1u))], item);
+                if (push) items[nextBase + base + __popc(b & ((1u << lane) - 1u))] = w;
             }
         }
-        if (__all_sync(0xffffffffu, fin)) break;
-        if (__any_sync(0xffffffffu, v >= 0)) {
-            idle = 0;
-        } else if (++idle > kSpinLimit) {
-            if (lane == 0) set_status(status, kDevWaitTimeout);
-            break;
-        } else {
-            backoff(idle);
-        }
     }
-    myMax = __reduce_max_sync(0xffffffffu, myMax);
-    if (lane == 0 && myMax > 0) atomicMax(maxLevel, myMax);
 }
 
 __global__ void k_live_flags(int64_t M, const int *L0, const uint8_t *dead, uint8_t *liveFlag, int *done) {
@@ -541,7 +492,6 @@ int Engine::strash_core(Batch &b, int64_t M, const int *L0, const int *L1, const
         launches_ += 4;
     }
     // 2. levels of live AND nodes
-    unsigned long long *items64 = nullptr;
     int *liveIdx = nullptr;
     if (topo) {
         liveIdx = ar_.get<int>(M + 1);
@@ -574,20 +524,31 @@ int Engine::strash_core(Batch &b, int64_t M, const int *L0, const int *L1, const
     int *adj = ar_.get<int>(nEdges + 1);
     if (!adj) return fail(CULS_E_OOM, "strash: scratch arena exhausted");
     k_csr_fill<<<gridM, kBlock, 0, s>>>(M, L0, L1, liveFlag, cursor, adj);
-    items64 = ar_.get<unsigned long long>(M + 1);
     liveIdx = ar_.get<int>(M + 1);
-    if (!items64 || !liveIdx) return fail(CULS_E_OOM, "strash: scratch arena exhausted");
+    int *ring = ar_.get<int>(8);
+    if (!liveIdx || !ring) return fail(CULS_E_OOM, "strash: scratch arena exhausted");
     check(cudaMemsetAsync(qc, 0, sizeof(int) * 8, s), "memset");
+    check(cudaMemsetAsync(ring, 0, sizeof(int) * 8, s), "memset");
     check(cudaMemsetAsync(graphLevels, 0, sizeof(int) * (G + 1), s), "memset");
     check(cudaMemsetAsync(level, 0, sizeof(int) * (M + 1), s), "memset");
-    check(compact_flags(flags, M, items, qc + 1, ar_, s), "compact");       // seeds; tail starts at their count
+    check(compact_flags(flags, M, items, ring + 1, ar_, s), "compact");     // level 1: the seeds
     check(compact_flags(liveFlag, M, liveIdx, qc + 3, ar_, s), "compact");  // live list and count
-    k_seed_items<<<gridM, kBlock, 0, s>>>(M + 1, items, qc + 1, items64);
+    launches_ += 2;
     if (prof_) this->mark(kMkLevelK0);
-    k_level_queue<<<gridQ, kBlock, 0, s>>>(items64, qc + 0, qc + 1, qc + 3, L0, L1, off, adj, pending, level, gidA,
-                                           graphLevels, qc + 4, status_);
+    // levels in launches of 64, until a level comes out empty; the ring
+    // then holds the number of nodes given a level (all live ones unless
+    // there is a cycle)
+    int L = 1;
+    while (true) {
+        for (int t = 0; t < 64; t++, L++)
+            k_level_step<<<gridQ, kBlock, 0, s>>>(L, items, ring, off, adj, pending, level, gidA, graphLevels, qc + 4);
+        launches_ += 64;
+        check(cudaMemcpyAsync(hostSmall_, ring, sizeof(int) * 6, cudaMemcpyDeviceToHost, s), "d2h");
+        if (sync()) return -1;
+        if (hostSmall_[L % 3] == 0) break;
+    }
+    check(cudaMemcpyAsync(qc + 1, ring + 3 + L % 3, sizeof(int), cudaMemcpyDeviceToDevice, s), "copy");
     if (prof_) this->mark(kMkLevelK1);
-    launches_ += 4;
     }
     // 3. processing order (level, position) and tentative ranks
     check(cudaMemcpyAsync(hostSmall_, qc, sizeof(int) * 8, cudaMemcpyDeviceToHost, s), "d2h");
