@@ -21,6 +21,12 @@ if not LIB_PATH.exists():
 _lib = ctypes.CDLL(str(LIB_PATH))
 
 CULS_OK = 0
+CULS_E_INVALID = -1
+CULS_E_OOM = -2
+CULS_E_BUDGET = -3
+CULS_E_PROBE = -4
+CULS_E_DEVICE = -5
+CULS_E_IO = -6
 CULS_E_BUSY = -7
 CULS_E_NOTFOUND = -8
 ERRORS = {-1: "CULS_E_INVALID", -2: "CULS_E_OOM", -3: "CULS_E_BUDGET", -4: "CULS_E_PROBE", -5: "CULS_E_DEVICE",
@@ -57,6 +63,11 @@ _lib.culs_sync.argtypes = [_vp]
 _lib.culs_graph_upload.argtypes = [_vp, _ip, _ip, _ip, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                    ctypes.POINTER(_vp)]
 _lib.culs_batch_upload.argtypes = [_vp, ctypes.c_int, ctypes.POINTER(_HostGraph), ctypes.POINTER(_vp)]
+_lib.culs_batch_upload_aiger.argtypes = [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_char_p),
+                                         ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(_vp)]
+_lib.culs_batch_download_aiger.argtypes = [_vp, _vp, ctypes.POINTER(_vp), ctypes.POINTER(ctypes.c_size_t)]
+_lib.culs_buffer_free.argtypes = [_vp]
+_lib.culs_buffer_free.restype = None
 _lib.culs_graph_free.argtypes = [_vp]
 _lib.culs_graph_count.argtypes = [_vp]
 _lib.culs_graph_stats.argtypes = [_vp, ctypes.c_int, _ip, _ip, _ip, _ip]
@@ -211,6 +222,15 @@ class Context:
                                          ctypes.byref(out)), "upload")
         return DeviceGraphs(self, out)
 
+    def upload_aiger_batch(self, files) -> "DeviceGraphs":
+        """Binary AIGER files' contents (bytes objects), decoded on the device."""
+        n = len(files)
+        data = (ctypes.c_char_p * n)(*files)
+        lens = (ctypes.c_size_t * n)(*[len(f) for f in files])
+        out = _vp()
+        self._err(_lib.culs_batch_upload_aiger(self.h, n, data, lens, ctypes.byref(out)), "AIGER upload")
+        return DeviceGraphs(self, out)
+
     def upload_batch(self, graphs) -> "DeviceGraphs":
         arr = (_HostGraph * len(graphs))(*[g.host() for g in graphs])
         out = _vp()
@@ -361,6 +381,19 @@ class DeviceGraphs:
         v = [ctypes.c_int32() for _ in range(4)]
         _check(_lib.culs_graph_stats(self.h, i, *[ctypes.byref(x) for x in v]), "stats")
         return dict(zip(["nPIs", "nPOs", "nAnds", "nLevels"], [x.value for x in v]))
+
+    def download_aiger_all(self):
+        """Every graph of the handle as binary AIGER file contents (bytes),
+        encoded on the device."""
+        n = len(self)
+        ptrs = (_vp * n)()
+        lens = (ctypes.c_size_t * n)()
+        self.ctx._err(_lib.culs_batch_download_aiger(self.ctx.h, self.h, ptrs, lens), "AIGER download")
+        out = []
+        for i in range(n):
+            out.append(ctypes.string_at(ptrs[i], lens[i]))
+            _lib.culs_buffer_free(ptrs[i])
+        return out
 
     def stats_all(self):
         """nPIs, nPOs, nAnds, nLevels of every graph, as int32 arrays."""

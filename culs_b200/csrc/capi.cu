@@ -117,6 +117,40 @@ int culs_graph_stats(const culs_graph *g, int index, int32_t *nPIs, int32_t *nPO
     return CULS_OK;
 }
 
+int culs_batch_upload_aiger(culs_ctx *ctx, int count, const uint8_t *const *data, const size_t *len,
+                            culs_graph **g) {
+    if (!ctx || !g || count < 1 || !data || !len) return CULS_E_INVALID;
+    *g = nullptr;
+    auto h = std::make_unique<culs_graph>();
+    h->owner = ctx;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    const int rc = set_err(ctx, ctx->eng.upload_aiger(h->b, count, data, len));
+    if (rc == CULS_OK) *g = h.release();
+    return rc;
+}
+
+int culs_batch_download_aiger(culs_ctx *ctx, const culs_graph *g, uint8_t **data, size_t *len) {
+    if (!ctx || !g || !data || !len) return CULS_E_INVALID;
+    std::vector<std::string> files;
+    {
+        std::lock_guard<std::mutex> lk(ctx->mu);
+        const int rc = set_err(ctx, ctx->eng.download_aiger(g->b, files));
+        if (rc != CULS_OK) return rc;
+    }
+    for (size_t i = 0; i < files.size(); i++) {
+        data[i] = static_cast<uint8_t *>(malloc(files[i].size() ? files[i].size() : 1));
+        if (!data[i]) {
+            for (size_t j = 0; j < i; j++) free(data[j]);
+            return CULS_E_OOM;
+        }
+        memcpy(data[i], files[i].data(), files[i].size());
+        len[i] = files[i].size();
+    }
+    return CULS_OK;
+}
+
+void culs_buffer_free(void *p) { free(p); }
+
 int culs_batch_stats(const culs_graph *g, int32_t *nPIs, int32_t *nPOs, int32_t *nAnds, int32_t *nLevels) {
     if (!g) return CULS_E_INVALID;
     for (int i = 0; i < g->b.G; i++) {

@@ -28,6 +28,7 @@ enum DevStatus : int32_t {
     kDevStackOverflow = 3, // an explicit traversal stack overflowed
     kDevBadGraph = 4,      // structural inconsistency (cycle, bad literal)
     kDevCapacity = 5,      // a work buffer was too small
+    kDevAigerFormat = 6,   // binary AIGER bytes do not decode
 };
 
 // Upper bound on spin iterations of a dependency wait (each iteration sleeps

@@ -153,6 +153,12 @@ class Engine {
     // Whole-batch download into caller arrays (graph i's fanins into f0[i],
     // f1[i], its POs into outs[i]); a null array pointer skips that part.
     int download_all(const Batch &b, int32_t *const *f0, int32_t *const *f1, int32_t *const *outs);
+    // Binary AIGER files' bytes in, decoded on the device (aiger_dev.cu).
+    int upload_aiger(Batch &b, int count, const uint8_t *const *data, const size_t *len);
+    // Every graph as a binary AIGER file's bytes, encoded on the device.
+    int download_aiger(const Batch &b, std::vector<std::string> &files);
+    // Sets every graph's nLevels to its depth (AIGMan::readFromMemory).
+    int batch_depth(Batch &b);
     int rw(Batch &b, bool useZeros, bool gpuDedup, RwStats *stats, RwDump *dump);
     int st(Batch &b, bool cpuOrder);
     int sync();

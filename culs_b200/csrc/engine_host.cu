@@ -17,9 +17,10 @@ int ExecCtx::status_check(const char *what) {
     if (st == kDevOk) return 0;
     cudaMemset(status, 0, sizeof(int));
     static const char *names[] = {"ok", "dependency wait timed out", "hash table full", "traversal stack overflow",
-                                  "malformed graph", "work buffer too small"};
-    if (err) *err = std::string(what) + ": " + (st >= 0 && st <= 5 ? names[st] : "device error");
+                                  "malformed graph", "work buffer too small", "malformed binary AIGER"};
+    if (err) *err = std::string(what) + ": " + (st >= 0 && st <= 6 ? names[st] : "device error");
     if (st == kDevWaitTimeout || st == kDevTableFull || st == kDevStackOverflow) return CULS_E_PROBE;
+    if (st == kDevAigerFormat) return CULS_E_IO;
     return CULS_E_INVALID;
 }
 

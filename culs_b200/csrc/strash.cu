@@ -697,4 +697,67 @@ int Engine::strash_core(Batch &b, int64_t M, const int *L0, const int *L1, const
     return check_status("strash output");
 }
 
+namespace {
+
+// AIGMan literals of graph-major arrays to position literals (-1 for the
+// constant and PIs), and each position's graph.
+__global__ void k_depth_prep(int64_t N, int G, const DevGraph *dg, const int *F0, const int *F1, int *L0, int *L1,
+                             int *gid) {
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < N; p += stride) {
+        const int g = graph_of_pos(dg, G, (int)p);
+        const int base = dg[g].base;
+        gid[p] = g;
+        if ((int)p - base <= dg[g].nPIs) {
+            L0[p] = L1[p] = -1;
+        } else {
+            L0[p] = F0[p] + 2 * base;
+            L1[p] = F1[p] + 2 * base;
+        }
+    }
+}
+
+}  // namespace
+
+// AIGMan::readFromMemory's nLevels for every graph of b (the level of its
+// deepest AND node, dangling ones included), by the st levelization.
+int Engine::batch_depth(Batch &b) {
+    const int64_t N = b.nObj;
+    const int G = b.G;
+    int rc;
+    if ((rc = ensure_arena((size_t)N * 24 + ((size_t)64 << 20)))) return rc;
+    ar_.reset();
+    int *L0 = ar_.get<int>(N + 1), *L1 = ar_.get<int>(N + 1), *gid = ar_.get<int>(N + 1), *level = ar_.get<int>(N + 1),
+        *done = ar_.get<int>(N + 1), *graphLevels = ar_.get<int>(G + 1);
+    uint8_t *dead = ar_.get<uint8_t>(N + 1), *live = ar_.get<uint8_t>(N + 1);
+    if (!L0 || !L1 || !gid || !level || !done || !graphLevels || !dead || !live)
+        return fail(CULS_E_OOM, "depth: arena exhausted");
+    cudaStream_t s = s_;
+    ExecCtx X = ctx();
+    for (auto &g : b.hg) g.cpos = g.base;
+    if ((rc = check(cudaMemcpyAsync(b.dg, b.hg.data(), sizeof(DevGraph) * G, cudaMemcpyHostToDevice, s), "h2d")))
+        return rc;
+    ChunkSched sched;
+    if ((rc = build_chunk_sched(X, b, kBlock, sched))) return rc;
+    int *qc = counters_;
+    if ((rc = check(cudaMemsetAsync(qc, 0, sizeof(int) * 8, s), "memset"))) return rc;
+    if ((rc = check(cudaMemsetAsync(graphLevels, 0, sizeof(int) * (G + 1), s), "memset"))) return rc;
+    if ((rc = check(cudaMemsetAsync(level, 0, sizeof(int) * (N + 1), s), "memset"))) return rc;
+    if ((rc = check(cudaMemsetAsync(dead, 0, (size_t)N + 1, s), "memset"))) return rc;
+    k_depth_prep<<<X.grid(N), kBlock, 0, s>>>(N, G, b.dg, b.F0, b.F1, L0, L1, gid);
+    k_live_flags<<<X.grid(N), kBlock, 0, s>>>(N, L0, dead, live, done);
+    k_st_levelize<<<(unsigned)(sms_ * 8), kBlock, 0, s>>>(sched, L0, L1, live, gid, level, done, graphLevels, qc + 5,
+                                                          qc + 4, status_);
+    launches_ += 3;
+    std::vector<int> hl(G);
+    if ((rc = check(cudaMemcpyAsync(hl.data(), graphLevels, sizeof(int) * G, cudaMemcpyDeviceToHost, s), "d2h")))
+        return rc;
+    if ((rc = sync())) return rc;
+    if ((rc = check_status("depth"))) return rc;
+    for (int g = 0; g < G; g++) b.hg[g].nLevels = hl[g];
+    rc = check(cudaMemcpyAsync(b.dg, b.hg.data(), sizeof(DevGraph) * G, cudaMemcpyHostToDevice, s), "h2d");
+    ar_.reset();
+    return rc ? rc : sync();
+}
+
 }  // namespace culs

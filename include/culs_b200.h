@@ -91,6 +91,19 @@ int culs_graph_upload(culs_ctx *ctx, const int32_t *fanin0, const int32_t *fanin
                       int32_t nPOs, int32_t nAnds, culs_graph **g);
 /* Copies `count` AIGs into one device-resident batch. */
 int culs_batch_upload(culs_ctx *ctx, int count, const culs_host_graph *graphs, culs_graph **g);
+/* `count` binary AIGER files' contents (data[i], len[i] bytes) into one
+ * batch: AIGMan::readFromMemory (src/aig_manager.cu:110-229, aigDecodeBinary
+ * :861-869) with the header and output lines read on the host and the
+ * delta-encoded AND section decoded on the device.  Accepts what
+ * culs_aiger_read accepts; anything else is CULS_E_IO. */
+int culs_batch_upload_aiger(culs_ctx *ctx, int count, const uint8_t *const *data, const size_t *len,
+                            culs_graph **g);
+/* Every graph of the handle as binary AIGER bytes, the file AIGMan::saveFile
+ * writes (src/aig_manager.cu:231-267, aigEncodeBinary :871-880), the AND
+ * section encoded on the device: data[i] receives a buffer of len[i] bytes
+ * allocated by the library; free each with culs_buffer_free. */
+int culs_batch_download_aiger(culs_ctx *ctx, const culs_graph *g, uint8_t **data, size_t *len);
+void culs_buffer_free(void *p);
 void culs_graph_free(culs_graph *g);
 int culs_graph_count(const culs_graph *g);
 /* Sizes and level of graph `index` (AIGMan::printStats, src/aig_manager.cu:604-612). */
