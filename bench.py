@@ -16,7 +16,8 @@ A step is one `rw; st` over the workload's graphs:
       reports throughput and p50/p99 submit-to-done latency
 `value` times device-resident steps (a device clone of the input, rw, st);
 `e2e` times the public C-ABI path from host arrays: upload, rw, st,
-download.  With --gpus N (under torchrun) every rank rewrites its own
+download; `e2e_aiger` the same from binary AIGER files' bytes to files'
+bytes, decoded and encoded on the device.  With --gpus N (under torchrun) every rank rewrites its own
 4,096 graphs (weak scaling, no data-path collective).
 """
 import argparse
@@ -407,6 +408,26 @@ def our_arm(args, group):
     ctx.sync()
     e2e_ms = group.max(ctx.profile_read()["user"])
     e2e_value = total_and * e2e_steps / (e2e_ms / 1e3)
+    # the same through binary AIGER files' bytes (the reference's read; rw;
+    # st; write): decoded and encoded on the device
+    files = d0.download_aiger_all()
+    aig_in = sum(len(f) for f in files)
+    group.barrier()
+    ctx.sync()
+    ctx.mark(0)
+    aig_out = 0
+    for _ in range(e2e_steps):
+        d = ctx.upload_aiger_batch(files)
+        ctx.rw_st(d)
+        res = d.download_aiger_all()
+        aig_out = sum(len(f) for f in res)
+        d.free()
+    ctx.mark(1)
+    ctx.sync()
+    aig_ms = group.max(ctx.profile_read()["user"])
+    e2e_aiger = {"value": total_and * e2e_steps / (aig_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": aig_in,
+                 "d2h_bytes_per_step": aig_out, "steps": e2e_steps,
+                 "path": "binary AIGER bytes in and out (culs_batch_upload_aiger, culs_batch_download_aiger)"}
     # roofline of the dominant kernel
     peak, peak_kind = measured_peak()
     kname = max(KERNELS, key=lambda k: prof.get(k, 0.0))
@@ -431,6 +452,7 @@ def our_arm(args, group):
             "roofline": roof,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": in_bytes,
                     "d2h_bytes_per_step": out_bytes, "steps": e2e_steps},
+            "e2e_aiger": e2e_aiger,
             "clocks": clk.summary(), "gpu_launches": launches,
             "stages_ms_last_step": {k: round(v, 3) for k, v in prof.items() if k not in ("user",)}}
     if group.rank == 0:

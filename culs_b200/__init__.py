@@ -63,8 +63,8 @@ _lib.culs_sync.argtypes = [_vp]
 _lib.culs_graph_upload.argtypes = [_vp, _ip, _ip, _ip, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                    ctypes.POINTER(_vp)]
 _lib.culs_batch_upload.argtypes = [_vp, ctypes.c_int, ctypes.POINTER(_HostGraph), ctypes.POINTER(_vp)]
-_lib.culs_batch_upload_aiger.argtypes = [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_char_p),
-                                         ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(_vp)]
+_lib.culs_batch_upload_aiger.argtypes = [_vp, ctypes.c_int, _vp, ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(_vp)]
+_lib.culs_batch_download_aiger_into.argtypes = [_vp, _vp, _vp, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]
 _lib.culs_batch_download_aiger.argtypes = [_vp, _vp, ctypes.POINTER(_vp), ctypes.POINTER(ctypes.c_size_t)]
 _lib.culs_buffer_free.argtypes = [_vp]
 _lib.culs_buffer_free.restype = None
@@ -223,12 +223,22 @@ class Context:
         return DeviceGraphs(self, out)
 
     def upload_aiger_batch(self, files) -> "DeviceGraphs":
-        """Binary AIGER files' contents (bytes objects), decoded on the device."""
+        """Binary AIGER files' contents (bytes or any contiguous byte
+        buffer), decoded on the device; nothing is copied on the way in."""
         n = len(files)
-        data = (ctypes.c_char_p * n)(*files)
-        lens = (ctypes.c_size_t * n)(*[len(f) for f in files])
+        keep, addr = [], np.empty(max(n, 1), np.uint64)
+        for i, f in enumerate(files):
+            if isinstance(f, bytes):
+                c = ctypes.c_char_p(f)
+                keep.append(c)
+                addr[i] = ctypes.cast(c, ctypes.c_void_p).value or 0
+            else:
+                a = np.frombuffer(f, np.uint8)
+                keep.append(a)
+                addr[i] = a.ctypes.data
+        lens = (ctypes.c_size_t * max(n, 1))(*[len(f) for f in files])
         out = _vp()
-        self._err(_lib.culs_batch_upload_aiger(self.h, n, data, lens, ctypes.byref(out)), "AIGER upload")
+        self._err(_lib.culs_batch_upload_aiger(self.h, n, addr.ctypes.data, lens, ctypes.byref(out)), "AIGER upload")
         return DeviceGraphs(self, out)
 
     def upload_batch(self, graphs) -> "DeviceGraphs":
@@ -383,17 +393,18 @@ class DeviceGraphs:
         return dict(zip(["nPIs", "nPOs", "nAnds", "nLevels"], [x.value for x in v]))
 
     def download_aiger_all(self):
-        """Every graph of the handle as binary AIGER file contents (bytes),
-        encoded on the device."""
+        """Every graph of the handle as binary AIGER file contents, encoded
+        on the device: memoryviews into one buffer holding the files back to
+        back (bytes(view) copies one out)."""
         n = len(self)
-        ptrs = (_vp * n)()
-        lens = (ctypes.c_size_t * n)()
-        self.ctx._err(_lib.culs_batch_download_aiger(self.ctx.h, self.h, ptrs, lens), "AIGER download")
-        out = []
-        for i in range(n):
-            out.append(ctypes.string_at(ptrs[i], lens[i]))
-            _lib.culs_buffer_free(ptrs[i])
-        return out
+        off = (ctypes.c_size_t * (n + 1))()
+        self.ctx._err(_lib.culs_batch_download_aiger_into(self.ctx.h, self.h, None, 0, off), "AIGER download")
+        buf = np.empty(max(off[n], 1), np.uint8)
+        self.ctx._err(_lib.culs_batch_download_aiger_into(self.ctx.h, self.h, buf.ctypes.data, off[n], off),
+                      "AIGER download")
+        mv = memoryview(buf)
+        o = list(off)
+        return [mv[o[i]:o[i + 1]] for i in range(n)]
 
     def stats_all(self):
         """nPIs, nPOs, nAnds, nLevels of every graph, as int32 arrays."""

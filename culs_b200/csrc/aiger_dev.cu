@@ -20,9 +20,12 @@
 // Encoding runs the other way: every AND writes its two numbers' byte
 // lengths, a scan places them, every AND writes its bytes, and the host
 // frames each graph's bytes with the header, the output lines and "c".
+#include <algorithm>
+#include <atomic>
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "kernels.cuh"
@@ -228,6 +231,49 @@ __global__ void k_gather_i64(int n, const int64_t *idx, const long long *src, lo
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) dst[k] = src[idx[k]];
 }
 
+// Graphs [0, G) in at most `parts` contiguous runs of about equal weight,
+// each run on its own host thread (the first on the caller's).
+template <class W, class F>
+void for_runs(int G, W weight, F fn) {
+    int64_t total = 0;
+    for (int g = 0; g < G; g++) total += weight(g);
+    const unsigned hw = std::thread::hardware_concurrency();
+    const int parts = total < (1 << 20) ? 1 : (int)std::max(1u, std::min({hw ? hw : 1u, 32u, (unsigned)G}));
+    std::vector<int> cut{0};
+    int64_t acc = 0;
+    for (int g = 0; g < G; g++) {
+        acc += weight(g);
+        if ((int)cut.size() < parts && acc * parts >= total * (int64_t)cut.size() && g + 1 < G) cut.push_back(g + 1);
+    }
+    cut.push_back(G);
+    std::vector<std::thread> th;
+    for (size_t r = 1; r + 1 < cut.size(); r++) th.emplace_back([&, r] { fn(cut[r], cut[r + 1]); });
+    fn(cut[0], cut[1]);
+    for (auto &t : th) t.join();
+}
+
+// Decimal digits of v >= 0 followed by '\n' at p; returns the end.
+char *put_line(char *p, int v) {
+    char t[12];
+    int n = 0;
+    do {
+        t[n++] = (char)('0' + v % 10);
+        v /= 10;
+    } while (v);
+    while (n) *p++ = t[--n];
+    *p++ = '\n';
+    return p;
+}
+
+int line_len(int v) {
+    int n = 2;
+    while (v >= 10) {
+        v /= 10;
+        n++;
+    }
+    return n;
+}
+
 // Host side of the header: "aig M I L O A\n" and O output lines; returns
 // false on anything the host reader (host_aiger.cpp) refuses.
 bool read_dec(const uint8_t *&p, const uint8_t *end, long long &v) {
@@ -276,10 +322,19 @@ int Engine::upload_aiger(Batch &b, int count, const uint8_t *const *data, const 
     std::vector<int64_t> regOff(count + 1), andBase(count + 1);
     int64_t nObj = 0, nPO = 0, nAnd = 0, bytes = 0;
     std::vector<size_t> body(count);
+    std::vector<int> head(3 * (size_t)count);
+    std::atomic<int> bad{-1};
+    for_runs(count, [&](int g) { return (int64_t)len[g] / 64 + 1; }, [&](int g0, int g1) {
+        for (int g = g0; g < g1; g++)
+            if (!data[g] || !parse_head(data[g], len[g], head[3 * g], head[3 * g + 1], head[3 * g + 2], outs[g], body[g])) {
+                int none = -1;
+                bad.compare_exchange_strong(none, g);
+                return;
+            }
+    });
+    if (bad.load() >= 0) return fail(CULS_E_IO, "upload: not binary AIGER (graph " + std::to_string(bad.load()) + ")");
     for (int g = 0; g < count; g++) {
-        int nPIs, nPOs, nAnds;
-        if (!data[g] || !parse_head(data[g], len[g], nPIs, nPOs, nAnds, outs[g], body[g]))
-            return fail(CULS_E_IO, "upload: not binary AIGER (graph " + std::to_string(g) + ")");
+        const int nPIs = head[3 * g], nPOs = head[3 * g + 1], nAnds = head[3 * g + 2];
         hg[g] = DevGraph{nPIs, nPOs, nAnds, 0, (int)nObj, (int)nPO, (int)nObj, 0};
         regOff[g] = bytes;
         andBase[g] = nAnd;
@@ -296,10 +351,12 @@ int Engine::upload_aiger(Batch &b, int count, const uint8_t *const *data, const 
     if ((rc = ensure_stage((size_t)(bytes + 3) / 4 + (size_t)nPO + 1))) return rc;
     uint8_t *sB = reinterpret_cast<uint8_t *>(stage_);
     int32_t *sPO = stage_ + (bytes + 3) / 4;
-    for (int g = 0; g < count; g++) {
-        memcpy(sB + regOff[g], data[g] + body[g], len[g] - body[g]);
-        if (!outs[g].empty()) memcpy(sPO + hg[g].poOff, outs[g].data(), sizeof(int32_t) * outs[g].size());
-    }
+    for_runs(count, [&](int g) { return regOff[g + 1] - regOff[g] + 1; }, [&](int g0, int g1) {
+        for (int g = g0; g < g1; g++) {
+            memcpy(sB + regOff[g], data[g] + body[g], len[g] - body[g]);
+            if (!outs[g].empty()) memcpy(sPO + hg[g].poOff, outs[g].data(), sizeof(int32_t) * outs[g].size());
+        }
+    });
     if (!b.pool) b.pool = pool_;
     if ((rc = check(b.reserve(nObj, nPO, count), "cudaMalloc"))) return rc;
     const int64_t nTiles = (bytes + kAigTile - 1) / kAigTile;
@@ -363,7 +420,7 @@ int Engine::upload_aiger(Batch &b, int count, const uint8_t *const *data, const 
     return batch_depth(b);
 }
 
-int Engine::download_aiger(const Batch &b, std::vector<std::string> &files) {
+int Engine::download_aiger(const Batch &b, uint8_t *buf, size_t cap, size_t *offsets) {
     const int G = b.G;
     int64_t nAnd = 0;
     std::vector<int64_t> andBase(G + 1);
@@ -398,7 +455,7 @@ int Engine::download_aiger(const Batch &b, std::vector<std::string> &files) {
     // the graphs' first bytes: offA at each graph's first AND (total past the last)
     std::vector<long long> hOff(G + 1, total);
     if (nAnd > 0) {
-        k_aig_enc_write<<<X.grid(nAnd), kBlock, 0, s>>>(nAnd, G, dAnd, b.dg, b.F0, b.F1, offA, dB);
+        if (buf) k_aig_enc_write<<<X.grid(nAnd), kBlock, 0, s>>>(nAnd, G, dAnd, b.dg, b.F0, b.F1, offA, dB);
         std::vector<int64_t> firstAnd;
         std::vector<int> which;
         for (int g = 0; g < G; g++)
@@ -427,26 +484,46 @@ int Engine::download_aiger(const Batch &b, std::vector<std::string> &files) {
     if ((rc = ensure_stage((size_t)(total + 3) / 4 + (size_t)b.nPO + 1))) return rc;
     uint8_t *sB = reinterpret_cast<uint8_t *>(stage_);
     int32_t *sPO = stage_ + (total + 3) / 4;
-    if (total && (rc = check(cudaMemcpyAsync(sB, dB, (size_t)total, cudaMemcpyDeviceToHost, s), "d2h"))) return rc;
+    if (buf && total && (rc = check(cudaMemcpyAsync(sB, dB, (size_t)total, cudaMemcpyDeviceToHost, s), "d2h")))
+        return rc;  // (the sizes need the numbers' lengths and the output literals only)
     if (b.nPO && (rc = check(cudaMemcpyAsync(sPO, b.PO, sizeof(int32_t) * b.nPO, cudaMemcpyDeviceToHost, s), "d2h")))
         return rc;
     if ((rc = sync())) return rc;
-    files.assign(G, std::string());
-    char line[64];
+    // file g = header, output lines, numbers, "c\n"; files back to back
+    std::vector<int> headLen(G);
+    std::vector<int64_t> textLen(G);
+    char hline[96];
     for (int g = 0; g < G; g++) {
         const DevGraph &d = b.hg[g];
-        std::string &f = files[g];
-        const long long body = hOff[g + 1] - hOff[g];
-        f.reserve((size_t)body + 16 * (size_t)d.nPOs + 64);
-        int k = snprintf(line, sizeof line, "aig %d %d 0 %d %d\n", d.nPIs + d.nAnds, d.nPIs, d.nPOs, d.nAnds);
-        f.append(line, (size_t)k);
-        for (int o = 0; o < d.nPOs; o++) {
-            k = snprintf(line, sizeof line, "%d\n", aig_inv_const(sPO[d.poOff + o]));
-            f.append(line, (size_t)k);
-        }
-        f.append(reinterpret_cast<const char *>(sB) + hOff[g], (size_t)body);
-        f.append("c\n");
+        headLen[g] = snprintf(hline, sizeof hline, "aig %d %d 0 %d %d\n", d.nPIs + d.nAnds, d.nPIs, d.nPOs, d.nAnds);
     }
+    for_runs(G, [&](int g) { return (int64_t)b.hg[g].nPOs + 1; }, [&](int g0, int g1) {
+        for (int g = g0; g < g1; g++) {
+            int64_t t = 0;
+            for (int o = 0; o < b.hg[g].nPOs; o++) t += line_len(aig_inv_const(sPO[b.hg[g].poOff + o]));
+            textLen[g] = t;
+        }
+    });
+    offsets[0] = 0;
+    for (int g = 0; g < G; g++)
+        offsets[g + 1] = offsets[g] + (size_t)headLen[g] + (size_t)textLen[g] + (size_t)(hOff[g + 1] - hOff[g]) + 2;
+    if (!buf) return 0;  // sizes only
+    if (cap < offsets[G]) return fail(CULS_E_INVALID, "download: AIGER buffer too small");
+    for_runs(G, [&](int g) { return (int64_t)(offsets[g + 1] - offsets[g]); }, [&](int g0, int g1) {
+        char line[96];
+        for (int g = g0; g < g1; g++) {
+            const DevGraph &d = b.hg[g];
+            char *p = reinterpret_cast<char *>(buf + offsets[g]);
+            snprintf(line, sizeof line, "aig %d %d 0 %d %d\n", d.nPIs + d.nAnds, d.nPIs, d.nPOs, d.nAnds);
+            memcpy(p, line, (size_t)headLen[g]);
+            p += headLen[g];
+            for (int o = 0; o < d.nPOs; o++) p = put_line(p, aig_inv_const(sPO[d.poOff + o]));
+            memcpy(p, sB + hOff[g], (size_t)(hOff[g + 1] - hOff[g]));
+            p += hOff[g + 1] - hOff[g];
+            *p++ = 'c';
+            *p++ = '\n';
+        }
+    });
     return 0;
 }
 

@@ -129,24 +129,33 @@ int culs_batch_upload_aiger(culs_ctx *ctx, int count, const uint8_t *const *data
     return rc;
 }
 
+int culs_batch_download_aiger_into(culs_ctx *ctx, const culs_graph *g, uint8_t *buf, size_t cap, size_t *offsets) {
+    if (!ctx || !g || !offsets) return CULS_E_INVALID;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    return set_err(ctx, ctx->eng.download_aiger(g->b, buf, cap, offsets));
+}
+
 int culs_batch_download_aiger(culs_ctx *ctx, const culs_graph *g, uint8_t **data, size_t *len) {
     if (!ctx || !g || !data || !len) return CULS_E_INVALID;
-    std::vector<std::string> files;
-    {
-        std::lock_guard<std::mutex> lk(ctx->mu);
-        const int rc = set_err(ctx, ctx->eng.download_aiger(g->b, files));
-        if (rc != CULS_OK) return rc;
-    }
-    for (size_t i = 0; i < files.size(); i++) {
-        data[i] = static_cast<uint8_t *>(malloc(files[i].size() ? files[i].size() : 1));
+    const int G = g->b.G;
+    std::vector<size_t> off(G + 1);
+    int rc = culs_batch_download_aiger_into(ctx, g, nullptr, 0, off.data());
+    if (rc != CULS_OK) return rc;
+    uint8_t *all = static_cast<uint8_t *>(malloc(off[G] ? off[G] : 1));
+    if (!all) return CULS_E_OOM;
+    rc = culs_batch_download_aiger_into(ctx, g, all, off[G], off.data());
+    for (int i = 0; i < G && rc == CULS_OK; i++) {
+        data[i] = static_cast<uint8_t *>(malloc(off[i + 1] - off[i] ? off[i + 1] - off[i] : 1));
         if (!data[i]) {
-            for (size_t j = 0; j < i; j++) free(data[j]);
-            return CULS_E_OOM;
+            for (int j = 0; j < i; j++) free(data[j]);
+            rc = CULS_E_OOM;
+            break;
         }
-        memcpy(data[i], files[i].data(), files[i].size());
-        len[i] = files[i].size();
+        memcpy(data[i], all + off[i], off[i + 1] - off[i]);
+        len[i] = off[i + 1] - off[i];
     }
-    return CULS_OK;
+    free(all);
+    return rc;
 }
 
 void culs_buffer_free(void *p) { free(p); }

@@ -155,8 +155,10 @@ class Engine {
     int download_all(const Batch &b, int32_t *const *f0, int32_t *const *f1, int32_t *const *outs);
     // Binary AIGER files' bytes in, decoded on the device (aiger_dev.cu).
     int upload_aiger(Batch &b, int count, const uint8_t *const *data, const size_t *len);
-    // Every graph as a binary AIGER file's bytes, encoded on the device.
-    int download_aiger(const Batch &b, std::vector<std::string> &files);
+    // Every graph as a binary AIGER file's bytes, encoded on the device,
+    // the files back to back in buf: offsets[0..G] (file g is
+    // [offsets[g], offsets[g+1])).  With buf null only the offsets are set.
+    int download_aiger(const Batch &b, uint8_t *buf, size_t cap, size_t *offsets);
     // Sets every graph's nLevels to its depth (AIGMan::readFromMemory).
     int batch_depth(Batch &b);
     int rw(Batch &b, bool useZeros, bool gpuDedup, RwStats *stats, RwDump *dump);

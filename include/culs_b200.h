@@ -104,6 +104,12 @@ int culs_batch_upload_aiger(culs_ctx *ctx, int count, const uint8_t *const *data
  * allocated by the library; free each with culs_buffer_free. */
 int culs_batch_download_aiger(culs_ctx *ctx, const culs_graph *g, uint8_t **data, size_t *len);
 void culs_buffer_free(void *p);
+/* The same files back to back in one caller buffer: offsets receives
+ * culs_graph_count(g) + 1 entries (file i is [offsets[i], offsets[i+1])).
+ * With buf null only the offsets are written (call once for the size, then
+ * with a buffer of at least offsets[count] bytes); a smaller cap is
+ * CULS_E_INVALID. */
+int culs_batch_download_aiger_into(culs_ctx *ctx, const culs_graph *g, uint8_t *buf, size_t cap, size_t *offsets);
 void culs_graph_free(culs_graph *g);
 int culs_graph_count(const culs_graph *g);
 /* Sizes and level of graph `index` (AIGMan::printStats, src/aig_manager.cu:604-612). */

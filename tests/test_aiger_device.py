@@ -65,6 +65,13 @@ def test_device_encode_equals_host_writer(ctx, tmp_path):
     out = d.download_aiger_all()
     for i, g in enumerate(gs):
         assert out[i] == host_bytes(g, tmp_path, f"w{i}"), i
+    # the library-allocated form gives the same bytes
+    ptrs = (C._vp * len(gs))()
+    lens = (C.ctypes.c_size_t * len(gs))()
+    assert C._lib.culs_batch_download_aiger(ctx.h, d.h, ptrs, lens) == 0
+    for i in range(len(gs)):
+        assert C.ctypes.string_at(ptrs[i], lens[i]) == out[i], i
+        C._lib.culs_buffer_free(ptrs[i])
     # after rw; st, and decoded again on the device
     ctx.rw_st(d)
     res = d.download_all()
