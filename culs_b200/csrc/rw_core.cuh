@@ -574,6 +574,18 @@ CULS_HD int mffc_size(const EvalIn &E, int root, const int (&leaves)[4], MffcTab
     }
 }
 
+// True when CalcMFFC of root w.r.t. these leaves is the root alone and no
+// table count reaches zero: its first two Decrease calls (the root's
+// fanins) are then all that runs.  A count reaches zero only for a fanin that
+// is not a leaf and has one reference, or -- both fanins the same node -- two.
+CULS_HD bool mffc_trivial(const EvalIn &E, int root, const int (&leaves)[4]) {
+    const int f0 = E.L0[root] >> 1, f1 = E.L1[root] >> 1;
+    const bool l0 = f0 == leaves[0] || f0 == leaves[1] || f0 == leaves[2] || f0 == leaves[3];
+    const bool l1 = f1 == leaves[0] || f1 == leaves[1] || f1 == leaves[2] || f1 == leaves[3];
+    if (f0 == f1) return l0 || E.ref[f0] > 2;
+    return (l0 || E.ref[f0] >= 2) && (l1 || E.ref[f1] >= 2);
+}
+
 CULS_HD int clz64(uint64_t x) {
 #if defined(__CUDA_ARCH__)
     return __clzll((long long)x);
@@ -639,13 +651,21 @@ CULS_HD void lib_probe_issue(const EvalIn &E, int q, uint32_t w, int isC, int *m
     p.num = num;
 }
 
+// IsDeleted (src/algorithms/rewrite.cu:312-316) on the MFFC's nodes: the
+// table entries whose count reached zero, nDel of them at del.
+CULS_HD bool mffc_member(int v, int nDel, const int *del) {
+    for (int j = 0; j < nDel; j++)
+        if (del[j] == v) return true;
+    return false;
+}
+
 template <class LevT>
-CULS_HD void lib_probe_finish(const EvalIn &E, const LibProbe &p, const int (&mffcId)[8], uint32_t zero, int *match,
-                              LevT *mlev, int stride, uint64_t &unmatched) {
+CULS_HD void lib_probe_finish(const EvalIn &E, const LibProbe &p, int nDel, const int *del, int *match, LevT *mlev,
+                              int stride, uint64_t &unmatched) {
     if (p.num < 0) return;
     // the slot carries the node's level, so a hit needs no second load
     const int2 r = region_resolve(E.tab, p.key, p.slot, E.status);
-    if (r.x != -1 && !mffc_deleted(r.x, mffcId, zero)) {
+    if (r.x != -1 && !mffc_member(r.x, nDel, del)) {
         match[p.num * stride] = r.x;
         mlev[p.num * stride] = (LevT)r.y;
     } else {
@@ -670,16 +690,15 @@ struct CutBest {
 
 // LevT holds library-node levels: int, or uint16_t when every level of the
 // graph plus the forest depth stays below 65,535.
+//
+// saved is CalcMFFC's count for this cut, and del its nDel MFFC nodes (the
+// table entries whose count reached zero), computed beforehand.
 template <class LevT>
 CULS_HD CutBest eval_cut(const EvalIn &E, int q, int cpos, uint32_t pk, int4 l, bool useZeros, int *match, LevT *mlev,
-                         int stride) {
+                         int stride, int saved, int nDel, const int *del) {
     CutBest best{-1, 0, -1};
     const uint32_t nLeaves = packed_nleaves(pk);
     const int leaves[4] = {l.x, l.y, l.z, nLeaves == 3 ? cpos : l.w};
-    MffcTab tab;
-    tab.size = 0;
-    const int saved = mffc_size(E, q, leaves, tab);
-    const uint32_t zero = mffc_zero_mask(tab);
     const uint32_t npn = E.lib->npn[pk & 0xFFFFu];
     const int uPhase = npn_phase(npn), cls = npn_class(npn);
     const uint32_t perm = *reinterpret_cast<const uint32_t *>(E.lib->perm4[npn_perm(npn)]);
@@ -704,10 +723,10 @@ CULS_HD CutBest eval_cut(const EvalIn &E, int q, int cpos, uint32_t pk, int4 l, 
         lib_probe_issue(E, q, bw.y, isC, match, mlev, stride, unmatched, p1);
         lib_probe_issue(E, q, bw.z, isC, match, mlev, stride, unmatched, p2);
         lib_probe_issue(E, q, bw.w, isC, match, mlev, stride, unmatched, p3);
-        lib_probe_finish(E, p0, tab.id, zero, match, mlev, stride, unmatched);
-        lib_probe_finish(E, p1, tab.id, zero, match, mlev, stride, unmatched);
-        lib_probe_finish(E, p2, tab.id, zero, match, mlev, stride, unmatched);
-        lib_probe_finish(E, p3, tab.id, zero, match, mlev, stride, unmatched);
+        lib_probe_finish(E, p0, nDel, del, match, mlev, stride, unmatched);
+        lib_probe_finish(E, p1, nDel, del, match, mlev, stride, unmatched);
+        lib_probe_finish(E, p2, nDel, del, match, mlev, stride, unmatched);
+        lib_probe_finish(E, p3, nDel, del, match, mlev, stride, unmatched);
     }
     const int nr = E.lib->nRoots[cls];
     for (int out = 0; out < nr; out++) {

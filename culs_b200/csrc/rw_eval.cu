@@ -60,6 +60,7 @@ struct EvalArgs {
     const int *wg;
     const DevGraph *dg;
     int useZeros;
+    int *mffcNodes;  // per warp of the grid, per item: up to 8 MFFC node positions
     int8_t *bestCut;
     uint8_t *bestOut;
     uint8_t *candFlag;
@@ -76,6 +77,9 @@ struct WarpItems {
     int off[kClassSlots];          // class-slot counts, then exclusive offsets
     uint16_t item[kWarpNodes * 8];  // local node * 8 + cut slot, in class-slot order
     int2 res[kWarpNodes * 8];       // {gain * 16 + root index, level} or {-1, 0}
+    uint16_t full[kWarpNodes * 8];  // items whose MFFC needs the full traversal
+    uint8_t saved[kWarpNodes * 8];  // per item: CalcMFFC's count
+    uint8_t nDel[kWarpNodes * 8];   // per item: its MFFC nodes (in EvalArgs::mffcNodes)
 };
 
 // A warp takes 32 * kNodesPerLane consecutive nodes of the graph-major
@@ -162,7 +166,54 @@ __global__ void __launch_bounds__(kEvalBlock, 8) k_evaluate(EvalArgs A) {
                     W.item[W.off[clsRank[h][k] >> 16] + (clsRank[h][k] & 0xFFFFu)] =
                         (uint16_t)((h * 32 + lane) * 8 + k);
         __syncwarp();
-        // 3. evaluate the items, 32 per round, in class-slot order
+        // 3. every item's MFFC: the trivial ones (the root alone, nothing
+        // deleted) at once, the others gathered and traversed 32 at a time,
+        // so the traversal runs in full rounds instead of in every round
+        int *const mffcNodes =
+            A.mffcNodes + ((int64_t)blockIdx.x * (kEvalBlock / 32) + (threadIdx.x >> 5)) * (kWarpNodes * 8 * 8);
+        int nFull = 0;
+        for (int it0 = 0; it0 < nItems; it0 += 32) {
+            const int it = it0 + lane;
+            bool full = false;
+            if (it < nItems) {
+                const int slot = W.item[it];
+                const int qq = A.byGraph[base + (slot >> 3)];
+                const int64_t idx = (int64_t)qq * 8 + (slot & 7);
+                const int4 l = A.cutL[idx];
+                const int leaves[4] = {l.x, l.y, l.z,
+                                       packed_nleaves((uint32_t)A.cutM[idx].y) == 3 ? A.dg[A.wg[qq]].cpos : l.w};
+                full = !mffc_trivial(A.E, qq, leaves);
+                W.saved[it] = 1;
+                W.nDel[it] = 0;
+            }
+            const unsigned b = __ballot_sync(0xffffffffu, full);
+            if (full) W.full[nFull + __popc(b & ((1u << lane) - 1u))] = (uint16_t)it;
+            nFull += __popc(b);
+        }
+        __syncwarp();
+        for (int k = lane; k < nFull; k += 32) {
+            const int it = W.full[k];
+            const int slot = W.item[it];
+            const int qq = A.byGraph[base + (slot >> 3)];
+            const int64_t idx = (int64_t)qq * 8 + (slot & 7);
+            const int4 l = A.cutL[idx];
+            const int leaves[4] = {l.x, l.y, l.z,
+                                   packed_nleaves((uint32_t)A.cutM[idx].y) == 3 ? A.dg[A.wg[qq]].cpos : l.w};
+            MffcTab tab;
+            tab.size = 0;
+            const int saved = mffc_size(A.E, qq, leaves, tab);
+            const uint32_t zero = mffc_zero_mask(tab);
+            int *del = mffcNodes + it * 8;
+            int n = 0;
+#define CULS_KEEP(k)             \
+    if ((zero >> k) & 1u) del[n++] = tab.id[k];
+            CULS_EACH8(CULS_KEEP)
+#undef CULS_KEEP
+            W.saved[it] = (uint8_t)saved;
+            W.nDel[it] = (uint8_t)n;
+        }
+        __syncwarp();
+        // 4. evaluate the items, 32 per round, in class-slot order
         for (int it = lane; it < nItems; it += 32) {
             const int slot = W.item[it];
             const int qq = A.byGraph[base + (slot >> 3)];
@@ -174,14 +225,16 @@ __global__ void __launch_bounds__(kEvalBlock, 8) k_evaluate(EvalArgs A) {
             const int4 l = A.cutL[idx];
             const int cpos = A.dg[g].cpos;
             CutBest b;
+            const int saved = W.saved[it], nDel = W.nDel[it];
+            const int *del = mffcNodes + it * 8;
             if (4 + A.E.lib->nNodes[npn_class(A.E.lib->npn[pk & 0xFFFFu])] <= kLibFast)
-                b = eval_cut(E, qq, cpos, pk, l, A.useZeros != 0, match, mlev, kEvalBlock);
+                b = eval_cut(E, qq, cpos, pk, l, A.useZeros != 0, match, mlev, kEvalBlock, saved, nDel, del);
             else  // a large forest: scratch in global memory
-                b = eval_cut(E, qq, cpos, pk, l, A.useZeros != 0, gmatch, gmlev, gstride);
+                b = eval_cut(E, qq, cpos, pk, l, A.useZeros != 0, gmatch, gmlev, gstride, saved, nDel, del);
             if (b.out >= 0) W.res[slot] = make_int2(b.gain * 16 + b.out, b.level);
         }
         __syncwarp();
-        // 4. fold each of this lane's nodes' cuts in slot order
+        // 5. fold each of this lane's nodes' cuts in slot order
 #pragma unroll
         for (int h = 0; h < kNodesPerLane; h++) {
             if (q[h] < 0) continue;
@@ -222,7 +275,8 @@ int rw_evaluate(ExecCtx &X, RwWork &w, const Batch &b) {
     w.cand = X.ar->get<int>(N);
     const unsigned evalGrid = X.grid(N, kEvalBlock);
     int *scratch = X.ar->get<int>((size_t)2 * kLibSlots * evalGrid * kEvalBlock);
-    if (!slots || !dOff || !w.bestCut || !w.bestOut || !candFlag || !w.cand || !scratch)
+    int *mffcNodes = X.ar->get<int>((size_t)evalGrid * (kEvalBlock / 32) * kWarpNodes * 8 * 8);
+    if (!slots || !dOff || !w.bestCut || !w.bestOut || !candFlag || !w.cand || !scratch || !mffcNodes)
         return X.fail(CULS_E_OOM, "rw: scratch arena exhausted (table)");
     w.tab = RegionTable{slots, dOff};
     int rc;
@@ -236,7 +290,7 @@ int rw_evaluate(ExecCtx &X, RwWork &w, const Batch &b) {
         k_table_build<<<X.grid(N), kBlock, 0, s>>>(w.nL0, N, w.byGraph, w.w0, w.w1, w.wg, w.wlev, w.dg, w.tab,
                                                    X.status);
         EvalArgs A{w.nL0, N, w.byGraph, scratch, EvalIn{w.w0, w.w1, w.ref, w.wlev, X.lib, TabRegion{}, X.status}, w.tab,
-                   w.cutL, w.cutM, w.wg, w.dg, w.useZeros ? 1 : 0, w.bestCut, w.bestOut, candFlag};
+                   w.cutL, w.cutM, w.wg, w.dg, w.useZeros ? 1 : 0, mffcNodes, w.bestCut, w.bestOut, candFlag};
         X.mark(kMkEvalK0);
         // 16-bit library levels when no level of the batch, plus a forest's
         // depth (at most 50 nodes), can reach 65,535
