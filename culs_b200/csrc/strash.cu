@@ -74,8 +74,10 @@ __global__ void __launch_bounds__(kBlock) k_dead_queue(WorkQueue q, const int *L
     }
 }
 
-// pending[v] = AND fanins of a live AND node; outdeg[u] = live AND fanouts.
-__global__ void k_live_degrees(int64_t M, const int *L0, const int *L1, const uint8_t *dead, int *pending, int *outdeg,
+// level[v] = 1 for a live AND node without AND fanins (the seeds), -1 for the
+// other AND nodes, 0 for the constant and PIs; outdeg[u] = live AND fanouts
+// (a node whose two fanins are one node counts once).
+__global__ void k_live_degrees(int64_t M, const int *L0, const int *L1, const uint8_t *dead, int *level, int *outdeg,
                                uint8_t *liveFlag, uint8_t *seedFlag) {
     int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < M; v += stride) {
@@ -89,12 +91,12 @@ __global__ void k_live_degrees(int64_t M, const int *L0, const int *L1, const ui
                 pend++;
                 atomicAdd(&outdeg[u0], 1);
             }
-            if (L0[u1] >= 0) {
+            if (L0[u1] >= 0 && u1 != u0) {
                 pend++;
                 atomicAdd(&outdeg[u1], 1);
             }
         }
-        pending[v] = pend;
+        level[v] = a < 0 ? 0 : (live && pend == 0 ? 1 : -1);
         seedFlag[v] = live && pend == 0;
     }
 }
@@ -105,7 +107,7 @@ __global__ void k_csr_fill(int64_t M, const int *L0, const int *L1, const uint8_
         if (!liveFlag[v]) continue;
         int u0 = L0[v] >> 1, u1 = L1[v] >> 1;
         if (L0[u0] >= 0) adj[atomicAdd(&cursor[u0], 1)] = (int)v;
-        if (L0[u1] >= 0) adj[atomicAdd(&cursor[u1], 1)] = (int)v;
+        if (L0[u1] >= 0 && u1 != u0) adj[atomicAdd(&cursor[u1], 1)] = (int)v;
     }
 }
 
@@ -113,15 +115,18 @@ __global__ void k_csr_fill(int64_t M, const int *L0, const int *L1, const uint8_
 // constant: 0), one launch per level.  The queue's levels are consecutive
 // segments of `items`; launch L reads its segment's start and size from a
 // three-slot ring (written by launch L - 1, which has finished), releases
-// the fanouts of every node of level L, and appends each fanout whose last
-// pending fanin this was to level L + 1's segment.  Thread 0 of block 0
+// the fanouts of every node of level L, and appends to level L + 1's
+// segment each fanout whose other fanin finished earlier (no pending
+// counters: a node's level is written when it is appended, so the levels up
+// to L are all known when launch L starts, and of two fanins on the same
+// level the one at the higher position appends).  Thread 0 of block 0
 // sets the next segment's start and clears the slot that launch L + 1 will
 // append to, which no other block of launch L touches.  No thread waits on
 // another.  ring[0..2]: segment sizes, ring[3..5]: segment starts, both by
 // level mod 3.
 __global__ void __launch_bounds__(kBlock) k_level_step(int L, int *items, int *ring, const int *off, const int *adj,
-                                                        int *pending, int *level, const int *gid, int *graphLevels,
-                                                        int *maxLevel) {
+                                                        const int *L0, const int *L1, int *level, const int *gid,
+                                                        int *graphLevels, int *maxLevel) {
     const int r = L % 3;
     const int start = ring[3 + r], n = ring[r];
     if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -136,21 +141,31 @@ __global__ void __launch_bounds__(kBlock) k_level_step(int L, int *items, int *r
     const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
     for (int64_t i0 = ((int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 32; i0 < n; i0 += warps * 32) {
         const int64_t i = i0 + lane;
-        int k = 0, e = 0;
+        int k = 0, e = 0, v = -1;
         if (i < n) {
-            const int v = items[start + i];
-            level[v] = L;
+            v = items[start + i];
             agg_max(graphLevels, gid[v], L);
             k = off[v];
             e = off[v + 1];
         }
-        // release the fanouts, one fanout per lane per round
+        // release the fanouts, one fanout per lane per round: v pushes w when
+        // w's other fanin is not an AND node, is below level L, or is on
+        // level L at a lower position (levels up to L are all set when the
+        // launch starts; later ones read as -1 or L + 1)
         while (__any_sync(0xffffffffu, k < e)) {
             bool push = false;
             int w = 0;
             if (k < e) {
                 w = adj[k++];
-                push = atomicSub(&pending[w], 1) == 1;
+                const int a = L0[w] >> 1, b = L1[w] >> 1;
+                const int u = a == v ? b : a;
+                if (u == v || L0[u] < 0) {
+                    push = true;
+                } else {
+                    const int lu = level[u];
+                    push = lu >= 0 && (lu < L || (lu == L && u < v));
+                }
+                if (push) level[w] = L + 1;
             }
             const unsigned b = __ballot_sync(0xffffffffu, push);
             if (b) {
@@ -513,7 +528,7 @@ int Engine::strash_core(Batch &b, int64_t M, const int *L0, const int *L1, const
         launches_ += 2;
     } else {
     check(cudaMemsetAsync(off, 0, sizeof(int) * (M + 2), s), "memset");
-    k_live_degrees<<<gridM, kBlock, 0, s>>>(M, L0, L1, dead, pending, off, liveFlag, flags);
+    k_live_degrees<<<gridM, kBlock, 0, s>>>(M, L0, L1, dead, level, off, liveFlag, flags);
     check(scan_exclusive(off, off, M + 1, nullptr, ar_, s), "scan");
     int *cursor = cnt;  // reuse
     check(cudaMemcpyAsync(cursor, off, sizeof(int) * (M + 1), cudaMemcpyDeviceToDevice, s), "copy");
@@ -530,7 +545,6 @@ int Engine::strash_core(Batch &b, int64_t M, const int *L0, const int *L1, const
     check(cudaMemsetAsync(qc, 0, sizeof(int) * 8, s), "memset");
     check(cudaMemsetAsync(ring, 0, sizeof(int) * 8, s), "memset");
     check(cudaMemsetAsync(graphLevels, 0, sizeof(int) * (G + 1), s), "memset");
-    check(cudaMemsetAsync(level, 0, sizeof(int) * (M + 1), s), "memset");
     check(compact_flags(flags, M, items, ring + 1, ar_, s), "compact");     // level 1: the seeds
     check(compact_flags(liveFlag, M, liveIdx, qc + 3, ar_, s), "compact");  // live list and count
     launches_ += 2;
@@ -541,7 +555,7 @@ int Engine::strash_core(Batch &b, int64_t M, const int *L0, const int *L1, const
     int L = 1;
     while (true) {
         for (int t = 0; t < 64; t++, L++)
-            k_level_step<<<gridQ, kBlock, 0, s>>>(L, items, ring, off, adj, pending, level, gidA, graphLevels, qc + 4);
+            k_level_step<<<gridQ, kBlock, 0, s>>>(L, items, ring, off, adj, L0, L1, level, gidA, graphLevels, qc + 4);
         launches_ += 64;
         check(cudaMemcpyAsync(hostSmall_, ring, sizeof(int) * 6, cudaMemcpyDeviceToHost, s), "d2h");
         if (sync()) return -1;
