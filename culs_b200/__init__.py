@@ -85,6 +85,10 @@ _lib.culs_submit.argtypes = [_vp, _ip, _ip, _ip, ctypes.c_int32, ctypes.c_int32,
 _lib.culs_poll.argtypes = [_vp, ctypes.c_int64, _ip, _ip, _ip, _ip]
 _lib.culs_wait.argtypes = [_vp, ctypes.c_int64, ctypes.c_int]
 _lib.culs_fetch.argtypes = [_vp, ctypes.c_int64, _ip, _ip, _ip, ctypes.POINTER(ctypes.c_double)]
+_lib.culs_submit_aiger.argtypes = [_vp, _vp, ctypes.c_size_t, ctypes.c_uint32, ctypes.c_uint32,
+                                   ctypes.POINTER(ctypes.c_int64)]
+_lib.culs_fetch_aiger.argtypes = [_vp, ctypes.c_int64, _vp, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t),
+                                  ctypes.POINTER(ctypes.c_double)]
 _lib.culs_graph_download.argtypes = [_vp, _vp, ctypes.c_int, _ip, _ip, _ip]
 _lib.culs_rw.argtypes = [_vp, _vp, ctypes.c_uint32]
 _lib.culs_st.argtypes = [_vp, _vp, ctypes.c_uint32]
@@ -324,6 +328,24 @@ class Context:
         lat = ctypes.c_double()
         self._err(_lib.culs_fetch(self.h, job, _p(f0), _p(f1), _p(outs), ctypes.byref(lat)), "fetch")
         return Aig(st["nPIs"], f0, f1, outs[:st["nPOs"]], st["nLevels"]), lat.value
+
+    def submit_aiger(self, data, zeros=False, gpu_dedup=True, cpu_st=False) -> int:
+        """A served job given as a binary AIGER file's bytes."""
+        f = (RW_ZEROS if zeros else 0) | (RW_GPU_DEDUP if gpu_dedup else 0)
+        a = np.frombuffer(data, np.uint8)
+        job = ctypes.c_int64()
+        self._err(_lib.culs_submit_aiger(self.h, a.ctypes.data if len(a) else None, len(a), f,
+                                         ST_CPU if cpu_st else 0, ctypes.byref(job)), "submit")
+        return job.value
+
+    def fetch_aiger(self, job):
+        """The finished AIGER job's result (bytes) and its latency in ms."""
+        n = ctypes.c_size_t()
+        self._err(_lib.culs_fetch_aiger(self.h, job, None, 0, ctypes.byref(n), None), "fetch")
+        buf = ctypes.create_string_buffer(max(n.value, 1))
+        lat = ctypes.c_double()
+        self._err(_lib.culs_fetch_aiger(self.h, job, buf, n.value, ctypes.byref(n), ctypes.byref(lat)), "fetch")
+        return buf.raw[:n.value], lat.value
 
     def rw_stats(self):
         out = (ctypes.c_int64 * 11)()

@@ -289,6 +289,26 @@ int culs_submit(culs_ctx *ctx, const int32_t *fanin0, const int32_t *fanin1, con
     return s->submit(fanin0, fanin1, outs, nPIs, nPOs, nAnds, rwFlags, stFlags, job);
 }
 
+int culs_submit_aiger(culs_ctx *ctx, const uint8_t *data, size_t len, uint32_t rwFlags, uint32_t stFlags,
+                      int64_t *job) {
+    if (!ctx) return CULS_E_INVALID;
+    auto s = server_of(ctx);
+    if (!s) return CULS_E_INVALID;
+    return s->submit_aiger(data, len, rwFlags, stFlags, job);
+}
+
+int culs_fetch_aiger(culs_ctx *ctx, int64_t job, uint8_t *buf, size_t cap, size_t *len, double *latencyMs) {
+    if (!ctx) return CULS_E_INVALID;
+    auto s = server_of(ctx);
+    if (!s) return CULS_E_NOTFOUND;
+    int rc = s->fetch_aiger(job, buf, cap, len, latencyMs);
+    if (rc < 0 && rc != CULS_E_BUSY && rc != CULS_E_NOTFOUND) {
+        std::lock_guard<std::mutex> lk(ctx->mu);
+        ctx->err = s->lastError();
+    }
+    return rc;
+}
+
 int culs_poll(culs_ctx *ctx, int64_t job, int32_t *nPIs, int32_t *nPOs, int32_t *nAnds, int32_t *nLevels) {
     if (!ctx) return CULS_E_INVALID;
     auto s = server_of(ctx);

@@ -1,5 +1,7 @@
 // Served mode (serve.cuh).
 #include <algorithm>
+#include <climits>
+#include <cstring>
 
 #include "serve.cuh"
 
@@ -65,6 +67,75 @@ int Server::submit(const int32_t *f0, const int32_t *f1, const int32_t *outs, in
     return CULS_OK;
 }
 
+// The header fields of a binary AIGER file ("aig M I L O A"), as the host
+// reader checks them (host_aiger.cpp): the job's sizes for admission.
+static bool aiger_sizes(const uint8_t *p, size_t len, int32_t &nPIs, int32_t &nPOs, int32_t &nAnds) {
+    const uint8_t *end = p + len;
+    if (len < 4 || memcmp(p, "aig ", 4) != 0) return false;
+    p += 4;
+    long long v[5];
+    for (int k = 0; k < 5; k++) {
+        if (p >= end || *p < '0' || *p > '9') return false;
+        long long x = 0;
+        while (p < end && *p >= '0' && *p <= '9') {
+            x = x * 10 + (*p++ - '0');
+            if (x > INT32_MAX) return false;
+        }
+        if (p >= end || *p++ != (k < 4 ? ' ' : '\n')) return false;
+        v[k] = x;
+    }
+    if (v[2] != 0 || v[0] != v[1] + v[4] || v[0] + 1 > INT32_MAX / 2) return false;
+    nPIs = (int32_t)v[1];
+    nPOs = (int32_t)v[3];
+    nAnds = (int32_t)v[4];
+    return true;
+}
+
+int Server::submit_aiger(const uint8_t *data, size_t len, uint32_t rwFlags, uint32_t stFlags, int64_t *id) {
+    if (!id || !data) return CULS_E_INVALID;
+    auto job = std::make_unique<ServeJob>();
+    if (!aiger_sizes(data, len, job->nPIs, job->nPOs, job->nAnds)) return CULS_E_IO;
+    job->rwFlags = rwFlags;
+    job->stFlags = stFlags;
+    job->aiger = true;
+    job->file.assign(reinterpret_cast<const char *>(data), len);
+    job->state = kQueued;
+    job->tSubmit = std::chrono::steady_clock::now();
+    {
+        std::lock_guard<std::mutex> lk(mu_);
+        job->id = nextId_++;
+        *id = job->id;
+        queue_.push_back(job->id);
+        jobs_[job->id] = std::move(job);
+    }
+    cvWork_.notify_one();
+    return CULS_OK;
+}
+
+int Server::fetch_aiger(int64_t id, uint8_t *buf, size_t cap, size_t *len, double *latencyMs) {
+    if (!len) return CULS_E_INVALID;
+    std::unique_ptr<ServeJob> j;
+    {
+        std::lock_guard<std::mutex> lk(mu_);
+        auto it = jobs_.find(id);
+        if (it == jobs_.end()) return CULS_E_NOTFOUND;
+        const int st = it->second->state;
+        if (st == kQueued || st == kRunning) return CULS_E_BUSY;
+        if (!it->second->aiger) return CULS_E_INVALID;  // fetched with culs_fetch
+        if (st == kDone) {
+            *len = it->second->file.size();
+            if (!buf) return CULS_OK;
+            if (cap < *len) return CULS_E_INVALID;
+        }
+        j = std::move(it->second);
+        jobs_.erase(it);
+    }
+    if (latencyMs) *latencyMs = std::chrono::duration<double, std::milli>(j->tDone - j->tSubmit).count();
+    if (j->state != kDone) return j->state;
+    memcpy(buf, j->file.data(), j->file.size());
+    return CULS_OK;
+}
+
 int Server::poll(int64_t id, int32_t *nPIs, int32_t *nPOs, int32_t *nAnds, int32_t *nLevels) {
     std::lock_guard<std::mutex> lk(mu_);
     auto it = jobs_.find(id);
@@ -103,6 +174,7 @@ int Server::fetch(int64_t id, int32_t *f0, int32_t *f1, int32_t *outs, double *l
         if (it == jobs_.end()) return CULS_E_NOTFOUND;
         const int st = it->second->state;
         if (st == kQueued || st == kRunning) return CULS_E_BUSY;
+        if (it->second->aiger) return CULS_E_INVALID;  // fetched with culs_fetch_aiger
         j = std::move(it->second);
         jobs_.erase(it);
     }
@@ -134,7 +206,7 @@ void Server::worker(Engine &eng, std::mutex &engMu) {
                 ServeJob *j = jobs_[id].get();
                 const size_t need = kBytesPerObj * (1 + (size_t)j->nPIs + j->nAnds);
                 const bool fits = batch.empty() || (bytes + need <= admit_ && (int)batch.size() < maxBatch_);
-                if (j->rwFlags == head->rwFlags && j->stFlags == head->stFlags && fits) {
+                if (j->rwFlags == head->rwFlags && j->stFlags == head->stFlags && j->aiger == head->aiger && fits) {
                     batch.push_back(j);
                     bytes += need;
                     j->state = kRunning;
@@ -153,7 +225,82 @@ void Server::worker(Engine &eng, std::mutex &engMu) {
     }
 }
 
+// A batch of AIGER jobs: decoded on the device together; when the batch's
+// bytes do not decode, every job is tried alone, so that a malformed file
+// fails its own job only.  Results are encoded on the device.
+void Server::run_aiger(Engine &eng, std::mutex &engMu, std::vector<ServeJob *> &batch) {
+    std::vector<std::pair<ServeJob *, int>> failed;
+    std::vector<ServeJob *> run = batch;
+    int rc;
+    std::string why;
+    {
+        std::lock_guard<std::mutex> lk(engMu);
+        auto upload = [&](Batch &b, const std::vector<ServeJob *> &js) {
+            std::vector<const uint8_t *> data(js.size());
+            std::vector<size_t> len(js.size());
+            for (size_t i = 0; i < js.size(); i++) {
+                data[i] = reinterpret_cast<const uint8_t *>(js[i]->file.data());
+                len[i] = js[i]->file.size();
+            }
+            return eng.upload_aiger(b, (int)js.size(), data.data(), len.data());
+        };
+        Batch b;
+        rc = upload(b, run);
+        if (rc == CULS_E_IO && run.size() > 1) {
+            std::vector<ServeJob *> good;
+            for (ServeJob *j : run) {
+                Batch one;
+                const int r = upload(one, std::vector<ServeJob *>{j});
+                if (r == CULS_OK)
+                    good.push_back(j);
+                else
+                    failed.emplace_back(j, r);
+            }
+            run = good;
+            rc = run.empty() ? CULS_OK : upload(b, run);
+        }
+        if (rc == CULS_OK && !run.empty()) {
+            const uint32_t rwf = run[0]->rwFlags, stf = run[0]->stFlags;
+            RwStats st{};
+            rc = eng.rw(b, (rwf & CULS_RW_ZEROS) != 0, (rwf & CULS_RW_GPU_DEDUP) != 0, &st, nullptr);
+            if (rc == CULS_OK) rc = eng.st(b, (stf & CULS_ST_CPU) != 0);
+            std::vector<size_t> off(run.size() + 1);
+            if (rc == CULS_OK) rc = eng.download_aiger(b, nullptr, 0, off.data());
+            std::string all;
+            if (rc == CULS_OK) {
+                all.resize(off[run.size()]);
+                rc = eng.download_aiger(b, reinterpret_cast<uint8_t *>(&all[0]), all.size(), off.data());
+            }
+            if (rc == CULS_OK)
+                for (size_t i = 0; i < run.size(); i++) {
+                    const DevGraph &d = b.hg[i];
+                    run[i]->file.assign(all, off[i], off[i + 1] - off[i]);
+                    run[i]->nPIs = d.nPIs;
+                    run[i]->nPOs = d.nPOs;
+                    run[i]->nAnds = d.nAnds;
+                    run[i]->nLevels = d.nLevels;
+                }
+        }
+        if (rc != CULS_OK || !failed.empty()) why = eng.error();
+    }
+    const auto now = std::chrono::steady_clock::now();
+    std::lock_guard<std::mutex> lk(mu_);
+    if (rc != CULS_OK || !failed.empty()) err_ = why;
+    for (ServeJob *j : run) {
+        j->state = rc == CULS_OK ? kDone : rc;
+        j->tDone = now;
+    }
+    for (auto &f : failed) {
+        f.first->state = f.second;
+        f.first->tDone = now;
+    }
+}
+
 void Server::run_batch(Engine &eng, std::mutex &engMu, std::vector<ServeJob *> &batch) {
+    if (batch[0]->aiger) {
+        run_aiger(eng, engMu, batch);
+        return;
+    }
     const int n = (int)batch.size();
     std::vector<const int32_t *> f0(n), f1(n), po(n);
     std::vector<int32_t> nPIs(n), nPOs(n), nAnds(n);

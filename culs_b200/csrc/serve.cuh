@@ -16,6 +16,7 @@
 #include <deque>
 #include <memory>
 #include <mutex>
+#include <string>
 #include <thread>
 #include <unordered_map>
 #include <vector>
@@ -29,6 +30,8 @@ struct ServeJob {
     uint32_t rwFlags = 0, stFlags = 0;  // CULS_RW_* / CULS_ST_*
     int32_t nPIs = 0, nPOs = 0, nAnds = 0, nLevels = 0;
     std::vector<int32_t> f0, f1, outs;  // the input, replaced by the result
+    bool aiger = false;                 // the job came and goes as binary AIGER bytes
+    std::string file;                   // those bytes (input, replaced by the result)
     int state = 0;                      // kQueued, kRunning, kDone, or a CULS_E_* code
     std::chrono::steady_clock::time_point tSubmit, tDone;
 };
@@ -48,6 +51,13 @@ class Server {
 
     int submit(const int32_t *f0, const int32_t *f1, const int32_t *outs, int32_t nPIs, int32_t nPOs, int32_t nAnds,
                uint32_t rwFlags, uint32_t stFlags, int64_t *id);
+    // A job given as a binary AIGER file's bytes; its result is fetched the
+    // same way (fetch_aiger).  The header is checked here; the AND section
+    // is decoded on the device with the rest of the job's batch.
+    int submit_aiger(const uint8_t *data, size_t len, uint32_t rwFlags, uint32_t stFlags, int64_t *id);
+    // With buf null *len receives the result's size; otherwise the result
+    // (at most cap bytes) is copied and the job forgotten.
+    int fetch_aiger(int64_t id, uint8_t *buf, size_t cap, size_t *len, double *latencyMs);
     // CULS_OK with the result's sizes when done, CULS_E_BUSY while queued or
     // running, CULS_E_NOTFOUND for an unknown id, or the job's error code.
     int poll(int64_t id, int32_t *nPIs, int32_t *nPOs, int32_t *nAnds, int32_t *nLevels);
@@ -60,6 +70,7 @@ class Server {
   private:
     void worker(Engine &eng, std::mutex &engMu);
     void run_batch(Engine &eng, std::mutex &engMu, std::vector<ServeJob *> &batch);
+    void run_aiger(Engine &eng, std::mutex &engMu, std::vector<ServeJob *> &batch);
 
     Engine &eng_;
     std::mutex &engMu_;

@@ -186,6 +186,16 @@ int culs_submit(culs_ctx *ctx, const int32_t *fanin0, const int32_t *fanin1, con
 int culs_poll(culs_ctx *ctx, int64_t job, int32_t *nPIs, int32_t *nPOs, int32_t *nAnds, int32_t *nLevels);
 int culs_wait(culs_ctx *ctx, int64_t job, int timeoutMs);
 int culs_fetch(culs_ctx *ctx, int64_t job, int32_t *fanin0, int32_t *fanin1, int32_t *outs, double *latencyMs);
+/* A served job given as a binary AIGER file's bytes (copied): its header is
+ * checked at once (CULS_E_IO when the host reader would refuse it), its AND
+ * section decoded on the device with the rest of its batch, which holds AIGER
+ * jobs only; a file whose bytes do not decode fails its own job with
+ * CULS_E_IO.  culs_fetch_aiger returns the result as a binary AIGER file:
+ * with buf null *len receives its size; otherwise it is copied (cap >=
+ * *len) and the job forgotten.  culs_poll and culs_wait serve both kinds. */
+int culs_submit_aiger(culs_ctx *ctx, const uint8_t *data, size_t len, uint32_t rwFlags, uint32_t stFlags,
+                      int64_t *job);
+int culs_fetch_aiger(culs_ctx *ctx, int64_t job, uint8_t *buf, size_t cap, size_t *len, double *latencyMs);
 
 /* --------------------------------------------------------------- tuning
  * Launch and schedule parameters: they change speed only, never results.

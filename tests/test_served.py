@@ -83,6 +83,49 @@ def test_served_workers_match_oracle(ctx):
     assert same_graph(h.download(), oracle_rw_st(gs[0]).graph())
 
 
+def test_served_aiger_jobs_match_oracle(ctx, tmp_path):
+    """Jobs given as binary AIGER bytes, mixed with array jobs: decoded and
+    encoded on the device in batches of their own kind; a file whose header
+    is fine but whose AND section does not decode fails its own job only."""
+    gs = graphs()
+    files = []
+    for i, g in enumerate(gs):
+        p = tmp_path / f"j{i}.aig"
+        C.write_aiger(p, g)
+        files.append(p.read_bytes())
+    bad = b"aig 3 2 0 1 1\n6\n\x00\x02c\n"  # delta 0: the fanin does not precede its node
+    ctx.serve_start(workers=2)
+    try:
+        jobs = []
+        for i, (g, f) in enumerate(zip(gs * 2, files * 2)):
+            jobs.append(("aig", ctx.submit_aiger(f, zeros=(i == 1)), g, i == 1))
+            if i == 2:
+                jobs.append(("bad", ctx.submit_aiger(bad), None, False))
+            jobs.append(("arr", ctx.submit(g), g, False))
+        with pytest.raises(C.CulsError) as e:  # a header the host reader refuses
+            ctx.submit_aiger(b"aag 1 1 0 1 0\n2\n")
+        assert e.value.code == C.CULS_E_IO
+        for kind, job, g, zeros in jobs:
+            if kind == "bad":
+                with pytest.raises(C.CulsError) as e:
+                    ctx.wait(job, 60000)
+                assert e.value.code == C.CULS_E_IO
+                continue
+            assert ctx.wait(job, 60000)
+            ref = oracle_rw_st(g, zeros=zeros).graph()
+            if kind == "aig":
+                data, lat = ctx.fetch_aiger(job)
+                p = tmp_path / "out.aig"
+                p.write_bytes(data)
+                out = C.read_aiger(p)
+            else:
+                out, lat = ctx.fetch(job)
+            assert same_graph(out, ref), (kind, job)
+            assert lat >= 0.0
+    finally:
+        ctx.serve_stop()
+
+
 def test_served_job_error_is_reported():
     small = C.Context(hbm_budget=1 << 20)
     small.serve_start()
