@@ -35,7 +35,7 @@ RW_ZEROS, RW_GPU_DEDUP, RW_DUMP = 1, 2, 4
 SERVE_BYTES_PER_OBJ = 720  # device bytes the served mode's admission charges per object
 ST_CPU = 1
 STAT_NAMES = ["replaced", "replaced_pos", "replaced_zero", "reverted", "compromised", "pre_eval", "small_cut",
-              "new_idx", "expected", "new_nodes", "candidates"]
+              "new_idx", "expected", "new_nodes", "candidates", "enum_warp_pairs"]
 DUMPS = ["reorder_f0", "reorder_f1", "reorder_out", "cuts", "selected", "replace", "new_f0", "new_f1", "choice"]
 
 
@@ -348,8 +348,8 @@ class Context:
         return buf.raw[:n.value], lat.value
 
     def rw_stats(self):
-        out = (ctypes.c_int64 * 11)()
-        _lib.culs_rw_stats(self.h, out, 11)
+        out = (ctypes.c_int64 * len(STAT_NAMES))()
+        _lib.culs_rw_stats(self.h, out, len(STAT_NAMES))
         return dict(zip(STAT_NAMES, list(out)))
 
     def dump(self):

@@ -373,9 +373,9 @@ int culs_autotune(culs_ctx *ctx, const culs_graph *sample, int rounds) {
 int culs_rw_stats(culs_ctx *ctx, int64_t *out, int n) {
     if (!ctx || !out) return CULS_E_INVALID;
     const culs::RwStats &s = ctx->last;
-    int64_t v[11] = {s.replaced, s.replacedPos, s.replacedZero, s.reverted, s.compromised, s.preEval,
-                     s.smallCut, s.newIdx,      s.expected,     s.newNodes, s.candidates};
-    for (int i = 0; i < n && i < 11; i++) out[i] = v[i];
+    int64_t v[12] = {s.replaced, s.replacedPos, s.replacedZero, s.reverted, s.compromised, s.preEval,
+                     s.smallCut, s.newIdx,      s.expected,     s.newNodes, s.candidates, s.warpPairs};
+    for (int i = 0; i < n && i < 12; i++) out[i] = v[i];
     return CULS_OK;
 }
 

@@ -44,6 +44,7 @@ struct DevGraph {
 struct RwStats {
     long long replaced, replacedPos, replacedZero, reverted, compromised, preEval, smallCut, newIdx, expected,
         newNodes, candidates;
+    long long warpPairs;  // fanin-cut pairs the one-node-per-warp enumeration replayed
 };
 
 // Device blocks freed by batches, kept for the next batch of a context (a

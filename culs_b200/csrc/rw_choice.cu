@@ -240,8 +240,11 @@ int rw_choice(ExecCtx &X, Batch &b, RwWork &w, RwStats *stats) {
                  w.repW,   w.useZeros ? 1 : 0,  stack,  (int)stackCap,       w.choice, dstats, X.status};
     k_choice<<<(G + 63) / 64, 64, 0, s>>>(A, G);
     X.launched(1);
-    unsigned long long hs[8];
+    unsigned long long hs[8], warpPairs = 0;
     if ((rc = X.check(cudaMemcpyAsync(hs, dstats, sizeof hs, cudaMemcpyDeviceToHost, s), "d2h"))) return rc;
+    if (w.warpPairs &&
+        (rc = X.check(cudaMemcpyAsync(&warpPairs, w.warpPairs, sizeof warpPairs, cudaMemcpyDeviceToHost, s), "d2h")))
+        return rc;
     if ((rc = X.sync())) return rc;
     if ((rc = X.status_check("rw choice"))) return rc;
     if (stats) {
@@ -257,6 +260,7 @@ int rw_choice(ExecCtx &X, Batch &b, RwWork &w, RwStats *stats) {
         stats->smallCut = 0;
         stats->newNodes = w.nNew;
         stats->candidates = nCand;
+        stats->warpPairs = (long long)warpPairs;
     }
     (void)b;
     return 0;

@@ -214,7 +214,9 @@ int culs_autotune(culs_ctx *ctx, const culs_graph *sample, int rounds);
 /* Counters of the last culs_rw (the summary CPUSolver::Rewrite prints,
  * src/algorithms/rewrite.cu:896-897,926): replaced, replaced with positive
  * gain, replaced with zero gain, reverted, compromised, without a cut, small
- * cut, without a replacement, real reduction, new nodes built, candidates. */
+ * cut, without a replacement, real reduction, new nodes built, candidates;
+ * then (no reference counterpart) the fanin-cut pairs the one-node-per-warp
+ * cut enumeration replayed. */
 int culs_rw_stats(culs_ctx *ctx, int64_t *out, int n);
 
 /* Per-node intermediate results of the last culs_rw run with CULS_RW_DUMP,

@@ -285,6 +285,9 @@ def test_both_enumeration_schedules_match_oracle(wide_min):
             d = c.upload(g)
             c.rw(d, dump=True)
             D = c.dump()
+            # pairs replayed by the warp-per-node schedule: none when every
+            # level runs one node per thread
+            assert (c.rw_stats()["enum_warp_pairs"] > 0) == (wide_min > 1), name
             o = Oracle()
             o.set_graph(to_oracle(g))
             o.rw()
