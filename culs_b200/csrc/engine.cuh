@@ -203,8 +203,13 @@ class Engine {
     // an in-order dataflow instead of a worklist).
     // unique: every node is its own representative (no duplicate merged):
     // the output is the input graph renumbered in processing order.
+    // procInv / procPos (not topo): an order of the positions that is
+    // topological up to a few fanins placed later (procInv[k] = position at
+    // order index k, procPos its inverse); levels then come from in-order
+    // passes instead of the level-synchronous worklist.
     int strash_core(Batch &b, int64_t M, const int *L0, const int *L1, const int *gid, const int *lid, const int *po,
-                    bool idOrder, bool removeDangling, bool foldTrivial, bool topo, bool unique = false);
+                    bool idOrder, bool removeDangling, bool foldTrivial, bool topo, bool unique = false,
+                    const int *procInv = nullptr, const int *procPos = nullptr);
     // strash_core over b's own graph-major arrays (the body of st).
     int strash_batch(Batch &b, bool idOrder, bool removeDangling, bool foldTrivial);
 

@@ -31,6 +31,50 @@ __global__ void k_rw_to_aigman(int64_t N, int64_t M, const int *wlev, const int 
     }
 }
 
+// The deduplication's processing order over W positions [0, M): each
+// level's original nodes in W order, then the new nodes whose owner
+// candidate is on that level, in position order (new positions are numbered
+// by owner, and owners in W order, so their owner levels never decrease).
+// Original fanins are on lower levels; a new node's fanins are its owner's
+// cut leaves, new nodes numbered before it, or existing nodes the
+// replacement reused, which may lie on the owner's level or above; buffers
+// left by the choice point at their replacement.  The order is thus
+// topological up to those last two kinds of fanins, which the level pass
+// resolves in later rounds.
+//   lvEnd[l]    = W positions on levels <= l
+//   newStart[l] = new nodes whose owner is on a level < l
+__global__ void k_level_ends(int64_t N, const int *wlev, int maxLevel, int *lvEnd) {
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < N; p += stride) {
+        const int l = wlev[p];
+        const int next = p + 1 < N ? wlev[p + 1] : maxLevel + 1;
+        for (int k = l; k < next; k++) lvEnd[k] = (int)(p + 1);
+    }
+}
+
+__global__ void k_new_starts(int64_t nNew, const int *ownLev, int maxLevel, int *newStart) {
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j <= nNew; j += stride) {
+        const int prev = j > 0 ? ownLev[j - 1] : -1;
+        const int cur = j < nNew ? ownLev[j] : maxLevel + 1;
+        for (int k = prev + 1; k <= cur; k++) newStart[k] = (int)j;
+    }
+}
+
+__global__ void k_proc_order(int64_t N, int64_t M, const int *wlev, const int *ownLev, const int *lvEnd,
+                             const int *newStart, int *inv, int *posOf, int *status) {
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t x = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; x < M; x += stride) {
+        const int64_t pos = x < N ? x + newStart[wlev[x]] : lvEnd[ownLev[x - N]] + (x - N);
+        if (pos < 0 || pos >= M) {
+            set_status(status, kDevBadGraph);
+            continue;
+        }
+        inv[pos] = (int)x;
+        posOf[x] = (int)pos;
+    }
+}
+
 void canon_cut(int4 l, int2 m, int *q) {
     Cut c;
     cut_unpack((uint32_t)m.y, c);
@@ -142,16 +186,25 @@ int Engine::rw(Batch &b, bool useZeros, bool gpuDedup, RwStats *stats, RwDump *d
     k_rw_to_aigman<<<X.grid(std::max<int64_t>(M, b.nPO)), kBlock, 0, s_>>>(N, M, w.wlev, w.gidAll, w.dg, w.L0, w.L1, o0,
                                                                            o1, b.nPO, w.wpo, opo);
     launches_ += 1;
+    int *procInv = ar_.get<int>(M + 1), *procPos = ar_.get<int>(M + 1);
+    int *lvEnd = ar_.get<int>(w.maxLevel + 2), *newStart = ar_.get<int>(w.maxLevel + 3);
+    if (!procInv || !procPos || !lvEnd || !newStart) return fail(CULS_E_OOM, "rw: arena exhausted (dedup)");
+    if ((rc = check(fill_i32(procInv, -1, M, s_), "fill"))) return rc;
+    k_level_ends<<<X.grid(N), kBlock, 0, s_>>>(N, w.wlev, w.maxLevel, lvEnd);
+    k_new_starts<<<X.grid(w.nNew + 1), kBlock, 0, s_>>>(w.nNew, w.newOwnLev, w.maxLevel, newStart);
+    k_proc_order<<<X.grid(M), kBlock, 0, s_>>>(N, M, w.wlev, w.newOwnLev, lvEnd, newStart, procInv, procPos, status_);
+    launches_ += 3;
+    if ((rc = X.sync()) || (rc = X.status_check("rw dedup order"))) return rc;
     if (gpuDedup) {
         // updateFromRewriteManager(2): GPU strash, which also ends the
         // rewrite manager's state (src/aig_manager.cu:523-546)
-        rc = strash_core(b, M, o0, o1, w.gidAll, w.wl, opo, false, true, true, false);
+        rc = strash_core(b, M, o0, o1, w.gidAll, w.wl, opo, false, true, true, false, false, procInv, procPos);
         b.keep = false;
     } else {
         // updateFromRewriteManager(1): the manager's graph (every node, in
         // its final Reorder numbering) is kept for a following rewrite, then
         // deduplicated in id order (src/aig_manager.cu:454-522)
-        rc = strash_core(b, M, o0, o1, w.gidAll, w.wl, opo, false, false, false, false, true);
+        rc = strash_core(b, M, o0, o1, w.gidAll, w.wl, opo, false, false, false, false, true, procInv, procPos);
         if (!rc) rc = check(b.keep_current(s_), "keep");
         if (!rc) {
             rc = strash_batch(b, false, false, false);

@@ -298,7 +298,7 @@ __global__ void k_rep_rebuild(int64_t nCand, int64_t N, const int *rootRef, cons
 
 __global__ void k_rep_newnodes(int64_t K, int64_t N, const int *canon, const int *f0, const int *f1, const uint8_t *c0,
                                const uint8_t *c1, const int *newPos, const int *owner, const int *cand, const int *wg,
-                               int *L0, int *L1, int *gidAll) {
+                               const int *wlev, int *L0, int *L1, int *gidAll, int *ownLev) {
     int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t T = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; T < K; T += stride) {
         if (canon[T] != T) continue;
@@ -308,6 +308,7 @@ __global__ void k_rep_newnodes(int64_t K, int64_t N, const int *canon, const int
         L0[q] = (a < N ? 2 * a : 2 * newPos[a - N]) + c0[T];
         L1[q] = (b < N ? 2 * b : 2 * newPos[b - N]) + c1[T];
         gidAll[q] = wg[cand[owner[T]]];
+        ownLev[q - N] = wlev[cand[owner[T]]];
     }
 }
 
@@ -428,9 +429,11 @@ int rw_replace(ExecCtx &X, Batch &b, RwWork &w) {
                                                      X.status);
     X.launched(1);
     if ((rc = rep_extend_only(X, w, nNew))) return rc;
+    w.newOwnLev = ar.get<int>(nNew + 1);
+    if (!w.newOwnLev) return X.fail(CULS_E_OOM, "rw: arena exhausted (replace)");
     if (K > 0)
-        k_rep_newnodes<<<X.grid(K), kBlock, 0, s>>>(K, N, canon, f0, f1, c0, c1, newPos, owner, w.cand, w.wg, w.L0,
-                                                    w.L1, w.gidAll);
+        k_rep_newnodes<<<X.grid(K), kBlock, 0, s>>>(K, N, canon, f0, f1, c0, c1, newPos, owner, w.cand, w.wg, w.wlev,
+                                                    w.L0, w.L1, w.gidAll, w.newOwnLev);
     k_rep_final<<<X.grid(nCand), kBlock, 0, s>>>(nCand, N, repT, newPos, w.repW);
     X.launched(2);
     if ((rc = X.sync())) return rc;

@@ -87,6 +87,7 @@ struct RwWork {
     int *L0 = nullptr, *L1 = nullptr;  // fanin literals of [0, N + nNew)
     int *gidAll = nullptr;             // graph of [0, N + nNew)
     uint8_t *del = nullptr;            // isDeleted over [0, N + nNew)
+    int *newOwnLev = nullptr;          // per new node: W level of its owner candidate (non-decreasing)
     int *choice = nullptr;             // per candidate outcome code
 };
 

@@ -238,6 +238,88 @@ __global__ void __launch_bounds__(kBlock) k_st_levelize(ChunkSched S, const int 
     if ((threadIdx.x & 31) == 0 && myMax > 0) atomicMax(maxLevel, myMax);
 }
 
+// Levels over an order that is topological up to a few fanins placed later
+// (the rewrite's deduplication: see k_proc_order).  A pass runs the nodes of
+// `list` in order; a node waits only for AND fanins earlier in the order.  A
+// fanin later in the order that is not done yet, or one left unresolved,
+// leaves the node unresolved (done = 2), and the unresolved nodes form the
+// next pass's list.  Every wait is on a node whose chunk was claimed
+// earlier, so no pass can deadlock, and each pass resolves at least the
+// unresolved nodes whose fanins are all resolved.
+__global__ void __launch_bounds__(kBlock) k_order_levelize(int64_t n, const int *list, const int *posOf, const int *L0,
+                                                            const int *L1, const uint8_t *liveFlag, const int *gid,
+                                                            int *level, int *done, int *graphLevels, int *counter,
+                                                            int *maxLevel, int *status) {
+    __shared__ int64_t s_begin;
+    int myMax = 0;
+    const int64_t nChunks = (n + kBlock - 1) / kBlock;
+    while (true) {
+        if (threadIdx.x == 0) {
+            const int64_t c = atomicAdd(counter, 1);
+            s_begin = c < nChunks ? c * kBlock : -1;
+        }
+        __syncthreads();
+        const int64_t begin = s_begin;
+        __syncthreads();
+        if (begin < 0) break;
+        const int64_t i = begin + threadIdx.x;
+        if (i >= n) continue;
+        const int v = list[i];
+        if (v < 0 || !liveFlag[v]) continue;
+        const int pv = posOf[v];
+        int lv = 0;
+        bool ok = true;
+        for (int k = 0; k < 2 && ok; k++) {
+            const int u = (k == 0 ? L0[v] : L1[v]) >> 1;
+            if (L0[u] < 0) continue;  // constant or PI: level 0
+            int d = ld_acquire(&done[u]);
+            if (d == 0 && posOf[u] < pv) {
+                if (!wait_ge(&done[u], 1, status)) {
+                    ok = false;
+                    break;
+                }
+                d = ld_acquire(&done[u]);
+            }
+            if (d != 1) {
+                ok = false;
+                break;
+            }
+            const int l = __ldcg(&level[u]);
+            lv = l > lv ? l : lv;
+        }
+        if (!ok) {
+            st_release(&done[v], 2);
+            continue;
+        }
+        lv += 1;
+        __stcg(&level[v], lv);
+        agg_max(graphLevels, gid[v], lv);
+        myMax = lv > myMax ? lv : myMax;
+        __threadfence();
+        st_release(&done[v], 1);
+    }
+    myMax = __reduce_max_sync(0xffffffffu, myMax);
+    if ((threadIdx.x & 31) == 0 && myMax > 0) atomicMax(maxLevel, myMax);
+}
+
+__global__ void k_unresolved_flags(int64_t n, const int *list, const int *done, uint8_t *flag) {
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const int v = list[i];
+        flag[i] = v >= 0 && done[v] == 2;
+    }
+}
+
+// next list = list[idx[k]], reset to pending
+__global__ void k_unresolved_next(int64_t n, const int *idx, const int *list, int *next, int *done) {
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride) {
+        const int v = list[idx[k]];
+        next[k] = v;
+        done[v] = 0;
+    }
+}
+
 __global__ void k_gather_levels(int64_t n, const int *idx, const int *level, uint32_t *keys, int *lvlCnt) {
     int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
@@ -473,7 +555,7 @@ __global__ void k_strash_out(int64_t nW, const int *wl, OutArgs A) {
 
 int Engine::strash_core(Batch &b, int64_t M, const int *L0, const int *L1, const int *gidA, const int *lidIn,
                         const int *po, bool idOrder, bool removeDangling, bool foldTrivial, bool topo,
-                        bool unique) {
+                        bool unique, const int *procInv, const int *procPos) {
     const int G = b.G;
     const int64_t nPO = b.nPO;
     cudaStream_t s = s_;
@@ -527,6 +609,53 @@ int Engine::strash_core(Batch &b, int64_t M, const int *L0, const int *L1, const
         if (prof_) this->mark(kMkLevelK1);
         launches_ += 2;
     } else {
+    // in-order passes over procInv; the worklist below is the fallback if a
+    // pass stops making progress (a cycle) or a wait times out
+    bool leveled = false;
+    if (procInv) {
+        liveIdx = ar_.get<int>(M + 1);
+        if (!liveIdx) return fail(CULS_E_OOM, "strash: scratch arena exhausted");
+        int *done = pending;
+        int *lists[2] = {cnt, off};  // free until the levels are known
+        int *idx = items;
+        check(cudaMemsetAsync(qc, 0, sizeof(int) * 8, s), "memset");
+        check(cudaMemsetAsync(graphLevels, 0, sizeof(int) * (G + 1), s), "memset");
+        check(cudaMemsetAsync(level, 0, sizeof(int) * (M + 1), s), "memset");
+        k_live_flags<<<gridM, kBlock, 0, s>>>(M, L0, dead, liveFlag, done);
+        check(compact_flags(liveFlag, M, liveIdx, qc + 3, ar_, s), "compact");  // live list and count
+        launches_ += 1;
+        if (prof_) this->mark(kMkLevelK0);
+        const int *list = procInv;
+        int64_t n = M;
+        for (int pass = 0; pass < 64; pass++) {
+            check(cudaMemsetAsync(qc + 5, 0, sizeof(int), s), "memset");
+            k_order_levelize<<<gridQ, kBlock, 0, s>>>(n, list, procPos, L0, L1, liveFlag, gidA, level, done,
+                                                      graphLevels, qc + 5, qc + 4, qc + 7);
+            k_unresolved_flags<<<grid_1d(n, kBlock, sms_ * 16), kBlock, 0, s>>>(n, list, done, flags);
+            launches_ += 2;
+            check(compact_flags(flags, n, idx, qc + 6, ar_, s), "compact");
+            check(cudaMemcpyAsync(hostSmall_, qc, sizeof(int) * 8, cudaMemcpyDeviceToHost, s), "d2h");
+            if (sync()) return -1;
+            const int64_t nu = hostSmall_[6];
+            if (hostSmall_[7] != 0) break;  // a wait timed out
+            if (nu == 0) {
+                leveled = true;
+                break;
+            }
+            if (pass > 0 && nu == n) break;  // no progress
+            int *next = lists[pass & 1];
+            k_unresolved_next<<<grid_1d(nu, kBlock, sms_ * 16), kBlock, 0, s>>>(nu, idx, list, next, done);
+            launches_ += 1;
+            list = next;
+            n = nu;
+        }
+        if (leveled) {
+            // every live node has its level
+            check(cudaMemcpyAsync(qc + 1, qc + 3, sizeof(int), cudaMemcpyDeviceToDevice, s), "copy");
+            if (prof_) this->mark(kMkLevelK1);
+        }
+    }
+    if (!leveled) {
     check(cudaMemsetAsync(off, 0, sizeof(int) * (M + 2), s), "memset");
     k_live_degrees<<<gridM, kBlock, 0, s>>>(M, L0, L1, dead, level, off, liveFlag, flags);
     check(scan_exclusive(off, off, M + 1, nullptr, ar_, s), "scan");
@@ -563,6 +692,7 @@ int Engine::strash_core(Batch &b, int64_t M, const int *L0, const int *L1, const
     }
     check(cudaMemcpyAsync(qc + 1, ring + 3 + L % 3, sizeof(int), cudaMemcpyDeviceToDevice, s), "copy");
     if (prof_) this->mark(kMkLevelK1);
+    }
     }
     // 3. processing order (level, position) and tentative ranks
     check(cudaMemcpyAsync(hostSmall_, qc, sizeof(int) * 8, cudaMemcpyDeviceToHost, s), "d2h");
