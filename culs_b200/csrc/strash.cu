@@ -22,6 +22,7 @@
 // single in-order dataflow pass whose dependency waits are per-level
 // completion counters (bounded spins).
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -610,9 +611,10 @@ int Engine::strash_core(Batch &b, int64_t M, const int *L0, const int *L1, const
         launches_ += 2;
     } else {
     // in-order passes over procInv; the worklist below is the fallback if a
-    // pass stops making progress (a cycle) or a wait times out
+    // pass stops making progress (a cycle) or a wait times out, and runs
+    // alone when CULS_DEDUP_WORKLIST is set (the tests compare the two)
     bool leveled = false;
-    if (procInv) {
+    if (procInv && !getenv("CULS_DEDUP_WORKLIST")) {
         liveIdx = ar_.get<int>(M + 1);
         if (!liveIdx) return fail(CULS_E_OOM, "strash: scratch arena exhausted");
         int *done = pending;
