@@ -40,7 +40,7 @@ __global__ void k_rw_to_aigman(int64_t N, int64_t M, const int *wlev, const int 
 // replacement reused, which may lie on the owner's level or above; buffers
 // left by the choice point at their replacement.  The order is thus
 // topological up to those last two kinds of fanins, which the level pass
-// resolves in later rounds.
+// resolves in later passes.
 //   lvEnd[l]    = W positions on levels <= l
 //   newStart[l] = new nodes whose owner is on a level < l
 __global__ void k_level_ends(int64_t N, const int *wlev, int maxLevel, int *lvEnd) {
