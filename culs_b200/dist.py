@@ -18,7 +18,10 @@ def shard(count, rank, world):
 
 
 class Group:
-    """Barrier and max/sum reductions; a no-op for a single process."""
+    """Barrier and max/sum reductions; a no-op for a single process.  Ranks
+    that wait for one another longer than CULS_PG_TIMEOUT_S seconds (default
+    600: the autotuner and warm-up steps run between collectives) end with an
+    error, as does a rank whose peers never join."""
 
     def __init__(self, backend=None):
         self.rank, self.world, self.local = rank_world()
@@ -32,7 +35,8 @@ class Group:
                 backend = "nccl" if torch.cuda.is_available() else "gloo"
             if backend == "nccl":
                 torch.cuda.set_device(self.local)
-            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+            timeout = float(os.environ.get("CULS_PG_TIMEOUT_S", "600"))
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=timeout))
             self.dist = dist
             self.torch = torch
             self.backend = backend
