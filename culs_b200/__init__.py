@@ -29,8 +29,9 @@ CULS_E_DEVICE = -5
 CULS_E_IO = -6
 CULS_E_BUSY = -7
 CULS_E_NOTFOUND = -8
+CULS_E_CANCELLED = -9
 ERRORS = {-1: "CULS_E_INVALID", -2: "CULS_E_OOM", -3: "CULS_E_BUDGET", -4: "CULS_E_PROBE", -5: "CULS_E_DEVICE",
-          -6: "CULS_E_IO", -7: "CULS_E_BUSY", -8: "CULS_E_NOTFOUND"}
+          -6: "CULS_E_IO", -7: "CULS_E_BUSY", -8: "CULS_E_NOTFOUND", -9: "CULS_E_CANCELLED"}
 RW_ZEROS, RW_GPU_DEDUP, RW_DUMP = 1, 2, 4
 SERVE_BYTES_PER_OBJ = 720  # device bytes the served mode's admission charges per object
 ST_CPU = 1
@@ -84,6 +85,7 @@ _lib.culs_submit.argtypes = [_vp, _ip, _ip, _ip, ctypes.c_int32, ctypes.c_int32,
                              ctypes.c_uint32, ctypes.POINTER(ctypes.c_int64)]
 _lib.culs_poll.argtypes = [_vp, ctypes.c_int64, _ip, _ip, _ip, _ip]
 _lib.culs_wait.argtypes = [_vp, ctypes.c_int64, ctypes.c_int]
+_lib.culs_cancel.argtypes = [_vp, ctypes.c_int64]
 _lib.culs_fetch.argtypes = [_vp, ctypes.c_int64, _ip, _ip, _ip, ctypes.POINTER(ctypes.c_double)]
 _lib.culs_submit_aiger.argtypes = [_vp, _vp, ctypes.c_size_t, ctypes.c_uint32, ctypes.c_uint32,
                                    ctypes.POINTER(ctypes.c_int64)]
@@ -317,11 +319,22 @@ class Context:
         self._err(rc, "wait")
         return True
 
+    def cancel(self, job):
+        """Takes a queued job out of the queue (it ends with CULS_E_CANCELLED);
+        raises CulsError(CULS_E_BUSY) once its batch runs."""
+        self._err(_lib.culs_cancel(self.h, job), "cancel")
+
     def fetch(self, job):
-        """The finished job's result and its submit-to-done latency in ms."""
-        st = self.poll(job)
-        if st is None:
+        """The finished job's result and its submit-to-done latency in ms.  A
+        job that failed or was cancelled raises its code and is forgotten."""
+        v = [ctypes.c_int32() for _ in range(4)]
+        rc = _lib.culs_poll(self.h, job, *[ctypes.byref(x) for x in v])
+        if rc == CULS_E_BUSY:
             raise CulsError(CULS_E_BUSY, "fetch: job still running")
+        if rc not in (0, CULS_E_NOTFOUND):
+            _lib.culs_fetch(self.h, job, None, None, None, None)  # forgets the failed job
+        self._err(rc, "fetch")
+        st = dict(zip(["nPIs", "nPOs", "nAnds", "nLevels"], [x.value for x in v]))
         n = 1 + st["nPIs"] + st["nAnds"]
         f0, f1 = np.empty(n, np.int32), np.empty(n, np.int32)
         outs = np.empty(max(st["nPOs"], 1), np.int32)

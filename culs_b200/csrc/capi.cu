@@ -316,6 +316,13 @@ int culs_poll(culs_ctx *ctx, int64_t job, int32_t *nPIs, int32_t *nPOs, int32_t 
     return s->poll(job, nPIs, nPOs, nAnds, nLevels);
 }
 
+int culs_cancel(culs_ctx *ctx, int64_t job) {
+    if (!ctx) return CULS_E_INVALID;
+    auto s = server_of(ctx);
+    if (!s) return CULS_E_NOTFOUND;
+    return s->cancel(job);
+}
+
 int culs_wait(culs_ctx *ctx, int64_t job, int timeoutMs) {
     if (!ctx) return CULS_E_INVALID;
     auto s = server_of(ctx);

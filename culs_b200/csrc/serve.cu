@@ -186,6 +186,22 @@ int Server::fetch(int64_t id, int32_t *f0, int32_t *f1, int32_t *outs, double *l
     return CULS_OK;
 }
 
+int Server::cancel(int64_t id) {
+    {
+        std::lock_guard<std::mutex> lk(mu_);
+        auto it = jobs_.find(id);
+        if (it == jobs_.end()) return CULS_E_NOTFOUND;
+        ServeJob &j = *it->second;
+        if (j.state == kRunning) return CULS_E_BUSY;
+        if (j.state != kQueued) return CULS_E_INVALID;
+        queue_.erase(std::find(queue_.begin(), queue_.end(), id));
+        j.state = CULS_E_CANCELLED;
+        j.tDone = std::chrono::steady_clock::now();
+    }
+    cvDone_.notify_all();
+    return CULS_OK;
+}
+
 void Server::worker(Engine &eng, std::mutex &engMu) {
     cudaSetDevice(eng.device());  // the current device is per thread
     while (true) {

@@ -65,6 +65,8 @@ class Server {
     int wait(int64_t id, int timeoutMs);
     // Copies a finished job's result out and forgets the job.
     int fetch(int64_t id, int32_t *f0, int32_t *f1, int32_t *outs, double *latencyMs);
+    // Takes a queued job out of the queue; it finishes with CULS_E_CANCELLED.
+    int cancel(int64_t id);
     const std::string &lastError() const { return err_; }
 
   private:

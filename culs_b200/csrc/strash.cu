@@ -637,7 +637,7 @@ int Engine::strash_core(Batch &b, int64_t M, const int *L0, const int *L1, const
             launches_ += 2;
             check(compact_flags(flags, n, idx, qc + 6, ar_, s), "compact");
             check(cudaMemcpyAsync(hostSmall_, qc, sizeof(int) * 8, cudaMemcpyDeviceToHost, s), "d2h");
-            if (sync()) return -1;
+            if (int e = sync()) return e;
             const int64_t nu = hostSmall_[6];
             if (hostSmall_[7] != 0) break;  // a wait timed out
             if (nu == 0) {
@@ -665,7 +665,7 @@ int Engine::strash_core(Batch &b, int64_t M, const int *L0, const int *L1, const
     check(cudaMemcpyAsync(cursor, off, sizeof(int) * (M + 1), cudaMemcpyDeviceToDevice, s), "copy");
     // number of live edges = off[M]
     check(cudaMemcpyAsync(hostSmall_, off + M, sizeof(int), cudaMemcpyDeviceToHost, s), "d2h");
-    if (sync()) return -1;
+    if (int e = sync()) return e;
     int64_t nEdges = hostSmall_[0];
     int *adj = ar_.get<int>(nEdges + 1);
     if (!adj) return fail(CULS_E_OOM, "strash: scratch arena exhausted");
@@ -689,7 +689,7 @@ int Engine::strash_core(Batch &b, int64_t M, const int *L0, const int *L1, const
             k_level_step<<<gridQ, kBlock, 0, s>>>(L, items, ring, off, adj, L0, L1, level, gidA, graphLevels, qc + 4);
         launches_ += 64;
         check(cudaMemcpyAsync(hostSmall_, ring, sizeof(int) * 6, cudaMemcpyDeviceToHost, s), "d2h");
-        if (sync()) return -1;
+        if (int e = sync()) return e;
         if (hostSmall_[L % 3] == 0) break;
     }
     check(cudaMemcpyAsync(qc + 1, ring + 3 + L % 3, sizeof(int), cudaMemcpyDeviceToDevice, s), "copy");
@@ -698,8 +698,8 @@ int Engine::strash_core(Batch &b, int64_t M, const int *L0, const int *L1, const
     }
     // 3. processing order (level, position) and tentative ranks
     check(cudaMemcpyAsync(hostSmall_, qc, sizeof(int) * 8, cudaMemcpyDeviceToHost, s), "d2h");
-    if (sync()) return -1;
-    if (check_status("strash levels")) return -1;
+    if (int e = sync()) return e;
+    if (int e = check_status("strash levels")) return e;
     int64_t nLive = hostSmall_[3];
     int maxLevel = hostSmall_[4];
     if (!topo && hostSmall_[1] != nLive) return fail(CULS_E_INVALID, "strash: the AIG has a cycle");
@@ -737,6 +737,17 @@ int Engine::strash_core(Batch &b, int64_t M, const int *L0, const int *L1, const
     // 4. hash in dataflow order
     uint32_t cap = 1024;
     while (cap < (uint32_t)std::min<int64_t>(nLive * 2, 1ll << 31)) cap <<= 1;
+    // CULS_STRASH_TABLE_CAP lowers the capacity (rounded up to a power of
+    // two): the tests use it to make the bounded probes run out and check
+    // that the call reports CULS_E_PROBE and leaves the graph as it was
+    if (const char *env = getenv("CULS_STRASH_TABLE_CAP")) {
+        const long long want = atoll(env);
+        if (want >= 1) {
+            uint32_t c = 1;
+            while ((long long)c < want && c < (1u << 31)) c <<= 1;
+            cap = std::min(cap, c);
+        }
+    }
     unsigned long long *tk = ar_.get<unsigned long long>(cap);
     int *tv = ar_.get<int>(cap);
     int *mapEnc = ar_.get<int>(M + 1);
@@ -764,8 +775,8 @@ int Engine::strash_core(Batch &b, int64_t M, const int *L0, const int *L1, const
     // In id order (CPU variants) the winners are ranked by position, not by
     // processing order: sort the winner list by rank.
     check(cudaMemcpyAsync(hostSmall_, qc, sizeof(int) * 8, cudaMemcpyDeviceToHost, s), "d2h");
-    if (sync()) return -1;
-    if (check_status("strash hashing")) return -1;
+    if (int e = sync()) return e;
+    if (int e = check_status("strash hashing")) return e;
     int64_t nW = hostSmall_[6];
     int *newLocalT = ar_.get<int>(nLive + 1);
     int *cntG = ar_.get<int>(G + 1);
@@ -802,7 +813,7 @@ int Engine::strash_core(Batch &b, int64_t M, const int *L0, const int *L1, const
     std::vector<int> hCnt(G), hLev(G);
     check(cudaMemcpyAsync(hCnt.data(), cntG, sizeof(int) * G, cudaMemcpyDeviceToHost, s), "d2h");
     check(cudaMemcpyAsync(hLev.data(), graphLevels, sizeof(int) * G, cudaMemcpyDeviceToHost, s), "d2h");
-    if (sync()) return -1;
+    if (int e = sync()) return e;
     // new graph table
     std::vector<DevGraph> ng = b.hg;
     int64_t base = 0;
@@ -819,7 +830,7 @@ int Engine::strash_core(Batch &b, int64_t M, const int *L0, const int *L1, const
     if (!dgNew) return fail(CULS_E_OOM, "strash: arena");
     // the output goes to the batch's spare buffers, swapped in at the end
     if (!b.pool) b.pool = pool_;
-    if (check(b.reserve_spare(nObjNew + 1, nPO + 1), "cudaMalloc")) return -1;
+    if (int e = check(b.reserve_spare(nObjNew + 1, nPO + 1), "cudaMalloc")) return e;
     int *F0n = b.F0s, *F1n = b.F1s, *POn = b.POs;
     check(cudaMemcpyAsync(dgNew, ng.data(), sizeof(DevGraph) * G, cudaMemcpyHostToDevice, s), "h2d");
     check(fill_i32(F0n, -1, nObjNew, s), "fill");
@@ -834,7 +845,7 @@ int Engine::strash_core(Batch &b, int64_t M, const int *L0, const int *L1, const
                                                                                                              O);
     launches_ += 1;
     check(cudaMemcpyAsync(b.dg, ng.data(), sizeof(DevGraph) * G, cudaMemcpyHostToDevice, s), "h2d");
-    if (sync()) return -1;
+    if (int e = sync()) return e;
     b.swap_spare();
     b.hg = ng;
     b.nObj = nObjNew;

@@ -35,6 +35,7 @@ extern "C" {
 #define CULS_E_IO (-6)       /* file missing, unreadable or not binary AIGER */
 #define CULS_E_BUSY (-7)     /* served job not finished yet */
 #define CULS_E_NOTFOUND (-8) /* unknown job id */
+#define CULS_E_CANCELLED (-9) /* served job cancelled before it ran */
 
 /* ------------------------------------------------------- host-side graphs */
 /* A graph held in host memory, arrays allocated with malloc by the library
@@ -186,6 +187,12 @@ int culs_submit(culs_ctx *ctx, const int32_t *fanin0, const int32_t *fanin1, con
 int culs_poll(culs_ctx *ctx, int64_t job, int32_t *nPIs, int32_t *nPOs, int32_t *nAnds, int32_t *nLevels);
 int culs_wait(culs_ctx *ctx, int64_t job, int timeoutMs);
 int culs_fetch(culs_ctx *ctx, int64_t job, int32_t *fanin0, int32_t *fanin1, int32_t *outs, double *latencyMs);
+/* culs_cancel takes a job that is still queued out of the queue: it finishes
+ * with CULS_E_CANCELLED (culs_poll, culs_wait and culs_fetch return that
+ * code; culs_fetch then forgets it).  A job already in a running batch
+ * completes (CULS_E_BUSY), a finished one is left as it is (CULS_E_INVALID),
+ * and an unknown id gives CULS_E_NOTFOUND. */
+int culs_cancel(culs_ctx *ctx, int64_t job);
 /* A served job given as a binary AIGER file's bytes (copied): its header is
  * checked at once (CULS_E_IO when the host reader would refuse it), its AND
  * section decoded on the device with the rest of its batch, which holds AIGER

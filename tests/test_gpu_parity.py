@@ -244,6 +244,24 @@ def test_budget_refusal(ctx):
     small.close()
 
 
+def test_strash_probe_cap_reports_and_leaves_graph(ctx, monkeypatch):
+    """A strash table too small for the graph: the bounded probes run out, the
+    call reports CULS_E_PROBE, the graph stays as it was and the context keeps
+    working (the status word is cleared)."""
+    g = C.gen_multiplier(32)
+    d = ctx.upload(g)
+    monkeypatch.setenv("CULS_STRASH_TABLE_CAP", "1024")
+    with pytest.raises(C.CulsError) as e:
+        ctx.st(d)
+    assert e.value.code == C.CULS_E_PROBE
+    monkeypatch.delenv("CULS_STRASH_TABLE_CAP")
+    assert same_graph(d.download(), g)
+    ctx.rw(d)
+    ctx.st(d)
+    assert same_graph(d.download(), oracle_rw_st(g).graph())
+    d.free()
+
+
 def test_invalid_graph_rejected(ctx):
     bad = C.Aig(2, np.array([-1, -1, -1, 8], np.int32), np.array([-1, -1, -1, 2], np.int32), np.array([6], np.int32))
     with pytest.raises(C.CulsError) as e:

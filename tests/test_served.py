@@ -140,3 +140,37 @@ def test_served_job_error_is_reported():
     finally:
         small.serve_stop()
         small.close()
+
+
+def test_cancel_queued_job(ctx):
+    # one worker taking one job per batch: the second job waits in the queue
+    # while the first (a 300k-AND graph) runs
+    big, small = C.gen_layered(31, 256, 64, 300000, 200, 4, 0.0, True), C.gen_multiplier(8)
+    ctx.serve_start(max_batch=1, workers=1)
+    try:
+        j1 = ctx.submit(big)
+        j2 = ctx.submit(small)
+        ctx.cancel(j2)
+        with pytest.raises(C.CulsError) as e:  # finished at once, with its code
+            ctx.wait(j2, 0)
+        assert e.value.code == C.CULS_E_CANCELLED
+        with pytest.raises(C.CulsError) as e:
+            ctx.poll(j2)
+        assert e.value.code == C.CULS_E_CANCELLED
+        with pytest.raises(C.CulsError) as e:  # fetching reports the code and forgets the job
+            ctx.fetch(j2)
+        assert e.value.code == C.CULS_E_CANCELLED
+        with pytest.raises(C.CulsError) as e:
+            ctx.poll(j2)
+        assert e.value.code == C.CULS_E_NOTFOUND
+        with pytest.raises(C.CulsError) as e:
+            ctx.cancel(10 ** 9)
+        assert e.value.code == C.CULS_E_NOTFOUND
+        assert ctx.wait(j1, 120000)
+        with pytest.raises(C.CulsError) as e:  # a finished job is not cancelled
+            ctx.cancel(j1)
+        assert e.value.code == C.CULS_E_INVALID
+        out, _ = ctx.fetch(j1)
+        assert same_graph(out, oracle_rw_st(big).graph())
+    finally:
+        ctx.serve_stop()
