@@ -85,11 +85,13 @@ void remove_dangling(Aig &g) {
 // fanin edge is complemented with probability 1/2.  POs are the first nPOs
 // nodes of the last layer (all of it when it is narrower), or, with
 // sinksArePOs, every AND node without fanouts (then no node dangles and the
-// AIG keeps exactly nAnds AND nodes).
-Aig layered(uint64_t seed, int nPIs, int nPOs, int64_t nAnds, int nLayers, int window, double pFar, bool withPIs,
-            bool sinksArePOs = false) {
+// AIG keeps exactly nAnds AND nodes).  Returns false when a layer has more
+// nodes than its window offers distinct fanin pairs (no strashed AIG has that
+// shape).
+bool layered(Aig &g, uint64_t seed, int nPIs, int nPOs, int64_t nAnds, int nLayers, int window, double pFar,
+             bool withPIs, bool sinksArePOs = false) {
     Rng r(seed);
-    Aig g;
+    g = Aig();
     g.nPIs = nPIs;
     int64_t nObjs = 1 + nPIs + nAnds;
     g.f0.assign(nObjs, -1);
@@ -125,7 +127,7 @@ Aig layered(uint64_t seed, int nPIs, int nPOs, int64_t nAnds, int nLayers, int w
                 if (a > b) std::swap(a, b);
                 uint64_t key = ((uint64_t)(uint32_t)a << 32) | (uint32_t)b;
                 if (seen.insert(key).second) break;
-                if (tries > 1000) abort();  // the pools are far larger than needed
+                if (tries > 1000) return false;  // the window's pairs are used up
             }
             g.f0[v] = a;
             g.f1[v] = b;
@@ -144,7 +146,7 @@ Aig layered(uint64_t seed, int nPIs, int nPOs, int64_t nAnds, int nLayers, int w
         for (int64_t v = lastLo; v < lastHi && (int)g.outs.size() < nPOs; v++) g.outs.push_back((int)(2 * v));
     }
     remove_dangling(g);
-    return g;
+    return true;
 }
 
 // Structural-hashing AIG builder used by the arithmetic generators.
@@ -242,7 +244,9 @@ int culs_gen_layered(uint64_t seed, int nPIs, int nPOs, int64_t nAnds, int nLaye
     if (!out || nPIs < 2 || nAnds < 0 || nLayers < 1 || window < 1 || nAnds + nPIs + 1 > INT32_MAX / 2)
         return CULS_E_INVALID;
     if (nAnds > 0 && nAnds < nLayers) return CULS_E_INVALID;
-    return export_graph(layered(seed, nPIs, nPOs, nAnds, nLayers, window, pFar, withPIs != 0), out);
+    Aig g;
+    if (!layered(g, seed, nPIs, nPOs, nAnds, nLayers, window, pFar, withPIs != 0)) return CULS_E_INVALID;
+    return export_graph(g, out);
 }
 
 int culs_gen_multiplier(int n, culs_host_graph *out) {
@@ -269,15 +273,20 @@ int culs_gen_batch(uint64_t tag, int first, int count, int64_t minAnds, int64_t 
                                                            u * (std::log((double)maxAnds) - std::log((double)minAnds))));
             int nPIs = minPIs + (int)r.below((uint64_t)(maxPIs - minPIs + 1));
             int nLayers = std::max(1, (int)std::llround(std::sqrt((double)nAnds)));
-            Aig g = layered(r.next(), nPIs, 0, nAnds, nLayers, 4, 0.0, true, true);
-            rc[k] = export_graph(g, &out[k]);
+            Aig g;
+            rc[k] = layered(g, r.next(), nPIs, 0, nAnds, nLayers, 4, 0.0, true, true) ? export_graph(g, &out[k])
+                                                                                       : CULS_E_INVALID;
         }
     };
     std::vector<std::thread> th;
     for (int t = 0; t < threads; t++) th.emplace_back(work, t);
     for (auto &x : th) x.join();
-    for (int k = 0; k < count; k++)
-        if (rc[k] != CULS_OK) return rc[k];
+    for (int k = 0; k < count; k++) {
+        if (rc[k] == CULS_OK) continue;
+        for (int j = 0; j < count; j++)  // no graph is returned on failure
+            if (rc[j] == CULS_OK) culs_host_graph_free(&out[j]);
+        return rc[k];
+    }
     return CULS_OK;
 }
 

@@ -98,6 +98,14 @@ def test_generators_deterministic_and_strashed():
     _check_strashed(m)
 
 
+def test_generator_refuses_impossible_shape():
+    """176 AND nodes in a first layer over 9 PIs (only 144 distinct
+    complemented fanin pairs exist there): an error code, not an abort."""
+    with pytest.raises(C.CulsError) as e:
+        C.gen_layered(201, 9, 11, 1408, 8, 3, 0.0, True)
+    assert e.value.code == C.CULS_E_INVALID
+
+
 def test_gen_batch_matches_sequential():
     par = C.gen_batch(4, 0, 6, 1000, 5000, 16, 512, threads=4)
     seq = C.gen_batch(4, 0, 6, 1000, 5000, 16, 512, threads=1)
