@@ -24,6 +24,8 @@
 #include <atomic>
 #include <cstdio>
 #include <cstring>
+#include <exception>
+#include <mutex>
 #include <string>
 #include <thread>
 #include <vector>
@@ -246,10 +248,28 @@ void for_runs(int G, W weight, F fn) {
         if ((int)cut.size() < parts && acc * parts >= total * (int64_t)cut.size() && g + 1 < G) cut.push_back(g + 1);
     }
     cut.push_back(G);
+    // an exception of any run is rethrown here once every started thread has
+    // been joined
+    std::exception_ptr err;
+    std::mutex mu;
+    auto call = [&](size_t r) {
+        try {
+            fn(cut[r], cut[r + 1]);
+        } catch (...) {
+            std::lock_guard<std::mutex> lk(mu);
+            if (!err) err = std::current_exception();
+        }
+    };
     std::vector<std::thread> th;
-    for (size_t r = 1; r + 1 < cut.size(); r++) th.emplace_back([&, r] { fn(cut[r], cut[r + 1]); });
-    fn(cut[0], cut[1]);
+    try {
+        for (size_t r = 1; r + 1 < cut.size(); r++) th.emplace_back(call, r);
+    } catch (...) {
+        for (auto &t : th) t.join();
+        throw;
+    }
+    call(0);
     for (auto &t : th) t.join();
+    if (err) std::rethrow_exception(err);
 }
 
 // Decimal digits of v >= 0 followed by '\n' at p; returns the end.

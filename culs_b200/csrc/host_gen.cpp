@@ -21,6 +21,7 @@
 #include <vector>
 
 #include "culs_b200.h"
+#include "guard.hpp"
 
 namespace {
 
@@ -228,7 +229,10 @@ int export_graph(const Aig &g, culs_host_graph *out) {
     out->fanin0 = (int32_t *)malloc(sizeof(int32_t) * (size_t)nObjs);
     out->fanin1 = (int32_t *)malloc(sizeof(int32_t) * (size_t)nObjs);
     out->outs = (int32_t *)malloc(sizeof(int32_t) * (size_t)std::max(1, out->nPOs));
-    if (!out->fanin0 || !out->fanin1 || !out->outs) return CULS_E_OOM;
+    if (!out->fanin0 || !out->fanin1 || !out->outs) {
+        culs_host_graph_free(out);
+        return CULS_E_OOM;
+    }
     memcpy(out->fanin0, g.f0.data(), sizeof(int32_t) * (size_t)nObjs);
     memcpy(out->fanin1, g.f1.data(), sizeof(int32_t) * (size_t)nObjs);
     if (out->nPOs) memcpy(out->outs, g.outs.data(), sizeof(int32_t) * (size_t)out->nPOs);
@@ -241,17 +245,21 @@ extern "C" {
 
 int culs_gen_layered(uint64_t seed, int nPIs, int nPOs, int64_t nAnds, int nLayers, int window, double pFar,
                      int withPIs, culs_host_graph *out) {
-    if (!out || nPIs < 2 || nAnds < 0 || nLayers < 1 || window < 1 || nAnds + nPIs + 1 > INT32_MAX / 2)
-        return CULS_E_INVALID;
-    if (nAnds > 0 && nAnds < nLayers) return CULS_E_INVALID;
-    Aig g;
-    if (!layered(g, seed, nPIs, nPOs, nAnds, nLayers, window, pFar, withPIs != 0)) return CULS_E_INVALID;
-    return export_graph(g, out);
+    return culs::guard_call(nullptr, [&]() -> int {
+        if (!out || nPIs < 2 || nAnds < 0 || nLayers < 1 || window < 1 || nAnds + nPIs + 1 > INT32_MAX / 2)
+            return CULS_E_INVALID;
+        if (nAnds > 0 && nAnds < nLayers) return CULS_E_INVALID;
+        Aig g;
+        if (!layered(g, seed, nPIs, nPOs, nAnds, nLayers, window, pFar, withPIs != 0)) return CULS_E_INVALID;
+        return export_graph(g, out);
+    });
 }
 
 int culs_gen_multiplier(int n, culs_host_graph *out) {
-    if (!out || n < 1 || n > 4096) return CULS_E_INVALID;
-    return export_graph(multiplier(n), out);
+    return culs::guard_call(nullptr, [&]() -> int {
+        if (!out || n < 1 || n > 4096) return CULS_E_INVALID;
+        return export_graph(multiplier(n), out);
+    });
 }
 
 // Batch of `count` layered graphs with sizes log-uniform in [minAnds,
@@ -261,33 +269,44 @@ int culs_gen_multiplier(int n, culs_host_graph *out) {
 // `threads` host threads; output order is graph order.
 int culs_gen_batch(uint64_t tag, int first, int count, int64_t minAnds, int64_t maxAnds, int minPIs, int maxPIs,
                    int threads, culs_host_graph *out) {
-    if (!out || count < 0 || minAnds < 1 || maxAnds < minAnds || minPIs < 2 || maxPIs < minPIs) return CULS_E_INVALID;
-    if (threads < 1) threads = 1;
-    std::vector<int> rc(count, CULS_OK);
-    auto work = [&](int t) {
-        for (int k = t; k < count; k += threads) {
-            uint64_t seed = splitmix((tag << 32) + (uint64_t)(first + k));
-            Rng r(seed);
-            double u = r.unit();
-            int64_t nAnds = (int64_t)std::llround(std::exp(std::log((double)minAnds) +
-                                                           u * (std::log((double)maxAnds) - std::log((double)minAnds))));
-            int nPIs = minPIs + (int)r.below((uint64_t)(maxPIs - minPIs + 1));
-            int nLayers = std::max(1, (int)std::llround(std::sqrt((double)nAnds)));
-            Aig g;
-            rc[k] = layered(g, r.next(), nPIs, 0, nAnds, nLayers, 4, 0.0, true, true) ? export_graph(g, &out[k])
-                                                                                       : CULS_E_INVALID;
+    return culs::guard_call(nullptr, [&]() -> int {
+        if (!out || count < 0 || minAnds < 1 || maxAnds < minAnds || minPIs < 2 || maxPIs < minPIs) return CULS_E_INVALID;
+        if (threads < 1) threads = 1;
+        std::vector<int> rc(count, CULS_E_INVALID);  // until the graph is made
+        auto work = [&](int t) {
+            for (int k = t; k < count; k += threads) {
+                rc[k] = culs::guard_call(nullptr, [&]() -> int {
+                    uint64_t seed = splitmix((tag << 32) + (uint64_t)(first + k));
+                    Rng r(seed);
+                    double u = r.unit();
+                    int64_t nAnds = (int64_t)std::llround(
+                        std::exp(std::log((double)minAnds) + u * (std::log((double)maxAnds) - std::log((double)minAnds))));
+                    int nPIs = minPIs + (int)r.below((uint64_t)(maxPIs - minPIs + 1));
+                    int nLayers = std::max(1, (int)std::llround(std::sqrt((double)nAnds)));
+                    Aig g;
+                    return layered(g, r.next(), nPIs, 0, nAnds, nLayers, 4, 0.0, true, true) ? export_graph(g, &out[k])
+                                                                                              : CULS_E_INVALID;
+                });
+            }
+        };
+        std::vector<std::thread> th;
+        try {
+            for (int t = 0; t < threads; t++) th.emplace_back(work, t);
+        } catch (...) {
+            for (auto &x : th) x.join();
+            for (int j = 0; j < count; j++)
+                if (rc[j] == CULS_OK) culs_host_graph_free(&out[j]);
+            throw;
         }
-    };
-    std::vector<std::thread> th;
-    for (int t = 0; t < threads; t++) th.emplace_back(work, t);
-    for (auto &x : th) x.join();
-    for (int k = 0; k < count; k++) {
-        if (rc[k] == CULS_OK) continue;
-        for (int j = 0; j < count; j++)  // no graph is returned on failure
-            if (rc[j] == CULS_OK) culs_host_graph_free(&out[j]);
-        return rc[k];
-    }
-    return CULS_OK;
+        for (auto &x : th) x.join();
+        for (int k = 0; k < count; k++) {
+            if (rc[k] == CULS_OK) continue;
+            for (int j = 0; j < count; j++)  // no graph is returned on failure
+                if (rc[j] == CULS_OK) culs_host_graph_free(&out[j]);
+            return rc[k];
+        }
+        return CULS_OK;
+    });
 }
 
 void culs_host_graph_free(culs_host_graph *g) {

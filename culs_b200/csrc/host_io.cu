@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cstring>
+#include <exception>
 #include <mutex>
 #include <thread>
 #include <vector>
@@ -37,12 +38,30 @@ int host_threads(int64_t work, int G) {
 }
 
 // Runs fn(run) for every run on its own thread (the first on the caller's).
+// An exception of any run is rethrown on the caller's thread once every
+// started thread has been joined.
 template <class F>
 void run_parallel(int runs, F fn) {
+    std::exception_ptr err;
+    std::mutex mu;
+    auto call = [&](int r) {
+        try {
+            fn(r);
+        } catch (...) {
+            std::lock_guard<std::mutex> lk(mu);
+            if (!err) err = std::current_exception();
+        }
+    };
     std::vector<std::thread> th;
-    for (int r = 1; r < runs; r++) th.emplace_back(fn, r);
-    fn(0);
+    try {
+        for (int r = 1; r < runs; r++) th.emplace_back(call, r);
+    } catch (...) {
+        for (auto &t : th) t.join();
+        throw;
+    }
+    call(0);
     for (auto &t : th) t.join();
+    if (err) std::rethrow_exception(err);
 }
 
 }  // namespace

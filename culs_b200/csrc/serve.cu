@@ -3,6 +3,7 @@
 #include <climits>
 #include <cstring>
 
+#include "guard.hpp"
 #include "serve.cuh"
 
 namespace culs {
@@ -236,7 +237,21 @@ void Server::worker(Engine &eng, std::mutex &engMu) {
                 rest.pop_back();
             }
         }
-        run_batch(eng, engMu, batch);
+        // a host exception (an allocation) fails the batch's jobs, not the
+        // worker thread and with it the process
+        const int rc = guard_call(nullptr, [&]() -> int {
+            run_batch(eng, engMu, batch);
+            return CULS_OK;
+        });
+        if (rc != CULS_OK) {
+            std::lock_guard<std::mutex> lk(mu_);
+            const auto now = std::chrono::steady_clock::now();
+            for (ServeJob *j : batch)
+                if (j->state == kRunning) {
+                    j->state = rc;
+                    j->tDone = now;
+                }
+        }
         cvDone_.notify_all();
     }
 }

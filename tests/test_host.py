@@ -106,6 +106,29 @@ def test_generator_refuses_impossible_shape():
     assert e.value.code == C.CULS_E_INVALID
 
 
+def test_host_allocation_failure_is_an_error_code():
+    """A C entry point whose host allocation fails returns CULS_E_OOM instead
+    of letting std::bad_alloc end the process (run in a child process whose
+    address space is capped 512 MiB above its size at start)."""
+    import subprocess
+    import sys
+    import textwrap
+    code = textwrap.dedent("""
+        import resource, culs_b200 as C
+        size = next(int(l.split()[1]) * 1024 for l in open("/proc/self/status") if l.startswith("VmSize"))
+        resource.setrlimit(resource.RLIMIT_AS, (size + (512 << 20), size + (512 << 20)))
+        try:
+            C.gen_layered(1, 64, 32, 50_000_000, 7000, 4, 0.0, True)
+            print("generated")
+        except C.CulsError as e:
+            print("error", e.code)
+    """)
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=120,
+                       cwd=os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    assert r.returncode == 0, r.stderr[-500:]
+    assert r.stdout.split() == ["error", str(C.CULS_E_OOM)]
+
+
 def test_gen_batch_matches_sequential():
     par = C.gen_batch(4, 0, 6, 1000, 5000, 16, 512, threads=4)
     seq = C.gen_batch(4, 0, 6, 1000, 5000, 16, 512, threads=1)
