@@ -73,16 +73,13 @@ int culs_graph_upload(culs_ctx *ctx, const int32_t *fanin0, const int32_t *fanin
     return culs::guard_call(ctx ? &ctx->err : &g_err, [&]() -> int {
         if (!ctx || !g || (!fanin0 && nAnds) || (!fanin1 && nAnds) || (!outs && nPOs)) return CULS_E_INVALID;
         std::lock_guard<std::mutex> lk(ctx->mu);
-        culs_graph *h = new culs_graph();
+        auto h = std::make_unique<culs_graph>();
         h->owner = ctx;
         int32_t zero = 0;
         const int32_t *p0 = fanin0 ? fanin0 : &zero, *p1 = fanin1 ? fanin1 : &zero, *po = outs ? outs : &zero;
         int rc = ctx->eng.upload(h->b, 1, &p0, &p1, &po, &nPIs, &nPOs, &nAnds);
-        if (rc != CULS_OK) {
-            delete h;
-            return set_err(ctx, rc);
-        }
-        *g = h;
+        if (rc != CULS_OK) return set_err(ctx, rc);
+        *g = h.release();
         return CULS_OK;
     });
 }
@@ -102,14 +99,11 @@ int culs_batch_upload(culs_ctx *ctx, int count, const culs_host_graph *graphs, c
             nPO[i] = graphs[i].nPOs;
             nA[i] = graphs[i].nAnds;
         }
-        culs_graph *h = new culs_graph();
+        auto h = std::make_unique<culs_graph>();
         h->owner = ctx;
         int rc = ctx->eng.upload(h->b, count, p0.data(), p1.data(), po.data(), nPI.data(), nPO.data(), nA.data());
-        if (rc != CULS_OK) {
-            delete h;
-            return set_err(ctx, rc);
-        }
-        *g = h;
+        if (rc != CULS_OK) return set_err(ctx, rc);
+        *g = h.release();
         return CULS_OK;
     });
 }
@@ -494,14 +488,12 @@ int culs_graph_clone(culs_ctx *ctx, const culs_graph *src, culs_graph **dst) {
     return culs::guard_call(ctx ? &ctx->err : &g_err, [&]() -> int {
         if (!ctx || !src || !dst) return CULS_E_INVALID;
         std::lock_guard<std::mutex> lk(ctx->mu);
-        culs_graph *h = *dst ? *dst : new culs_graph();
+        std::unique_ptr<culs_graph> fresh(*dst ? nullptr : new culs_graph());
+        culs_graph *h = *dst ? *dst : fresh.get();
         h->owner = ctx;
         int rc = ctx->eng.clone(src->b, h->b);
-        if (rc != CULS_OK) {
-            if (!*dst) delete h;
-            return set_err(ctx, rc);
-        }
-        *dst = h;
+        if (rc != CULS_OK) return set_err(ctx, rc);
+        if (fresh) *dst = fresh.release();
         return CULS_OK;
     });
 }
