@@ -345,6 +345,7 @@ void Server::run_batch(Engine &eng, std::mutex &engMu, std::vector<ServeJob *> &
     }
     const uint32_t rwf = batch[0]->rwFlags, stf = batch[0]->stFlags;
     int rc;
+    bool written = false;  // the jobs' arrays hold (part of) the results
     std::string why;
     {
         std::lock_guard<std::mutex> lk(engMu);
@@ -357,6 +358,7 @@ void Server::run_batch(Engine &eng, std::mutex &engMu, std::vector<ServeJob *> &
         if (rc == CULS_OK) rc = eng.st(b, (stf & CULS_ST_CPU) != 0);
         if (rc == CULS_OK) {
             std::vector<int32_t *> o0(n), o1(n), oo(n);
+            written = true;
             for (int i = 0; i < n; i++) {
                 const DevGraph &d = b.hg[i];
                 const size_t m = 1 + (size_t)d.nPIs + d.nAnds;
@@ -372,6 +374,15 @@ void Server::run_batch(Engine &eng, std::mutex &engMu, std::vector<ServeJob *> &
             rc = eng.download_all(b, o0.data(), o1.data(), oo.data());
         }
         if (rc != CULS_OK) why = eng.error();
+    }
+    if (rc != CULS_OK && n > 1 && !written && rc != CULS_E_DEVICE) {
+        // one job's failure (a malformed graph, a cap) stays its own: each
+        // job runs again alone
+        for (ServeJob *j : batch) {
+            std::vector<ServeJob *> one{j};
+            run_batch(eng, engMu, one);
+        }
+        return;
     }
     const auto now = std::chrono::steady_clock::now();
     std::lock_guard<std::mutex> lk(mu_);

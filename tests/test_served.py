@@ -1,6 +1,7 @@
 """Batch and served entry points (culs_rw_st_batch, culs_submit / culs_poll /
 culs_wait / culs_fetch): every result equals the oracle's `rw; st` of the
 same graph, exactly, whichever batch a graph or job ends up in."""
+import numpy as np
 import pytest
 
 import culs_b200 as C
@@ -172,5 +173,33 @@ def test_cancel_queued_job(ctx):
         assert e.value.code == C.CULS_E_INVALID
         out, _ = ctx.fetch(j1)
         assert same_graph(out, oracle_rw_st(big).graph())
+    finally:
+        ctx.serve_stop()
+
+
+def test_bad_job_fails_alone(ctx):
+    """A malformed graph (a fanin that is not below its node) batched with
+    valid ones fails with CULS_E_INVALID; the others still match the oracle."""
+    big = C.gen_layered(32, 256, 64, 300000, 200, 4, 0.0, True)
+    good = [C.gen_multiplier(8), C.gen_layered(33, 32, 16, 3000, 30, 4, 0.0, True)]
+    m = C.gen_multiplier(6)
+    f0 = np.array(m.fanin0, copy=True)
+    f0[-1] = 2 * (len(f0) - 1)  # the last AND node as its own fanin
+    bad = C.Aig(m.nPIs, f0, np.asarray(m.fanin1), np.asarray(m.outs))
+    ctx.serve_start(workers=1)
+    try:
+        j0 = ctx.submit(big)  # runs while the next three queue up as one batch
+        js = [ctx.submit(good[0]), ctx.submit(bad), ctx.submit(good[1])]
+        for j in [j0] + js:
+            try:
+                ctx.wait(j, 120000)
+            except C.CulsError:
+                pass
+        with pytest.raises(C.CulsError) as e:
+            ctx.fetch(js[1])
+        assert e.value.code == C.CULS_E_INVALID
+        for j, g in [(j0, big), (js[0], good[0]), (js[2], good[1])]:
+            out, _ = ctx.fetch(j)
+            assert same_graph(out, oracle_rw_st(g).graph())
     finally:
         ctx.serve_stop()
