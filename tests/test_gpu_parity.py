@@ -262,6 +262,20 @@ def test_strash_probe_cap_reports_and_leaves_graph(ctx, monkeypatch):
     d.free()
 
 
+def test_batch_beyond_30_bit_positions_is_refused(ctx):
+    """Node positions are 30-bit: a batch of 3 x 200M AND nodes is refused
+    with CULS_E_INVALID from its sizes alone, before any array is read (each
+    graph here passes 4-element arrays)."""
+    one = np.zeros(4, np.int32)
+    hg = (C._HostGraph * 3)()
+    for h in hg:
+        h.nPIs, h.nPOs, h.nAnds = 1, 0, 200_000_000
+        h.fanin0 = h.fanin1 = h.outs = one.ctypes.data_as(C._ip)
+    out = C._vp()
+    assert C._lib.culs_batch_upload(ctx.h, 3, hg, C.ctypes.byref(out)) == C.CULS_E_INVALID
+    assert out.value is None
+
+
 def test_invalid_graph_rejected(ctx):
     bad = C.Aig(2, np.array([-1, -1, -1, 8], np.int32), np.array([-1, -1, -1, 2], np.int32), np.array([6], np.int32))
     with pytest.raises(C.CulsError) as e:
