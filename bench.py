@@ -36,7 +36,18 @@ sys.path.insert(0, str(ROOT))
 
 import numpy as np  # noqa: E402
 
-from culs_b200.dist import Group  # noqa: E402
+
+def _load_dist():
+    """culs_b200/dist.py loaded by path: importing it as culs_b200.dist would
+    load the package and its CUDA library, which the reference arm must not."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("culs_b200_dist", ROOT / "culs_b200" / "dist.py")
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+Group = _load_dist().Group
 
 METRIC = "rw+st AND-nodes/sec"
 UNIT = "AND-nodes/s"
@@ -50,23 +61,27 @@ KERNELS = {
 }
 
 
-def make_workload(name, rank):
-    import culs_b200 as C
+def make_workload(name, rank, gen=None):
+    """The workload's graphs.  `gen` supplies the seeded generators: the
+    product package by default; the reference arm passes oracle.workload,
+    the same generator sources built without the product's CUDA library."""
+    if gen is None:
+        import culs_b200 as gen
     threads = os.cpu_count() or 8
     if name == "c4":
-        return C.gen_batch(4, rank * 4096, 4096, 1000, 200000, 16, 512, threads=threads)
+        return gen.gen_batch(4, rank * 4096, 4096, 1000, 200000, 16, 512, threads=threads)
     if name == "c5":  # the served workload's job pool
-        return served_pool()
+        return served_pool(gen=gen)
     if name == "c4m":  # profiling case: the first 256 graphs of the c4 family
-        return C.gen_batch(4, rank * 4096, 256, 1000, 200000, 16, 512, threads=threads)
+        return gen.gen_batch(4, rank * 4096, 256, 1000, 200000, 16, 512, threads=threads)
     if name == "c3":
-        return [C.gen_layered(3 + rank, 4096, 4096, 10_000_000, 2000, 3, 0.2, False)]
+        return [gen.gen_layered(3 + rank, 4096, 4096, 10_000_000, 2000, 3, 0.2, False)]
     if name == "c3m":  # profiling case: a 1M-AND member of the c3 family
-        return [C.gen_layered(3 + rank, 4096, 4096, 1_000_000, 200, 3, 0.2, False)]
+        return [gen.gen_layered(3 + rank, 4096, 4096, 1_000_000, 200, 3, 0.2, False)]
     if name == "c2":
-        return [C.gen_multiplier(64)]
+        return [gen.gen_multiplier(64)]
     if name == "c1":
-        return [C.gen_layered(1 + rank, 64, 32, 5000, 40, 4, 0.0, True)]
+        return [gen.gen_layered(1 + rank, 64, 32, 5000, 40, 4, 0.0, True)]
     raise SystemExit(f"unknown workload {name}")
 
 
@@ -125,25 +140,38 @@ def measured_peak():
     return 6650.0, "fallback"
 
 
-def traffic_per_node(kernel):
-    """DRAM bytes per AND node of `kernel` from its committed ncu summary
-    (profiles/<kernel>_traffic.json), if present."""
+def traffic_per_node(kernel, workload):
+    """DRAM bytes per input AND node of `kernel` from its committed ncu
+    summary (profiles/<kernel>_traffic.json), when that capture is of the
+    same workload family (a smaller member, scaled by the AND nodes
+    processed); (None, None) otherwise."""
     p = ROOT / "profiles" / f"{kernel}_traffic.json"
     if p.exists():
         d = json.loads(p.read_text())
-        return float(d["dram_bytes_per_and_node"]), d.get("source", "")
+        if workload in d.get("families", []):
+            return float(d["dram_bytes_per_and_node"]), d.get("source", "")
     return None, None
+
+
+def cpu_model():
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
 
 
 def cpu_baseline(name, graphs, budget_s=12.0, threads=None):
     """Times the CPU restatement of the reference rw;st (oracle/, kind
     "port") on a bounded sample of the workload, on `threads` host threads
     (ctypes releases the GIL, one graph per call)."""
-    import culs_b200 as C
     from oracle.oracle import Graph, Oracle
+    from oracle import workload as W
     threads = threads or (os.cpu_count() or 1)
     if name in ("c3", "c3m"):  # the 10M graph takes minutes on one core: a 1M-AND member of the same family
-        sample = [C.gen_layered(3, 4096, 4096, 1_000_000, 200, 3, 0.2, False)]
+        sample = [W.gen_layered(3, 4096, 4096, 1_000_000, 200, 3, 0.2, False)]
         desc = "c3 family (80% window-3 / 20% far fanins), one 1M-AND graph, 1 thread"
         threads = 1
     else:
@@ -171,7 +199,7 @@ def cpu_baseline(name, graphs, budget_s=12.0, threads=None):
         for f in futs:
             done += f.result()
     dt = time.perf_counter() - t0
-    return {"value": done / dt, "unit": UNIT, "cores": threads, "kind": "port",
+    return {"value": done / dt, "unit": UNIT, "cores": threads, "cpu_model": cpu_model(), "kind": "port",
             "sample": f"{desc}: {done} AND nodes in {dt:.1f} s"}
 
 
@@ -182,7 +210,7 @@ def reference_gpu_path(graphs, max_nodes=4_000_000, timeout_s=600):
     best of 2 runs after a warm-up.  None when the harness or a GPU is
     missing."""
     import tempfile
-    import culs_b200 as C
+    from oracle import workload as W
     exe = ROOT / "oracle" / "_ref" / "rw_harness"
     if not exe.exists():
         return None
@@ -198,7 +226,7 @@ def reference_gpu_path(graphs, max_nodes=4_000_000, timeout_s=600):
             if nodes >= max_nodes:
                 break
             f = Path(d) / f"g{i}.aig"
-            C.write_aiger(f, g)
+            W.write_aiger(f, g)
             files.append(str(f))
             nodes += g.nAnds
         r = subprocess.run([str(exe), "time", "2"] + files, capture_output=True, text=True, timeout=timeout_s)
@@ -218,7 +246,8 @@ def reference_arm(args, group):
     CPU implementation to run), all host threads, a bounded sample per step."""
     if group.rank != 0:
         return 0
-    graphs = make_workload(args.workload, 0)
+    from oracle import workload as W
+    graphs = make_workload(args.workload, 0, gen=W)
     budget = 6.0
     for _ in range(args.warmup):
         cpu_baseline(args.workload, graphs, budget_s=1.0)
@@ -270,14 +299,15 @@ def plain_path(ctx, graphs, budget_s=8.0, e2e=False):
                       (", upload + rw;st + download, wall clock" if e2e else ", device-resident, CUDA events")}
 
 
-def served_pool(seed=5, count=128):
+def served_pool(seed=5, count=128, gen=None):
     """Job pool of the served workload: half seeded c4-family graphs with AND
     counts log-uniform in 500-2M, half n x n array multipliers, n uniform in
     8-128."""
-    import culs_b200 as C
+    if gen is None:
+        import culs_b200 as gen
     rng = np.random.default_rng(seed)
-    pool = C.gen_batch(seed, 0, count // 2, 500, 2_000_000, 16, 512, threads=os.cpu_count() or 8)
-    pool += [C.gen_multiplier(int(n)) for n in rng.integers(8, 129, count - count // 2)]
+    pool = gen.gen_batch(seed, 0, count // 2, 500, 2_000_000, 16, 512, threads=os.cpu_count() or 8)
+    pool += [gen.gen_multiplier(int(n)) for n in rng.integers(8, 129, count - count // 2)]
     return pool
 
 
@@ -379,6 +409,79 @@ def served_arm(args, group):
     return 0
 
 
+def parity_sample(ctx, graphs, dw, count=64, largest=8):
+    """Checks the timed batch's outputs outside the timed region: a fixed
+    sample of its graphs (the `largest` largest and the rest spread evenly
+    over the batch) is downloaded from the batch result `dw` and compared
+    node for node with the plain single-graph path run on the same input
+    graph.  Returns the summary that goes into the JSON line."""
+    import culs_b200 as C
+    n = len(graphs)
+    by_size = sorted(range(n), key=lambda i: -graphs[i].nAnds)
+    pick = list(by_size[:largest])
+    rest = [i for i in range(n) if i not in set(pick)]
+    step = max(1, len(rest) // max(1, count - len(pick)))
+    pick += rest[::step][:count - len(pick)]
+    bad = []
+    nodes = 0
+    for i in sorted(pick):
+        got = dw.download(i)
+        d = ctx.upload(graphs[i])
+        ctx.rw_st(d)
+        ref = d.download()
+        d.free()
+        same = (np.array_equal(got.fanin0, ref.fanin0) and np.array_equal(got.fanin1, ref.fanin1)
+                and np.array_equal(got.outs, ref.outs))
+        if not same:
+            bad.append(i)
+        nodes += graphs[i].nAnds
+    return {"checked": len(pick), "mismatches": len(bad), "mismatched_graphs": bad[:16],
+            "and_nodes_checked": nodes, "largest_checked": graphs[by_size[0]].nAnds if n else 0,
+            "against": "plain single-graph path on the same input graph, node for node"}
+
+
+def parity_digest(dw, workload):
+    """The single-graph workloads with a committed oracle digest
+    (tests/golden/c3_layered10M.json: SHA-256 of the oracle's rw;st result on
+    the same seeded graph) are checked against it."""
+    import hashlib
+    p = ROOT / "tests" / "golden" / "c3_layered10M.json"
+    if workload != "c3" or not p.exists():
+        return None
+    want = json.loads(p.read_text())["rw_st"]
+    got = dw.download(0)
+    h = hashlib.sha256()
+    for a in (got.fanin0, got.fanin1, got.outs):
+        h.update(np.ascontiguousarray(np.asarray(a, np.int32)).tobytes())
+    ok = h.hexdigest() == want["sha256"]
+    return {"checked": 1, "mismatches": 0 if ok else 1, "and_nodes_checked": got.nAnds,
+            "against": "oracle rw;st digest (tests/golden/c3_layered10M.json)"}
+
+
+def single_graph_c2(ctx, reps=5):
+    """Config 2 on the plain single-graph path: the 64x64 array multiplier,
+    device-resident (clone + rw;st, CUDA events), median of `reps` runs after
+    two warm-ups."""
+    import culs_b200 as C
+    g = C.gen_multiplier(64)
+    d0 = ctx.upload(g)
+    times = []
+    for r in range(reps + 2):
+        d = ctx.clone(d0)
+        ctx.sync()
+        ctx.mark(0)
+        ctx.rw_st(d)
+        ctx.mark(1)
+        ctx.sync()
+        if r >= 2:
+            times.append(ctx.profile_read()["user"])
+        d.free()
+    d0.free()
+    ms = statistics.median(times)
+    return {"workload": WORKLOAD_DESC["c2"], "and_nodes": g.nAnds, "ms": ms, "value": g.nAnds / (ms / 1e3),
+            "unit": UNIT, "runs_ms": [round(t, 3) for t in times]}
+
+
 def our_arm(args, group):
     import culs_b200 as C
     ctx = C.Context(device=group.local)
@@ -455,7 +558,7 @@ def our_arm(args, group):
     kdesc, alg = KERNELS[kname]
     k_ms = prof[kname]
     achieved = alg * n_and / (k_ms / 1e3) / 1e9 if k_ms > 0 else None
-    tpn, tsrc = traffic_per_node(kname)
+    tpn, tsrc = traffic_per_node(kname, args.workload)
     roof = {"kernel": f"{kname} ({kdesc})", "bound": "hbm", "achieved": achieved, "peak": peak,
             "peak_kind": f"{peak_kind} hbm_gbs", "unit": "GB/s", "frac": achieved / peak if achieved else None,
             "traffic": tpn * n_and if tpn else None, "traffic_source": tsrc,
@@ -476,17 +579,26 @@ def our_arm(args, group):
             "e2e_aiger": e2e_aiger,
             "clocks": clk.summary(), "gpu_launches": launches,
             "stages_ms_last_step": {k: round(v, 3) for k, v in prof.items() if k not in ("user",)}}
+    # parity of the timed result (outside the timed region): a sample of the
+    # batch against the plain path, or the single graph against its digest
+    if len(graphs) > 1:
+        par = parity_sample(ctx, graphs, dw)
+    else:
+        par = parity_digest(dw, args.workload)
+    line["parity"] = par
+    bad = group.sum(par["mismatches"] if par else 0)
     if group.rank == 0:
         if group.world == 1 and len(graphs) > 1:
             plain = plain_path(ctx, graphs)
             line["plain_single_graph_path"] = plain
             line["batched_vs_plain"] = value / plain["value"] if plain["value"] else None
+            line["single_graph_c2"] = single_graph_c2(ctx)
         line["cpu_baseline"] = cpu_baseline(args.workload, graphs) if group.world == 1 else None
         print(json.dumps(line), flush=True)
     dw.free()
     d0.free()
     ctx.close()
-    return 0
+    return 1 if bad else 0
 
 
 def main():

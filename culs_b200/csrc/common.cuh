@@ -95,18 +95,33 @@ inline void set_status(int *status, int code) {
 inline void backoff(int64_t) {}
 #endif
 
+// A status pointer handed to a kernel addresses two words: status[0] is the
+// status word the first failing thread writes, status[1] the spin bound of
+// the dependency waits that report into it (0 means kSpinLimit).  The host
+// lowers the bound (CULS_SPIN_LIMIT) to make waits run out on purpose.
+CULS_HD int64_t spin_limit(const int *status) {
+    const int l = ld_cg(status + 1);
+    return l > 0 ? (int64_t)l : kSpinLimit;
+}
+
 // Waits until *flag >= target.  Returns false (and records kDevWaitTimeout)
-// when the bound expires, so that no dependency wait can hang the GPU.
+// when the bound expires, so that no dependency wait can hang the GPU.  A
+// wait also gives up at once, without recording anything, when the status
+// word already holds an error: the call has failed, and the work it waits
+// for may itself have been skipped, so one expired wait does not make every
+// dependent wait spin out its own bound.
 CULS_HD bool wait_ge(const int *flag, int target, int *status) {
-    int64_t it = 0;
-    while (ld_acquire(flag) < target) {
-        if (++it > kSpinLimit) {
+    if (ld_acquire(flag) >= target) return true;
+    const int64_t lim = spin_limit(status);
+    for (int64_t it = 1;; ++it) {
+        if ((it & 31) == 1 && ld_cg(status) != kDevOk) return false;
+        if (it >= lim) {
             set_status(status, kDevWaitTimeout);
             return false;
         }
         backoff(it);
+        if (ld_acquire(flag) >= target) return true;
     }
-    return true;
 }
 
 // MurmurHash3 64-bit finalizer (public domain, Austin Appleby).

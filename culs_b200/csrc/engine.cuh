@@ -192,6 +192,7 @@ class Engine {
     int ensure_arena(size_t bytes);
     int ensure_stage(size_t ints);  // pinned host staging of at least `ints` int32
     ExecCtx ctx();
+    void apply_spin_limit();
 
     // stage helpers
     // Strash over M positions: L0/L1 are AIGMan-convention literals over
@@ -216,7 +217,8 @@ class Engine {
     std::string err_;
     cudaStream_t s_ = nullptr;
     RwLib *lib_ = nullptr;
-    int *status_ = nullptr;     // device status word
+    int *status_ = nullptr;     // device status word and spin bound (2 ints)
+    int spinLimit_ = 0;         // the bound last written to status_[1]
     int *counters_ = nullptr;   // device scratch counters
     int *hostSmall_ = nullptr;  // pinned host scratch
     int32_t *stage_ = nullptr;  // pinned staging for uploads and downloads

@@ -1,5 +1,6 @@
 // Engine set-up, batch upload/download and the `st` command.
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -292,7 +293,22 @@ int Engine::check_status(const char *what) {
     return X.status_check(what);
 }
 
+// CULS_SPIN_LIMIT (spin iterations, 0 or unset = the built-in bound of about
+// one second) bounds every dependency wait of the next calls; the tests lower
+// it to make waits run out on purpose.  Read at each call, like
+// CULS_STRASH_TABLE_CAP.
+void Engine::apply_spin_limit() {
+    const char *env = getenv("CULS_SPIN_LIMIT");
+    long long want = env ? atoll(env) : 0;
+    if (want < 0 || want > (1ll << 30)) want = 0;
+    if ((int)want == spinLimit_) return;
+    const int v = (int)want;
+    // pageable source: the call returns once v has been staged
+    if (cudaMemcpyAsync(status_ + 1, &v, sizeof(int), cudaMemcpyHostToDevice, s_) == cudaSuccess) spinLimit_ = v;
+}
+
 ExecCtx Engine::ctx() {
+    apply_spin_limit();
     ExecCtx X;
     X.s = s_;
     X.ar = &ar_;
@@ -326,8 +342,9 @@ int Engine::init(size_t hbmBudget) {
     if (!rc) rc = check(cudaMemcpy(lib_, h, sizeof(RwLib), cudaMemcpyHostToDevice), "library upload");
     delete h;
     if (rc) return rc;
-    if ((rc = check(cudaMalloc(&status_, sizeof(int)), "cudaMalloc"))) return rc;
-    if ((rc = check(cudaMemset(status_, 0, sizeof(int)), "memset"))) return rc;
+    // status word and the spin bound of dependency waits (see common.cuh)
+    if ((rc = check(cudaMalloc(&status_, sizeof(int) * 2), "cudaMalloc"))) return rc;
+    if ((rc = check(cudaMemset(status_, 0, sizeof(int) * 2), "memset"))) return rc;
     if ((rc = check(cudaMalloc(&counters_, sizeof(int) * 64), "cudaMalloc"))) return rc;
     if ((rc = check(cudaMallocHost(&hostSmall_, sizeof(int) * 64), "cudaMallocHost"))) return rc;
     for (auto &e : ev_)

@@ -138,15 +138,18 @@ __device__ __forceinline__ int queue_try_pop_warp(const WorkQueue &q, int &h, bo
 }
 
 // End-of-round bookkeeping of a worklist warp: returns true when the warp
-// must leave (all lanes drained, or no progress for kSpinLimit rounds, which
-// is recorded in *status).
+// must leave (all lanes drained; the status word already holds an error; or
+// no progress for spin_limit(status) rounds, which is recorded in *status).
+// The decision is uniform across the warp.
 __device__ __forceinline__ bool queue_round_end(bool fin, bool progressed, int64_t &idle, int *status) {
     if (__all_sync(0xffffffffu, fin)) return true;
     if (__any_sync(0xffffffffu, progressed)) {
         idle = 0;
         return false;
     }
-    if (++idle > kSpinLimit) {
+    int failed = (threadIdx.x & 31) == 0 ? (ld_cg(status) != kDevOk) : 0;
+    if (__shfl_sync(0xffffffffu, failed, 0)) return true;
+    if (++idle > spin_limit(status)) {
         if ((threadIdx.x & 31) == 0) set_status(status, kDevWaitTimeout);
         return true;
     }

@@ -1,15 +1,16 @@
 // culs_levels_noalloc: AIG level computation that allocates no memory.
 //
-// Some callers cannot call cudaMalloc: code running inside a CUDA graph
-// being captured, a host process whose memory pool is owned and sized by
-// another runtime, or an allocator-free embedding that must not fragment a
-// device heap shared with other work.  For them this entry point computes the
-// ASAP level of every object of one AIG (the same per-node recurrence as the
-// levelization kernel of the rewriting pass, k_front_levelize in
-// rw_front.cu) with its scratch -- completion flags, level words, a work
-// counter and a status word -- in a fixed file-scope device array instead of
-// the engine's arena.  The caller passes device pointers to the inputs and to
-// the outputs.
+// Some callers cannot call cudaMalloc: a host process whose device memory is
+// owned and sized by another runtime, or an allocator-free embedding that
+// must not fragment a device heap shared with other work.  For them this
+// entry point computes the ASAP level of every object of one AIG (the same
+// per-node recurrence as the levelization kernel of the rewriting pass,
+// k_front_levelize in rw_front.cu) with its scratch -- completion flags,
+// level words, a work counter, a status word and its spin bound -- in a
+// fixed file-scope device array instead of the engine's arena.  The caller
+// passes device pointers to the inputs and to the outputs.  The call
+// synchronises the caller's stream and reads the status word back before it
+// returns.
 //
 // Limits and sharing:
 //  * at most CULS_LEVELS_NOALLOC_MAX_OBJS objects (1 + nPIs + nAnds); larger
@@ -22,7 +23,9 @@
 //    serialised by the caller;
 //  * the first call on a device looks up the array's device address
 //    (cudaGetSymbolAddress) with that device current, so make that first
-//    call before any stream capture begins.
+//    call before any stream capture begins.  The address is kept for the
+//    life of the process: a device reset (cudaDeviceReset) in between
+//    invalidates it, and calls after one are not supported.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -57,7 +60,8 @@ __global__ void k_na_init(int nObjs, int nPIs, int *done, int *lp, int *ctl) {
 // Variant of k_front_levelize: the same in-order dataflow over a
 // topologically ordered AIG (chunks claimed in increasing order, bounded
 // waits on the fanins' completion flags), reading AIGMan literals of one
-// graph and writing plain levels.  ctl = {counter, max level, status}.
+// graph and writing plain levels.  ctl = {counter, max level, status, spin
+// bound}; the status and its spin bound are the pair culs::wait_ge reads.
 __global__ void __launch_bounds__(kBlockNA) k_na_levelize(int nObjs, const int *f0, const int *f1, int *done, int *lp,
                                                            int *ctl, int *levels) {
     __shared__ int s_chunk;
@@ -127,9 +131,10 @@ extern "C" int culs_levels_noalloc(const int32_t *d_fanin0, const int32_t *d_fan
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     k_na_levelize<<<sms * 4, kBlockNA, 0, s>>>((int)nObjs, d_fanin0, d_fanin1, done, lp, ctl, d_levels);
     if (cudaGetLastError() != cudaSuccess) return CULS_E_DEVICE;
-    cudaMemcpyAsync(d_maxLevel, &ctl[1], sizeof(int32_t), cudaMemcpyDeviceToDevice, s);
+    if (cudaMemcpyAsync(d_maxLevel, &ctl[1], sizeof(int32_t), cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+        return CULS_E_DEVICE;
     int status = 0;
-    cudaMemcpyAsync(&status, &ctl[2], sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (cudaMemcpyAsync(&status, &ctl[2], sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess) return CULS_E_DEVICE;
     if (cudaStreamSynchronize(s) != cudaSuccess) return CULS_E_DEVICE;
     if (status == culs::kDevBadGraph) return CULS_E_INVALID;
     if (status != 0) return CULS_E_PROBE;

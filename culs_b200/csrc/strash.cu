@@ -621,6 +621,8 @@ int Engine::strash_core(Batch &b, int64_t M, const int *L0, const int *L1, const
         int *lists[2] = {cnt, off};  // free until the levels are known
         int *idx = items;
         check(cudaMemsetAsync(qc, 0, sizeof(int) * 8, s), "memset");
+        // qc[7] is these passes' own status word; qc[8] its spin bound
+        check(cudaMemcpyAsync(qc + 8, status_ + 1, sizeof(int), cudaMemcpyDeviceToDevice, s), "copy");
         check(cudaMemsetAsync(graphLevels, 0, sizeof(int) * (G + 1), s), "memset");
         check(cudaMemsetAsync(level, 0, sizeof(int) * (M + 1), s), "memset");
         k_live_flags<<<gridM, kBlock, 0, s>>>(M, L0, dead, liveFlag, done);

@@ -246,18 +246,22 @@ int culs_dump_copy(culs_ctx *ctx, int which, int32_t *out);
 
 /* ASAP level of every object of one AIG without allocating any memory.  No
  * counterpart in the reference: it serves callers that cannot call
- * cudaMalloc (code inside a CUDA graph capture, hosts whose device memory is
- * owned by another runtime, allocator-free embeddings).  d_fanin0/d_fanin1
- * are device pointers to the AIGMan fanin arrays of one topologically
- * ordered graph (1 + nPIs + nAnds entries, constant and PIs ignored);
- * d_levels receives one level per object and d_maxLevel the depth (0 without
- * AND nodes), both device pointers; stream is a cudaStream_t (NULL = the
- * default stream) and the call returns after the stream has drained.  The
- * scratch is a fixed device array of CULS_LEVELS_NOALLOC_MAX_OBJS objects
+ * cudaMalloc -- hosts whose device memory is owned and sized by another
+ * runtime, and allocator-free embeddings that must not fragment a device
+ * heap shared with other work.  d_fanin0/d_fanin1 are device pointers to the
+ * AIGMan fanin arrays of one topologically ordered graph (1 + nPIs + nAnds
+ * entries, constant and PIs ignored); d_levels receives one level per object
+ * and d_maxLevel the depth (0 without AND nodes), both device pointers;
+ * stream is a cudaStream_t (NULL = the default stream).  The call
+ * synchronises that stream and reads a status word back to the host before
+ * it returns: CULS_E_INVALID for a fanin that is not earlier than its node.
+ * The scratch is a fixed device array of CULS_LEVELS_NOALLOC_MAX_OBJS objects
  * (about 8 MiB, held by every GPU that loads the library until exit); larger
- * graphs get CULS_E_INVALID.  All calls share that array, so calls that
- * overlap on the GPU race; the first call on each device looks the array up
- * and should come before any stream capture.  Needs no culs_ctx. */
+ * graphs get CULS_E_INVALID before anything is launched.  All calls share
+ * that array, so calls that overlap on the GPU race.  The first call on each
+ * device looks the array's address up with that device current and should
+ * come before any stream capture begins; a device reset in the same process
+ * invalidates that address and is not supported.  Needs no culs_ctx. */
 #define CULS_LEVELS_NOALLOC_MAX_OBJS (1 << 20)
 int culs_levels_noalloc(const int32_t *d_fanin0, const int32_t *d_fanin1, int32_t nPIs, int32_t nAnds,
                         int32_t *d_levels, int32_t *d_maxLevel, void *stream);

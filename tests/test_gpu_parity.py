@@ -3,6 +3,7 @@ against the reference's golden fixtures.  Integer work: every comparison is
 exact (tolerance 0)."""
 import hashlib
 import json
+import os
 from pathlib import Path
 
 import numpy as np
@@ -172,6 +173,57 @@ def test_large_single_graph_matches_oracle(ctx):
     assert a.nLevels == b.nLevels
 
 
+def _digest(*arrays):
+    h = hashlib.sha256()
+    for a in arrays:
+        h.update(np.ascontiguousarray(np.asarray(a, np.int32)).tobytes())
+    return h.hexdigest()
+
+
+def test_full_size_single_graph_matches_oracle_digest(ctx):
+    """The 10M-AND single-graph workload (seeded layered AIG, 4,096 PIs and
+    POs, 2,000 layers, 80% window-3 / 20% far fanins): the CUDA path's `rw;
+    st` result equals the oracle's exactly, checked through the SHA-256 of
+    its fanin and output arrays recorded by tests/golden/make_c3_digest.py
+    (the oracle takes about a minute of CPU per pass at this size)."""
+    rec = json.loads((GOLDEN / "c3_layered10M.json").read_text())
+    g = C.gen_layered(*rec["args"])
+    assert _digest(g.fanin0, g.fanin1, g.outs) == rec["input"]["sha256"]
+    d = ctx.upload(g)
+    ctx.rw_st(d)
+    out = d.download()
+    d.free()
+    want = rec["rw_st"]
+    assert (out.nAnds, out.nLevels, out.nPOs) == (want["nAnds"], want["nLevels"], want["nPOs"])
+    assert _digest(out.fanin0, out.fanin1, out.outs) == want["sha256"]
+
+
+def test_wide_c4_family_batch_equals_plain_path_and_oracle(ctx):
+    """256 graphs of the batched workload's family (AND counts log-uniform
+    1k-200k) plus two 200k-AND members, in one batch: every graph's result
+    equals the plain single-graph path on the same graph, node for node, and
+    the largest graphs and a spread sample equal the oracle."""
+    from concurrent.futures import ThreadPoolExecutor
+    gs = C.gen_batch(4, 0, 256, 1000, 200_000, 16, 512, threads=8)
+    gs += C.gen_batch(4, 9000, 2, 200_000, 200_000, 16, 512, threads=8)
+    assert max(g.nAnds for g in gs) > 150_000
+    db = ctx.upload_batch(gs)
+    ctx.rw_st(db)
+    outs = db.download_all()
+    for i, g in enumerate(gs):
+        d = ctx.upload(g)
+        ctx.rw_st(d)
+        assert same_graph(outs[i], d.download()), i
+        d.free()
+    db.free()
+    by_size = sorted(range(len(gs)), key=lambda i: -gs[i].nAnds)
+    sample = by_size[:6] + by_size[6::16]
+    with ThreadPoolExecutor(max_workers=min(16, os.cpu_count() or 4)) as ex:
+        refs = list(ex.map(lambda i: oracle_rw_st(gs[i]).graph(), sample))
+    for i, r in zip(sample, refs):
+        assert same_graph(outs[i], r), i
+
+
 def test_batch_of_generated_graphs_matches_oracle(ctx):
     gs = C.gen_batch(4, 0, 24, 1000, 20000, 16, 512, threads=8)
     db = ctx.upload_batch(gs)
@@ -255,6 +307,34 @@ def test_strash_probe_cap_reports_and_leaves_graph(ctx, monkeypatch):
         ctx.st(d)
     assert e.value.code == C.CULS_E_PROBE
     monkeypatch.delenv("CULS_STRASH_TABLE_CAP")
+    assert same_graph(d.download(), g)
+    ctx.rw(d)
+    ctx.st(d)
+    assert same_graph(d.download(), oracle_rw_st(g).graph())
+    d.free()
+
+
+def test_expired_waits_report_probe_quickly_and_leave_graph(ctx, monkeypatch):
+    """CULS_SPIN_LIMIT=1: a dependency wait that is not satisfied at its first
+    look runs out.  On a deep layered graph the rewrite's dataflow kernels
+    wait, so the call reports CULS_E_PROBE; once one wait has failed the
+    others give up at once instead of spinning out their own bound, so the
+    error comes back quickly.  The graph stays as it was and, with the bound
+    restored, the context runs rw; st and equals the oracle."""
+    import time
+    g = C.gen_layered(11, 64, 32, 200_000, 2000, 3, 0.2, False)
+    d = ctx.upload(g)
+    monkeypatch.setenv("CULS_SPIN_LIMIT", "1")
+    t0 = time.perf_counter()
+    with pytest.raises(C.CulsError) as e:
+        ctx.rw(d)
+    dt = time.perf_counter() - t0
+    assert e.value.code == C.CULS_E_PROBE
+    assert dt < 5.0
+    with pytest.raises(C.CulsError) as e:
+        ctx.st(d)
+    assert e.value.code == C.CULS_E_PROBE
+    monkeypatch.delenv("CULS_SPIN_LIMIT")
     assert same_graph(d.download(), g)
     ctx.rw(d)
     ctx.st(d)

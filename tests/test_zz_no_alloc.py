@@ -1,10 +1,14 @@
 """culs_levels_noalloc: the entry point for callers that cannot allocate
-device memory (inside a CUDA graph capture, or where another runtime owns
-the device memory).  Its scratch is a fixed device array, so this test
-checks, over two calls in a row, that it returns the same depth as the
-existing entry points (culs_graph_upload + culs_graph_stats) and the same
-per-node levels as a host recurrence -- exact, like every integer check here
--- and that it refuses graphs beyond its fixed limit."""
+device memory (a host whose device memory is owned and sized by another
+runtime, or an allocator-free embedding).  Its scratch is a fixed device
+array shared by every call, so this test checks, over two calls in a row,
+that it returns the same depth as the existing entry points
+(culs_graph_upload + culs_graph_stats) and the same per-node levels as a
+host recurrence -- exact, like every integer check here -- and that it
+refuses graphs beyond its fixed limit, refuses a graph whose fanin is not
+earlier than its node after the kernel has run, and works on a stream other
+than the default one.  This file is collected last, so a run that stops at
+its first failure has run every other test before it."""
 import ctypes
 
 import numpy as np
@@ -27,13 +31,14 @@ def host_levels(g):
     return lev
 
 
-def run_noalloc(torch, g):
-    f0 = torch.tensor(np.asarray(g.fanin0, np.int32), device="cuda")
+def run_noalloc(torch, g, fanin0=None, stream=None):
+    f0 = torch.tensor(np.asarray(g.fanin0 if fanin0 is None else fanin0, np.int32), device="cuda")
     f1 = torch.tensor(np.asarray(g.fanin1, np.int32), device="cuda")
     lev = torch.full((g.nObjs,), -7, dtype=torch.int32, device="cuda")
     mx = torch.full((1,), -7, dtype=torch.int32, device="cuda")
     torch.cuda.synchronize()
-    rc = _f(f0.data_ptr(), f1.data_ptr(), g.nPIs, g.nAnds, lev.data_ptr(), mx.data_ptr(), None)
+    rc = _f(f0.data_ptr(), f1.data_ptr(), g.nPIs, g.nAnds, lev.data_ptr(), mx.data_ptr(),
+            None if stream is None else stream.cuda_stream)
     torch.cuda.synchronize()
     return rc, lev.cpu().numpy(), int(mx.cpu().item())
 
@@ -49,6 +54,31 @@ def test_levels_noalloc_two_calls_match_existing_entry_points():
         assert mx == depth
         np.testing.assert_array_equal(lev, host_levels(g))
     ctx.close()
+
+
+def test_levels_noalloc_on_a_caller_stream():
+    torch = pytest.importorskip("torch")
+    g = C.gen_multiplier(12)
+    rc, lev, mx = run_noalloc(torch, g, stream=torch.cuda.Stream())
+    assert rc == 0
+    np.testing.assert_array_equal(lev, host_levels(g))
+    assert mx == int(host_levels(g).max())
+
+
+def test_levels_noalloc_rejects_a_fanin_that_is_not_earlier():
+    """A node whose fanin is itself: the kernel records the malformed graph
+    and the call returns CULS_E_INVALID; the next call on a good graph is
+    unaffected by the shared array's leftover contents."""
+    torch = pytest.importorskip("torch")
+    g = C.gen_multiplier(8)
+    bad = np.array(g.fanin0, np.int32)
+    v = g.nObjs - 3
+    bad[v] = 2 * v
+    rc, _, _ = run_noalloc(torch, g, fanin0=bad)
+    assert rc == -1  # CULS_E_INVALID
+    rc, lev, _ = run_noalloc(torch, g)
+    assert rc == 0
+    np.testing.assert_array_equal(lev, host_levels(g))
 
 
 def test_levels_noalloc_refuses_oversized_graph():
