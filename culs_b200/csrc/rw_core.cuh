@@ -619,33 +619,30 @@ CULS_HD int lib_added(const RwLib *lib, int cls, int out, uint64_t unmatched) {
 
 // One library node of an evaluation batch (the body of EvaluateNode's node
 // loop, src/algorithms/rewrite.cu:400-428), split in two so that a batch's
-// table probes are in flight together: lib_probe_issue decides from the
-// fanins' unmatched bits alone whether the node can match (both fanins
-// matched, neither to the root) and, when it can, loads the home slot of its
-// structural-hash key; lib_probe_finish resolves the probe into a match
-// (recording the matched node and its level) or marks the node unmatched.
-// An unmatched node's match and level entries are left as they are: its
-// level is computed afterwards, and only for the roots that qualify
-// (lib_cone_levels).
+// table probes are in flight together: lib_probe_issue sets the node's level
+// from its fanins and, when both fanins are matched (and not to the root),
+// loads the home slot of its structural-hash key; lib_probe_finish resolves
+// the probe into a match or marks the node unmatched.
 struct LibProbe {
     unsigned long long key;
     int4 slot;  // the key's home slot
     int num;    // library index, or -1 when no probe is pending
 };
 
-CULS_HD void lib_probe_issue(const EvalIn &E, int q, uint32_t w, int isC, const int *match, int stride,
+template <class LevT>
+CULS_HD void lib_probe_issue(const EvalIn &E, int q, uint32_t w, int isC, int *match, LevT *mlev, int stride,
                              uint64_t &unmatched, LibProbe &p) {
     p.num = -1;
     if (w == kNoLibNode) return;
     const int num = (int)((w >> 18) & 63u) + 4;
     const int in0 = ln_f0(w), in1 = ln_f1(w);
-    // inputs (0..3) are never unmatched
-    if (((unmatched >> in0) | (unmatched >> in1)) & 1ull) {
-        unmatched |= 1ull << num;
-        return;
-    }
     const int m0 = match[in0 * stride], m1 = match[in1 * stride];
-    if (m0 == q || m1 == q) {
+    const int lv0 = mlev[in0 * stride], lv1 = mlev[in1 * stride];
+    mlev[num * stride] = (LevT)(1 + (lv0 > lv1 ? lv0 : lv1));
+    match[num * stride] = -1;
+    const bool uin0 = in0 >= 4 && ((unmatched >> in0) & 1ull);
+    const bool uin1 = in1 >= 4 && ((unmatched >> in1) & 1ull);
+    if (uin0 || uin1 || m0 == q || m1 == q) {
         unmatched |= 1ull << num;
         return;
     }
@@ -688,26 +685,6 @@ CULS_HD void lib_probe_finish(const EvalIn &E, const LibProbe &p, int nDel, cons
     }
 }
 
-// Levels of the library nodes in `cone` (a set of internal nodes closed
-// under fanins within the unmatched ones), in index order, as EvaluateNode
-// assigns them (rewrite.cu:405-407,417): an input has its leaf's level, a
-// matched node the level of the node it matched, an unmatched node one
-// more than its deeper fanin.
-template <class LevT>
-CULS_HD void lib_cone_levels(const EvalIn &E, int cls, uint64_t cone, uint64_t unmatched, const int *match,
-                             LevT *mlev, int stride) {
-#pragma unroll
-    for (int j = 0; j < 4; j++) mlev[j * stride] = (LevT)E.level[match[j * stride]];
-    uint64_t todo = cone & unmatched;
-    while (todo) {
-        const int j = 63 - clz64(todo & (~todo + 1ull));  // lowest set bit
-        todo &= todo - 1ull;
-        const uint32_t w = E.lib->node[cls][j - 4];
-        const int lv0 = mlev[ln_f0(w) * stride], lv1 = mlev[ln_f1(w) * stride];
-        mlev[j * stride] = (LevT)(1 + (lv0 > lv1 ? lv0 : lv1));
-    }
-}
-
 template <class T>
 CULS_HD T pick4v(const T (&v)[4], int i) {
     return i == 0 ? v[0] : (i == 1 ? v[1] : (i == 2 ? v[2] : v[3]));
@@ -737,80 +714,79 @@ CULS_HD CutBest eval_cut(const EvalIn &E, int q, int cpos, uint32_t pk, int4 l, 
     const uint32_t npn = E.lib->npn[pk & 0xFFFFu];
     const int uPhase = npn_phase(npn), cls = npn_class(npn);
     const uint32_t perm = *reinterpret_cast<const uint32_t *>(E.lib->perm4[npn_perm(npn)]);
-    const int isC = uPhase & 15;
+    int isC = 0;
 #pragma unroll
-    for (int j = 0; j < 4; j++) match[j * stride] = pick4v(leaves, (int)((perm >> (8 * j)) & 255u));
+    for (int j = 0; j < 4; j++) {
+        const int m = pick4v(leaves, (int)((perm >> (8 * j)) & 255u));
+        match[j * stride] = m;
+        mlev[j * stride] = (LevT)E.level[m];
+        if (uPhase >> j & 1) isC |= 1 << j;
+    }
     // The library nodes in the reference's index order, regrouped into
     // batches of equal depth: every node reads only its fanins' entries, so
-    // this order yields the same matches and unmatched bits.
+    // this order yields the same match, level and unmatched bits.
     //
-    // When the cut's MFFC is the root alone (saved = 1) and zero-gain
-    // replacements are off, a root qualifies only with no unmatched node in
-    // its cone, and `added` only grows: a root is dropped at the first
-    // unmatched node of its cone, a node in no remaining root's cone is not
-    // visited (only cone nodes feed a root's gain and level, and a node's
-    // fanins lie in every cone that holds it), and the walk ends when no
-    // root is left.  The roots that remain are exactly those the full walk
-    // accepts, with the same gains and levels.
+    // Roots that can no longer qualify are dropped as the walk goes: a root
+    // qualifies only with gain = saved - added >= minGain, and `added` (the
+    // unmatched nodes of its cone) only grows, so a root whose cone already
+    // holds more than saved - minGain unmatched nodes is out.  A node in no
+    // live root's cone is not visited -- only cone nodes feed a root's
+    // gain and level, and a node's fanins lie in every cone that holds it --
+    // and the walk ends when no root is left.  The roots that stay are
+    // exactly those the full walk would accept, with the same gains and
+    // levels, so the result is unchanged.
     const int nr = E.lib->nRoots[cls];
-    const bool prune = saved == 1 && !useZeros;
-    uint32_t live = (1u << nr) - 1u;
+    const int budget = saved - (useZeros ? 0 : 1);
+    uint32_t live = budget < 0 ? 0u : ((1u << nr) - 1u);
     uint64_t unmatched = 0;
     const int nb = E.lib->nBatches[cls];
     const uint4 *lbatch = E.lib->batch[cls];
     const unsigned long long *lroots = E.lib->batchRoots[cls];
+    const unsigned long long *cones = E.lib->rootCone[cls];
     for (int bi = 0; bi < nb && live; bi++) {
-        uint4 bw = lbatch[bi];
+        const uint4 bw = lbatch[bi];
         const unsigned long long rm = lroots[bi];
-        if (prune) {
-            if (!((uint32_t)rm & live)) bw.x = kNoLibNode;
-            if (!((uint32_t)(rm >> 16) & live)) bw.y = kNoLibNode;
-            if (!((uint32_t)(rm >> 32) & live)) bw.z = kNoLibNode;
-            if (!((uint32_t)(rm >> 48) & live)) bw.w = kNoLibNode;
-        }
+        const uint32_t r0 = (uint32_t)rm & 0xFFFFu, r1 = (uint32_t)(rm >> 16) & 0xFFFFu;
+        const uint32_t r2 = (uint32_t)(rm >> 32) & 0xFFFFu, r3 = (uint32_t)(rm >> 48) & 0xFFFFu;
         LibProbe p0, p1, p2, p3;  // the batch's probes in flight together
         const uint64_t before = unmatched;
-        lib_probe_issue(E, q, bw.x, isC, match, stride, unmatched, p0);
-        lib_probe_issue(E, q, bw.y, isC, match, stride, unmatched, p1);
-        lib_probe_issue(E, q, bw.z, isC, match, stride, unmatched, p2);
-        lib_probe_issue(E, q, bw.w, isC, match, stride, unmatched, p3);
+        lib_probe_issue(E, q, (r0 & live) ? bw.x : kNoLibNode, isC, match, mlev, stride, unmatched, p0);
+        lib_probe_issue(E, q, (r1 & live) ? bw.y : kNoLibNode, isC, match, mlev, stride, unmatched, p1);
+        lib_probe_issue(E, q, (r2 & live) ? bw.z : kNoLibNode, isC, match, mlev, stride, unmatched, p2);
+        lib_probe_issue(E, q, (r3 & live) ? bw.w : kNoLibNode, isC, match, mlev, stride, unmatched, p3);
         lib_probe_finish(E, p0, nDel, del, match, mlev, stride, unmatched);
         lib_probe_finish(E, p1, nDel, del, match, mlev, stride, unmatched);
         lib_probe_finish(E, p2, nDel, del, match, mlev, stride, unmatched);
         lib_probe_finish(E, p3, nDel, del, match, mlev, stride, unmatched);
-        if (prune && unmatched != before) {
-            // drop the roots whose cone gained an unmatched node
-            const uint64_t fresh = unmatched & ~before;
-            uint32_t dead = 0;
-            if (bw.x != kNoLibNode && ((fresh >> (((bw.x >> 18) & 63u) + 4)) & 1ull)) dead |= (uint32_t)rm;
-            if (bw.y != kNoLibNode && ((fresh >> (((bw.y >> 18) & 63u) + 4)) & 1ull)) dead |= (uint32_t)(rm >> 16);
-            if (bw.z != kNoLibNode && ((fresh >> (((bw.z >> 18) & 63u) + 4)) & 1ull)) dead |= (uint32_t)(rm >> 32);
-            if (bw.w != kNoLibNode && ((fresh >> (((bw.w >> 18) & 63u) + 4)) & 1ull)) dead |= (uint32_t)(rm >> 48);
-            live &= ~dead;
+        // roots whose cone gained an unmatched node in this batch
+        const uint64_t fresh = unmatched & ~before;
+        uint32_t touched = 0;
+        if (fresh) {
+            if (bw.x != kNoLibNode && ((fresh >> (((bw.x >> 18) & 63u) + 4)) & 1ull)) touched |= r0;
+            if (bw.y != kNoLibNode && ((fresh >> (((bw.y >> 18) & 63u) + 4)) & 1ull)) touched |= r1;
+            if (bw.z != kNoLibNode && ((fresh >> (((bw.z >> 18) & 63u) + 4)) & 1ull)) touched |= r2;
+            if (bw.w != kNoLibNode && ((fresh >> (((bw.w >> 18) & 63u) + 4)) & 1ull)) touched |= r3;
+        }
+        touched &= live;
+        if (budget == 0) {
+            live &= ~touched;
+        } else {
+            while (touched) {
+                const int r = ctz32(touched);
+                touched &= touched - 1u;
+                if (popc64(cones[r] & unmatched) > budget) live &= ~(1u << r);
+            }
         }
     }
-    if (!live) return best;
-    const int minGain = useZeros ? 0 : 1;
-    bool leveled = false;
     for (int out = 0; out < nr; out++) {
         if (!((live >> out) & 1u)) continue;
         const int rt = E.lib->roots[cls][out];
-        const bool rtMatched = rt < 4 || !((unmatched >> rt) & 1ull);
-        if (rtMatched && match[rt * stride] == q) continue;
+        if (match[rt * stride] == q) continue;
         const int added = lib_added(E.lib, cls, out, unmatched);
-        const int gain = saved - added;
-        if (gain < minGain) continue;
-        if (best.out >= 0 && gain < best.gain) continue;
-        if (!leveled) {
-            // levels of every live root's unmatched cone nodes, once
-            uint64_t cone = 0;
-            for (int r = 0; r < nr; r++)
-                if ((live >> r) & 1u) cone |= E.lib->rootCone[cls][r];
-            lib_cone_levels(E, cls, cone, unmatched, match, mlev, stride);
-            leveled = true;
-        }
         const int rtLevel = mlev[rt * stride];
-        if (best.out >= 0 && gain == best.gain && rtLevel >= best.level) continue;
+        const int gain = saved - added;
+        if (gain < 0 || (gain == 0 && !useZeros)) continue;
+        if (best.out >= 0 && (gain < best.gain || (gain == best.gain && rtLevel >= best.level))) continue;
         best = CutBest{gain, rtLevel, out};
     }
     return best;
