@@ -208,7 +208,6 @@ static bool decode_lib(const unsigned char *b, size_t n, RwLib &L) {
     memset(L.roots, 0, sizeof L.roots);
     memset(L.batch, 0xFF, sizeof L.batch);
     memset(L.rootCone, 0, sizeof L.rootCone);
-    memset(L.batchRoots, 0, sizeof L.batchRoots);
     for (int c = 0; c < kNumClasses; c++) {
         if (L.nNodes[c] > kMaxLibNodes - 4 || L.nRoots[c] > 16) return false;
         if (!need((size_t)L.nNodes[c] * 4 + L.nRoots[c])) return false;
@@ -253,21 +252,6 @@ static bool decode_lib(const unsigned char *b, size_t n, RwLib &L) {
         for (int r = 0; r < L.nRoots[c]; r++) {
             if (L.roots[c][r] >= 4 + L.nNodes[c]) return false;
             L.rootCone[c][r] = cone[L.roots[c][r]];
-        }
-        // per batch entry: the roots whose cone holds its node
-        for (int bi = 0; bi < nb; bi++) {
-            const uint32_t ent[kLibBatch] = {L.batch[c][bi].x, L.batch[c][bi].y, L.batch[c][bi].z,
-                                             L.batch[c][bi].w};
-            unsigned long long rm = 0;
-            for (int e = 0; e < kLibBatch; e++) {
-                if (ent[e] == kNoLibNode) continue;
-                const int j = (int)((ent[e] >> 18) & 63u) + 4;
-                uint32_t m = 0;
-                for (int r = 0; r < L.nRoots[c]; r++)
-                    if ((L.rootCone[c][r] >> j) & 1ull) m |= 1u << r;
-                rm |= (unsigned long long)m << (16 * e);
-            }
-            L.batchRoots[c][bi] = rm;
         }
     }
     int order[kNumClasses];

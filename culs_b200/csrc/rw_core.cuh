@@ -38,10 +38,6 @@ struct RwLib {
     // Per class and root: bit j set for every internal node j (j >= 4) in
     // the root's cone, the root included.
     unsigned long long rootCone[kNumClasses][16];
-    // Per class and evaluation batch: for each of the batch's four entries
-    // (16 bits each, entry e at bit 16 * e), the roots whose cone holds that
-    // entry's node.
-    unsigned long long batchRoots[kNumClasses][kMaxLibNodes];
     // Evaluation order of the classes: by number of batches, then class, so
     // that cut items sorted by this slot put forests of equal batch count
     // side by side.
@@ -590,14 +586,6 @@ CULS_HD bool mffc_trivial(const EvalIn &E, int root, const int (&leaves)[4]) {
     return (l0 || E.ref[f0] >= 2) && (l1 || E.ref[f1] >= 2);
 }
 
-CULS_HD int ctz32(uint32_t x) {
-#if defined(__CUDA_ARCH__)
-    return __ffs((int)x) - 1;
-#else
-    return __builtin_ctz(x);
-#endif
-}
-
 CULS_HD int clz64(uint64_t x) {
 #if defined(__CUDA_ARCH__)
     return __clzll((long long)x);
@@ -725,61 +713,23 @@ CULS_HD CutBest eval_cut(const EvalIn &E, int q, int cpos, uint32_t pk, int4 l, 
     // The library nodes in the reference's index order, regrouped into
     // batches of equal depth: every node reads only its fanins' entries, so
     // this order yields the same match, level and unmatched bits.
-    //
-    // Roots that can no longer qualify are dropped as the walk goes: a root
-    // qualifies only with gain = saved - added >= minGain, and `added` (the
-    // unmatched nodes of its cone) only grows, so a root whose cone already
-    // holds more than saved - minGain unmatched nodes is out.  A node in no
-    // live root's cone is not visited -- only cone nodes feed a root's
-    // gain and level, and a node's fanins lie in every cone that holds it --
-    // and the walk ends when no root is left.  The roots that stay are
-    // exactly those the full walk would accept, with the same gains and
-    // levels, so the result is unchanged.
-    const int nr = E.lib->nRoots[cls];
-    const int budget = saved - (useZeros ? 0 : 1);
-    uint32_t live = budget < 0 ? 0u : ((1u << nr) - 1u);
     uint64_t unmatched = 0;
     const int nb = E.lib->nBatches[cls];
     const uint4 *lbatch = E.lib->batch[cls];
-    const unsigned long long *lroots = E.lib->batchRoots[cls];
-    const unsigned long long *cones = E.lib->rootCone[cls];
-    for (int bi = 0; bi < nb && live; bi++) {
+    for (int bi = 0; bi < nb; bi++) {
         const uint4 bw = lbatch[bi];
-        const unsigned long long rm = lroots[bi];
-        const uint32_t r0 = (uint32_t)rm & 0xFFFFu, r1 = (uint32_t)(rm >> 16) & 0xFFFFu;
-        const uint32_t r2 = (uint32_t)(rm >> 32) & 0xFFFFu, r3 = (uint32_t)(rm >> 48) & 0xFFFFu;
         LibProbe p0, p1, p2, p3;  // the batch's probes in flight together
-        const uint64_t before = unmatched;
-        lib_probe_issue(E, q, (r0 & live) ? bw.x : kNoLibNode, isC, match, mlev, stride, unmatched, p0);
-        lib_probe_issue(E, q, (r1 & live) ? bw.y : kNoLibNode, isC, match, mlev, stride, unmatched, p1);
-        lib_probe_issue(E, q, (r2 & live) ? bw.z : kNoLibNode, isC, match, mlev, stride, unmatched, p2);
-        lib_probe_issue(E, q, (r3 & live) ? bw.w : kNoLibNode, isC, match, mlev, stride, unmatched, p3);
+        lib_probe_issue(E, q, bw.x, isC, match, mlev, stride, unmatched, p0);
+        lib_probe_issue(E, q, bw.y, isC, match, mlev, stride, unmatched, p1);
+        lib_probe_issue(E, q, bw.z, isC, match, mlev, stride, unmatched, p2);
+        lib_probe_issue(E, q, bw.w, isC, match, mlev, stride, unmatched, p3);
         lib_probe_finish(E, p0, nDel, del, match, mlev, stride, unmatched);
         lib_probe_finish(E, p1, nDel, del, match, mlev, stride, unmatched);
         lib_probe_finish(E, p2, nDel, del, match, mlev, stride, unmatched);
         lib_probe_finish(E, p3, nDel, del, match, mlev, stride, unmatched);
-        // roots whose cone gained an unmatched node in this batch
-        const uint64_t fresh = unmatched & ~before;
-        uint32_t touched = 0;
-        if (fresh) {
-            if (bw.x != kNoLibNode && ((fresh >> (((bw.x >> 18) & 63u) + 4)) & 1ull)) touched |= r0;
-            if (bw.y != kNoLibNode && ((fresh >> (((bw.y >> 18) & 63u) + 4)) & 1ull)) touched |= r1;
-            if (bw.z != kNoLibNode && ((fresh >> (((bw.z >> 18) & 63u) + 4)) & 1ull)) touched |= r2;
-            if (bw.w != kNoLibNode && ((fresh >> (((bw.w >> 18) & 63u) + 4)) & 1ull)) touched |= r3;
-        }
-        touched &= live;
-        if (budget == 0) {
-            live &= ~touched;
-        } else {
-            while (touched) {
-                const int r = ctz32(touched);
-                touched &= touched - 1u;
-                if (popc64(cones[r] & unmatched) > budget) live &= ~(1u << r);
-            }
-        }
     }
+    const int nr = E.lib->nRoots[cls];
     for (int out = 0; out < nr; out++) {
-        if (!((live >> out) & 1u)) continue;
         const int rt = E.lib->roots[cls][out];
         if (match[rt * stride] == q) continue;
         const int added = lib_added(E.lib, cls, out, unmatched);
