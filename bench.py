@@ -56,7 +56,10 @@ UNIT = "AND-nodes/s"
 # one that takes longest.
 KERNELS = {
     "k_enumerate": ("cut enumeration", 584),  # 2 fanin cut sets read + own set written
-    "k_evaluate": ("MFFC + NPN match + gain", 328),  # own cuts, fanins, refs, levels, table probes
+    # table build and evaluation alternate per group of graphs inside one
+    # marked region: own cuts, fanins, refs, levels, table probes (328) plus
+    # the build's byGraph, fanins, graph, level reads and slot write (36)
+    "k_evaluate": ("existence-table build + MFFC + NPN match + gain", 364),
     "k_dedup": ("strash hashing dataflow", 52),  # fanins, level, map, table slot, key out
 }
 

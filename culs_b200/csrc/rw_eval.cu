@@ -10,6 +10,7 @@
 // k_evaluate); the match/level scratch of a library walk lives in shared
 // memory laid out entry-major, so lanes reading the same library entry hit
 // distinct banks.
+#include <algorithm>
 #include <vector>
 
 #include "rw_work.cuh"
@@ -34,10 +35,11 @@ __global__ void k_table_clear(int64_t n, TabSlot *slots) {
         reinterpret_cast<int4 *>(slots)[i] = make_int4(-1, -1, 0x7FFFFFFF, 0);
 }
 
-__global__ void k_table_build(int64_t nL0, int64_t N, const int *byGraph, const int *w0, const int *w1, const int *wg,
-                              const int *wlev, const DevGraph *dg, RegionTable tab, int *status) {
+// Inserts the AND nodes at graph-major indices [lo, hi) of byGraph.
+__global__ void k_table_build(int64_t nL0, int64_t lo, int64_t hi, const int *byGraph, const int *w0, const int *w1,
+                              const int *wg, const int *wlev, const DevGraph *dg, RegionTable tab, int *status) {
     int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += stride) {
+    for (int64_t i = lo + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < hi; i += stride) {
         const int q = byGraph[i];
         if (q < nL0) continue;  // constant or PI
         int f0 = w0[q], f1 = w1[q];
@@ -50,7 +52,7 @@ __global__ void k_table_build(int64_t nL0, int64_t N, const int *byGraph, const 
 }
 
 struct EvalArgs {
-    int64_t nL0, N;
+    int64_t nL0, lo, hi;  // evaluates the nodes at graph-major indices [lo, hi) of byGraph
     const int *byGraph;
     int *scratch;  // 2 * kLibSlots ints per thread of the grid, thread-minor
     EvalIn E;
@@ -104,11 +106,11 @@ __global__ void __launch_bounds__(kEvalBlock, 8) k_evaluate(EvalArgs A) {
     const int gstride = gridDim.x * blockDim.x;
     int *gmatch = A.scratch + gtid;
     LevT *gmlev = reinterpret_cast<LevT *>(A.scratch + (int64_t)kLibSlots * gstride) + gtid;
-    const int64_t nWarpChunks = (A.N + kWarpNodes - 1) / kWarpNodes;
+    const int64_t nWarpChunks = (A.hi - A.lo + kWarpNodes - 1) / kWarpNodes;
     const int64_t warpStride = (int64_t)gridDim.x * (kEvalBlock / 32);
     for (int64_t wc = (int64_t)blockIdx.x * (kEvalBlock / 32) + (threadIdx.x >> 5); wc < nWarpChunks;
          wc += warpStride) {
-        const int64_t base = wc * kWarpNodes;
+        const int64_t base = A.lo + wc * kWarpNodes;
         for (int c = lane; c < kClassSlots; c += 32) W.off[c] = 0;
         __syncwarp();
         // 1. this lane's nodes: their evaluable cuts and class slots
@@ -118,7 +120,7 @@ __global__ void __launch_bounds__(kEvalBlock, 8) k_evaluate(EvalArgs A) {
         for (int h = 0; h < kNodesPerLane; h++) {
             const int local = h * 32 + lane;
             q[h] = -1;
-            if (base + local < A.N) {
+            if (base + local < A.hi) {
                 q[h] = A.byGraph[base + local];
                 if (q[h] < A.nL0) q[h] = -1;  // constant or PI
             }
@@ -287,19 +289,36 @@ int rw_evaluate(ExecCtx &X, RwWork &w, const Batch &b) {
     if ((rc = X.check(cudaMemsetAsync(candFlag, 0, N, s), "memset"))) return rc;
     if (nAnd > 0) {
         k_table_clear<<<X.grid(nSlots), kBlock, 0, s>>>(nSlots, slots);
-        k_table_build<<<X.grid(N), kBlock, 0, s>>>(w.nL0, N, w.byGraph, w.w0, w.w1, w.wg, w.wlev, w.dg, w.tab,
-                                                   X.status);
-        EvalArgs A{w.nL0, N, w.byGraph, scratch, EvalIn{w.w0, w.w1, w.ref, w.wlev, X.lib, TabRegion{}, X.status}, w.tab,
-                   w.cutL, w.cutM, w.wg, w.dg, w.useZeros ? 1 : 0, mffcNodes, w.bestCut, w.bestOut, candFlag};
         X.mark(kMkEvalK0);
-        // 16-bit library levels when no level of the batch, plus a forest's
-        // depth (at most 50 nodes), can reach 65,535
-        if (w.maxLevel + 64 < 0xFFFF)
-            k_evaluate<uint16_t><<<evalGrid, kEvalBlock, 0, s>>>(A);
-        else
-            k_evaluate<int><<<evalGrid, kEvalBlock, 0, s>>>(A);
+        // Graphs in groups of at most kGroupSlots table slots (256 MB of
+        // regions), each group's regions built right before its nodes are
+        // evaluated, so the probes find them in L2 instead of DRAM (a single
+        // larger graph is a group of its own).
+        constexpr int64_t kGroupSlots = 16ll << 20;
+        const bool lev16 = w.maxLevel + 64 < 0xFFFF;  // see the launch below
+        int g0 = 0;
+        while (g0 < w.G) {
+            int g1 = g0 + 1;
+            while (g1 < w.G && off[g1 + 1] - off[g0] <= kGroupSlots) g1++;
+            const int64_t lo = b.hg[g0].base, hi = g1 < w.G ? (int64_t)b.hg[g1].base : N;
+            k_table_build<<<X.grid(hi - lo), kBlock, 0, s>>>(w.nL0, lo, hi, w.byGraph, w.w0, w.w1, w.wg, w.wlev,
+                                                             w.dg, w.tab, X.status);
+            EvalArgs A{w.nL0,  lo,     hi,     w.byGraph, scratch,
+                       EvalIn{w.w0, w.w1, w.ref, w.wlev, X.lib, TabRegion{}, X.status},
+                       w.tab,  w.cutL, w.cutM, w.wg,      w.dg,
+                       w.useZeros ? 1 : 0, mffcNodes, w.bestCut, w.bestOut, candFlag};
+            const unsigned grid = std::min(evalGrid, X.grid(hi - lo, kEvalBlock));
+            // 16-bit library levels when no level of the batch, plus a
+            // forest's depth (at most 50 nodes), can reach 65,535
+            if (lev16)
+                k_evaluate<uint16_t><<<grid, kEvalBlock, 0, s>>>(A);
+            else
+                k_evaluate<int><<<grid, kEvalBlock, 0, s>>>(A);
+            X.launched(2);
+            g0 = g1;
+        }
         X.mark(kMkEvalK1);
-        X.launched(3);
+        X.launched(1);
     }
     if ((rc = X.check(compact_flags(candFlag, N, w.cand, X.counters + 8, *X.ar, s), "compact"))) return rc;
     if ((rc = X.check(cudaMemcpyAsync(X.hostSmall + 8, X.counters + 8, sizeof(int), cudaMemcpyDeviceToHost, s), "d2h")))
