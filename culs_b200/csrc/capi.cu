@@ -404,7 +404,7 @@ int culs_set_param(culs_ctx *ctx, int which, int64_t value) {
                 t.enumBlocksPerSm = (int)value;
                 return CULS_OK;
             case CULS_PARAM_ENUM_CHUNK_NODES:
-                if (value != 32 && value != 64 && value != 128) return CULS_E_INVALID;
+                if (value < 32 || value > 1024 || value % 32) return CULS_E_INVALID;
                 t.enumChunkNodes = (int)value;
                 return CULS_OK;
             default:

@@ -30,7 +30,7 @@ struct ExecCtx;
 struct Tune {
     int enumWideMin = 16384;   // levels this wide run one node per thread, narrower one per warp
     int enumBlocksPerSm = 8;   // persistent enumeration blocks per SM
-    int enumChunkNodes = 64;   // nodes per chunk of a one-node-per-thread level: 32, 64 or 128
+    int enumChunkNodes = 128;  // nodes per chunk of a one-node-per-thread level (a multiple of 32)
 };
 
 struct DevGraph {

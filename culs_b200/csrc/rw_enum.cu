@@ -337,10 +337,10 @@ __device__ __forceinline__ void enum_node_warp(const EnumArgs &A, int64_t q, int
     if (lane == 0) st_release(&A.done[q], 1);
 }
 
-// One node per lane at a time on wide levels.  A lane's current node: its 8
-// slots in registers (the trivial cut in slot 0), its fanins and the mask of
-// the fanin-cut pairs CutEnumerate tries (both slots used, at most 4 leaves
-// by signature), bit i * 8 + j: visiting the set bits in order is the
+// One node per lane on wide levels.  A lane's node: its 8 slots in
+// registers (the trivial cut in slot 0), its fanins and the mask of the
+// fanin-cut pairs CutEnumerate tries (both slots used, at most 4 leaves by
+// signature), bit i * 8 + j: visiting the set bits in order is the
 // reference's i-major loop.
 struct LaneNode {
     Slot S[8];
@@ -349,25 +349,36 @@ struct LaneNode {
     int u0, u1, c0, c1;
 };
 
-// What a lane learns about a node before it enumerates it: the pair mask,
-// the fanin literals and the trivial cut's signature bit.  A failed wait
-// leaves the mask empty, so the node publishes its trivial cut alone (the
-// call then reports the status word's error).
-struct NodeInfo {
-    uint64_t pairs;
-    int f0, f1;
-    uint32_t lid;
-};
-
-__device__ __forceinline__ void node_info(const EnumArgs &A, int64_t q, NodeInfo &I) {
-    I.f0 = A.w0[q];
-    I.f1 = A.w1[q];
-    I.lid = A.lidLow[q];
-    I.pairs = 0;
-    A.cutA[q * 8] = make_int2((int)clamp_ref(A.ref[q]), (int)(I.lid << 12));  // the trivial cut's aux
-    const int u0 = I.f0 >> 1, u1 = I.f1 >> 1;
-    if (!wait_ge(&A.done[u0], 1, A.status) || !wait_ge(&A.done[u1], 1, A.status)) return;
-    const int2 *M0 = A.cutM + (int64_t)u0 * 8, *M1 = A.cutM + (int64_t)u1 * 8;
+// Starts node q on this lane: slot 0 the trivial cut, the other slots
+// free; waits (bounded) for both fanins and builds the pair mask.  A failed
+// wait leaves the mask empty, so the node publishes its trivial cut alone
+// (the call then reports the status word's error).
+__device__ __forceinline__ void lane_node_begin(const EnumArgs &A, int64_t q, LaneNode &N) {
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        N.S[k].pk = 0;
+        N.S[k].sign = 0;
+        N.S[k].l[0] = N.S[k].l[1] = N.S[k].l[2] = N.S[k].l[3] = 0;
+    }
+    N.q = q;
+    Cut c;
+    c.sign = 1u << A.lidLow[q];
+    c.tt = 0xAAAAu;
+    c.nLeaves = 1;
+    c.used = 1;
+    c.value = 1001u;
+    N.S[0].l[0] = (int)q;
+    N.S[0].sign = c.sign;
+    N.S[0].pk = cut_pack(c);
+    A.cutA[q * 8] = make_int2((int)clamp_ref(A.ref[q]), (int)((uint32_t)A.lidLow[q] << 12));
+    const int f0 = A.w0[q], f1 = A.w1[q];
+    N.u0 = f0 >> 1;
+    N.u1 = f1 >> 1;
+    N.c0 = f0 & 1;
+    N.c1 = f1 & 1;
+    N.pairs = 0;
+    if (!wait_ge(&A.done[N.u0], 1, A.status) || !wait_ge(&A.done[N.u1], 1, A.status)) return;
+    const int2 *M0 = A.cutM + (int64_t)N.u0 * 8, *M1 = A.cutM + (int64_t)N.u1 * 8;
     uint32_t s1[8], used1 = 0;
 #pragma unroll
     for (int j = 0; j < 8; j++) {
@@ -381,34 +392,8 @@ __device__ __forceinline__ void node_info(const EnumArgs &A, int64_t q, NodeInfo
         if (!packed_used((uint32_t)mi.y)) continue;
 #pragma unroll
         for (int j = 0; j < 8; j++)
-            if (((used1 >> j) & 1u) && popc32((uint32_t)mi.x | s1[j]) <= 4) I.pairs |= 1ull << (i * 8 + j);
+            if (((used1 >> j) & 1u) && popc32((uint32_t)mi.x | s1[j]) <= 4) N.pairs |= 1ull << (i * 8 + j);
     }
-}
-
-// Makes node q (with its info) the lane's current node: slot 0 the trivial
-// cut, the other slots free.
-__device__ __forceinline__ void lane_node_begin(int64_t q, const NodeInfo &I, LaneNode &N) {
-#pragma unroll
-    for (int k = 0; k < 8; k++) {
-        N.S[k].pk = 0;
-        N.S[k].sign = 0;
-        N.S[k].l[0] = N.S[k].l[1] = N.S[k].l[2] = N.S[k].l[3] = 0;
-    }
-    N.q = q;
-    Cut c;
-    c.sign = 1u << I.lid;
-    c.tt = 0xAAAAu;
-    c.nLeaves = 1;
-    c.used = 1;
-    c.value = 1001u;
-    N.S[0].l[0] = (int)q;
-    N.S[0].sign = c.sign;
-    N.S[0].pk = cut_pack(c);
-    N.u0 = I.f0 >> 1;
-    N.u1 = I.f1 >> 1;
-    N.c0 = I.f0 & 1;
-    N.c1 = I.f1 & 1;
-    N.pairs = I.pairs;
 }
 
 // The next admissible pair of the lane's node: CutEnumerate's body for one
@@ -487,45 +472,41 @@ __device__ __forceinline__ void lane_node_end(const EnumArgs &A, const LaneNode 
     }
 }
 
-// The nodes [base, base + cnt) of one wide level (cnt <= 32 * K): lane l
-// enumerates nodes l, l + 32, ..., l + 32 (K - 1) one after another.  All K
-// nodes' pair masks are gathered up front, so a lane moves on to its next
-// node without a memory round trip; a warp runs as many rounds as its
-// busiest lane's total pairs, and K nodes per lane even out the pair counts
-// (they vary about twofold between the nodes of a warp).  Nodes of one level
-// never read each other, so a lane never waits on another lane of its warp;
-// the chunk's nodes are published together, after one fence, when it is
-// done.
-template <int K>
+// The nodes [base, base + cnt) of one wide level, one node per lane at a
+// time.  Every round each lane with a node replays one admissible pair; a
+// lane whose node has no pair left publishes it and takes the chunk's next
+// node, so lanes stay busy while the chunk lasts instead of idling until
+// the warp's busiest node is done (admissible pairs per node vary about
+// twofold within a warp).  Nodes of one level never read each other, so a
+// lane never waits on another lane of its warp, and the chunk's nodes are
+// published together when it is done.
 __device__ __forceinline__ void enum_chunk_thread(const EnumArgs &A, int64_t base, int cnt, int lane) {
     const unsigned F = 0xffffffffu;
-    NodeInfo I[K];
-#pragma unroll
-    for (int j = 0; j < K; j++) {
-        I[j].pairs = 0;
-        if (lane + 32 * j < cnt) node_info(A, base + lane + 32 * j, I[j]);
-    }
     LaneNode N;
-    int cur = 0;
     bool active = lane < cnt;
-    if (active) lane_node_begin(base + lane, I[0], N);
+    if (active) lane_node_begin(A, base + lane, N);
+    int next = 32;  // the chunk's next unclaimed node, the same on every lane
     while (true) {
         if (active && !N.pairs) {
             lane_node_end(A, N);
-            cur++;
             active = false;
-#pragma unroll
-            for (int j = 1; j < K; j++)
-                if (cur == j && lane + 32 * j < cnt) {
-                    lane_node_begin(base + lane + 32 * j, I[j], N);
-                    active = true;
-                }
+        }
+        const unsigned need = __ballot_sync(F, !active);
+        if (need && next < cnt) {
+            const int idx = next + __popc(need & ((1u << lane) - 1u));
+            if (!active && idx < cnt) {
+                lane_node_begin(A, base + idx, N);
+                active = true;
+            }
+            next += __popc(need);
         }
         if (!__any_sync(F, active)) break;
         if (active && N.pairs) lane_node_step(A, N);
         __syncwarp();
     }
-    // one fence for the whole chunk, then its nodes are published
+    // one fence for the whole chunk, then its nodes are published: nodes
+    // of the next levels read them only after their flag, and a fence per
+    // finishing round would stall the warp once per distinct pair count
     __threadfence();
     __syncwarp();
     for (int i = lane; i < cnt; i += 32) st_release(&A.done[base + i], 1);
@@ -536,7 +517,6 @@ __device__ __forceinline__ void enum_chunk_thread(const EnumArgs &A, int64_t bas
 // one-node chunks, each node on a whole warp (latency: a narrow level's
 // time is the time of its slowest node).  Warps claim chunks in level
 // order, so every fanin of a claimed node lies in an earlier, claimed chunk.
-template <int K>
 __global__ void __launch_bounds__(kEnumBlock, 3) k_enumerate(EnumArgs A) {
     const unsigned F = 0xffffffffu;
     const int lane = threadIdx.x & 31;
@@ -560,7 +540,7 @@ __global__ void __launch_bounds__(kEnumBlock, 3) k_enumerate(EnumArgs A) {
         if (w >= A.wideMin) {
             const int64_t first = k * A.chunkNodes;
             const int cnt = (int)(w - first < A.chunkNodes ? w - first : A.chunkNodes);
-            enum_chunk_thread<K>(A, base + first, cnt, lane);
+            enum_chunk_thread(A, base + first, cnt, lane);
         } else {
             enum_node_warp(A, base + k, lane);
         }
@@ -614,15 +594,7 @@ int rw_enumerate(ExecCtx &X, RwWork &w) {
                X.tune->enumChunkNodes, w.w0, w.w1, w.ref, w.lidLow, w.cutL, w.cutM, cutA, done,
                X.counters, w.warpPairs, X.status};
     X.mark(kMkEnumK0);
-    // K nodes per lane on wide levels: one kernel per K, so that no
-    // variant's registers weigh on another's
-    const unsigned grid = (unsigned)(X.sms * X.tune->enumBlocksPerSm);
-    if (A.chunkNodes == 32)
-        k_enumerate<1><<<grid, kEnumBlock, 0, s>>>(A);
-    else if (A.chunkNodes == 64)
-        k_enumerate<2><<<grid, kEnumBlock, 0, s>>>(A);
-    else
-        k_enumerate<4><<<grid, kEnumBlock, 0, s>>>(A);
+    k_enumerate<<<(unsigned)(X.sms * X.tune->enumBlocksPerSm), kEnumBlock, 0, s>>>(A);
     X.mark(kMkEnumK1);
     X.launched(6);
     if ((rc = X.check(cudaGetLastError(), "enumerate launch"))) return rc;

@@ -67,7 +67,7 @@ int Engine::autotune(const Batch &sample, int rounds) {
             best = t;
         }
     }
-    const int chunks[] = {32, 64, 128};
+    const int chunks[] = {32, 64, 128, 256};
     for (int c : chunks) {
         if (rc) break;
         Tune t = best;

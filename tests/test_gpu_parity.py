@@ -385,10 +385,10 @@ def test_graph_deeper_than_16_bit_levels_matches_oracle():
         c.close()
 
 
-@pytest.mark.parametrize("wide_min,chunk", [(1, 32), (1, 64), (1, 128), (1 << 30, 64)])
+@pytest.mark.parametrize("wide_min,chunk", [(1, 32), (1, 128), (1, 1024), (1 << 30, 128)])
 def test_both_enumeration_schedules_match_oracle(wide_min, chunk):
-    """Every level on one thread per node (1, each lane taking 1, 2 or 4
-    nodes of a chunk), or every level on one warp per node (2^30): the
+    """Every level on one thread per node (1, with warps taking chunks of 32,
+    128 or 1,024 nodes), or every level on one warp per node (2^30): the
     enumeration schedule changes speed, never results."""
     c = C.Context()
     try:
