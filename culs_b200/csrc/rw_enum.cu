@@ -462,7 +462,7 @@ __device__ __forceinline__ void lane_node_step(const EnumArgs &A, LaneNode &N) {
     if (m.n < 2) N.pairs = 0;  // enumeration of this node stops (rewrite.cu:291)
 }
 
-// Writes the lane's node's 8 slots (published with the rest of its chunk).
+// Writes the lane's node's 8 slots and publishes it.
 __device__ __forceinline__ void lane_node_end(const EnumArgs &A, const LaneNode &N) {
     const int64_t q = N.q;
 #pragma unroll
@@ -470,6 +470,8 @@ __device__ __forceinline__ void lane_node_end(const EnumArgs &A, const LaneNode 
         A.cutL[q * 8 + k] = make_int4(N.S[k].l[0], N.S[k].l[1], N.S[k].l[2], N.S[k].l[3]);
         A.cutM[q * 8 + k] = make_int2((int)N.S[k].sign, (int)N.S[k].pk);
     }
+    __threadfence();
+    st_release(&A.done[q], 1);
 }
 
 // The nodes [base, base + cnt) of one wide level, one node per lane at a
@@ -478,8 +480,7 @@ __device__ __forceinline__ void lane_node_end(const EnumArgs &A, const LaneNode 
 // node, so lanes stay busy while the chunk lasts instead of idling until
 // the warp's busiest node is done (admissible pairs per node vary about
 // twofold within a warp).  Nodes of one level never read each other, so a
-// lane never waits on another lane of its warp, and the chunk's nodes are
-// published together when it is done.
+// lane never waits on another lane of its warp.
 __device__ __forceinline__ void enum_chunk_thread(const EnumArgs &A, int64_t base, int cnt, int lane) {
     const unsigned F = 0xffffffffu;
     LaneNode N;
@@ -504,12 +505,6 @@ __device__ __forceinline__ void enum_chunk_thread(const EnumArgs &A, int64_t bas
         if (active && N.pairs) lane_node_step(A, N);
         __syncwarp();
     }
-    // one fence for the whole chunk, then its nodes are published: nodes
-    // of the next levels read them only after their flag, and a fence per
-    // finishing round would stall the warp once per distinct pair count
-    __threadfence();
-    __syncwarp();
-    for (int i = lane; i < cnt; i += 32) st_release(&A.done[base + i], 1);
 }
 
 // Levels are cut into chunks that never cross a level: a wide level into
