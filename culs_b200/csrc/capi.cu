@@ -403,10 +403,6 @@ int culs_set_param(culs_ctx *ctx, int which, int64_t value) {
                 if (value < 1 || value > 64) return CULS_E_INVALID;
                 t.enumBlocksPerSm = (int)value;
                 return CULS_OK;
-            case CULS_PARAM_ENUM_CHUNK_NODES:
-                if (value < 32 || value > 1024 || value % 32) return CULS_E_INVALID;
-                t.enumChunkNodes = (int)value;
-                return CULS_OK;
             default:
                 return CULS_E_INVALID;
         }
@@ -421,7 +417,6 @@ int culs_get_param(culs_ctx *ctx, int which, int64_t *value) {
         switch (which) {
             case CULS_PARAM_ENUM_WIDE_MIN: *value = t.enumWideMin; return CULS_OK;
             case CULS_PARAM_ENUM_BLOCKS_PER_SM: *value = t.enumBlocksPerSm; return CULS_OK;
-            case CULS_PARAM_ENUM_CHUNK_NODES: *value = t.enumChunkNodes; return CULS_OK;
             default: return CULS_E_INVALID;
         }
     });

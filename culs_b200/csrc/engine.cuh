@@ -30,7 +30,6 @@ struct ExecCtx;
 struct Tune {
     int enumWideMin = 16384;   // levels this wide run one node per thread, narrower one per warp
     int enumBlocksPerSm = 8;   // persistent enumeration blocks per SM
-    int enumChunkNodes = 128;  // nodes per chunk of a one-node-per-thread level (a multiple of 32)
 };
 
 struct DevGraph {

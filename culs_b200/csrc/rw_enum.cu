@@ -26,7 +26,6 @@ struct EnumArgs {
     const int *chunkStart;  // first chunk of each level; maxLevel + 2 entries
     int maxLevel;
     int wideMin;            // levels at least this wide run thread-per-node
-    int chunkNodes;         // nodes per chunk of such a level (a multiple of 32)
     const int *w0, *w1;
     const int *ref;
     const uint8_t *lidLow;
@@ -337,174 +336,136 @@ __device__ __forceinline__ void enum_node_warp(const EnumArgs &A, int64_t q, int
     if (lane == 0) st_release(&A.done[q], 1);
 }
 
-// One node per lane on wide levels.  A lane's node: its 8 slots in
-// registers (the trivial cut in slot 0), its fanins and the mask of the
-// fanin-cut pairs CutEnumerate tries (both slots used, at most 4 leaves by
-// signature), bit i * 8 + j: visiting the set bits in order is the
-// reference's i-major loop.
-struct LaneNode {
+// One node on one thread (wide levels): the slots in registers, the
+// admissible pairs visited in order.  All lanes of the warp call it (valid:
+// the lane has a node) and run as many rounds as the lane with the most
+// admissible pairs, one pair per round and back in step after each, so
+// lanes that finish a pair early do not drift into later pairs alone.
+__device__ __forceinline__ void enum_node_thread(const EnumArgs &A, int64_t q, bool valid) {
     Slot S[8];
-    uint64_t pairs;
-    int64_t q;
-    int u0, u1, c0, c1;
-};
-
-// Starts node q on this lane: slot 0 the trivial cut, the other slots
-// free; waits (bounded) for both fanins and builds the pair mask.  A failed
-// wait leaves the mask empty, so the node publishes its trivial cut alone
-// (the call then reports the status word's error).
-__device__ __forceinline__ void lane_node_begin(const EnumArgs &A, int64_t q, LaneNode &N) {
 #pragma unroll
     for (int k = 0; k < 8; k++) {
-        N.S[k].pk = 0;
-        N.S[k].sign = 0;
-        N.S[k].l[0] = N.S[k].l[1] = N.S[k].l[2] = N.S[k].l[3] = 0;
+        S[k].pk = 0;
+        S[k].sign = 0;
+        S[k].l[0] = S[k].l[1] = S[k].l[2] = S[k].l[3] = 0;
     }
-    N.q = q;
-    Cut c;
-    c.sign = 1u << A.lidLow[q];
-    c.tt = 0xAAAAu;
-    c.nLeaves = 1;
-    c.used = 1;
-    c.value = 1001u;
-    N.S[0].l[0] = (int)q;
-    N.S[0].sign = c.sign;
-    N.S[0].pk = cut_pack(c);
-    A.cutA[q * 8] = make_int2((int)clamp_ref(A.ref[q]), (int)((uint32_t)A.lidLow[q] << 12));
-    const int f0 = A.w0[q], f1 = A.w1[q];
-    N.u0 = f0 >> 1;
-    N.u1 = f1 >> 1;
-    N.c0 = f0 & 1;
-    N.c1 = f1 & 1;
-    N.pairs = 0;
-    if (!wait_ge(&A.done[N.u0], 1, A.status) || !wait_ge(&A.done[N.u1], 1, A.status)) return;
-    const int2 *M0 = A.cutM + (int64_t)N.u0 * 8, *M1 = A.cutM + (int64_t)N.u1 * 8;
-    uint32_t s1[8], used1 = 0;
-#pragma unroll
-    for (int j = 0; j < 8; j++) {
-        const int2 mj = M1[j];
-        s1[j] = (uint32_t)mj.x;
-        used1 |= packed_used((uint32_t)mj.y) << j;
+    if (valid) {
+        Cut c;
+        c.sign = 1u << A.lidLow[q];
+        c.tt = 0xAAAAu;
+        c.nLeaves = 1;
+        c.used = 1;
+        c.value = 1001u;
+        S[0].l[0] = (int)q;
+        S[0].sign = c.sign;
+        S[0].pk = cut_pack(c);
+        A.cutA[q * 8] = make_int2((int)clamp_ref(A.ref[q]), (int)((uint32_t)A.lidLow[q] << 12));
     }
+    const int f0 = valid ? A.w0[q] : 0, f1 = valid ? A.w1[q] : 0;
+    const int u0 = f0 >> 1, u1 = f1 >> 1, c0 = f0 & 1, c1 = f1 & 1;
+    bool ok = valid && wait_ge(&A.done[u0], 1, A.status) && wait_ge(&A.done[u1], 1, A.status);
+    uint64_t pairs = 0;
+    const int2 *M0 = A.cutM + (int64_t)u0 * 8, *M1 = A.cutM + (int64_t)u1 * 8;
+    if (ok) {
+        // the pairs CutEnumerate tries (both slots used, at most 4 leaves
+        // by signature), bit i * 8 + j: visiting the set bits in order is
+        // the reference's i-major loop, and every lane takes its k-th pair
+        // in the same iteration
+        {
+            uint32_t s1[8], used1 = 0;
 #pragma unroll
-    for (int i = 0; i < 8; i++) {
-        const int2 mi = M0[i];
-        if (!packed_used((uint32_t)mi.y)) continue;
+            for (int j = 0; j < 8; j++) {
+                const int2 mj = M1[j];
+                s1[j] = (uint32_t)mj.x;
+                used1 |= packed_used((uint32_t)mj.y) << j;
+            }
 #pragma unroll
-        for (int j = 0; j < 8; j++)
-            if (((used1 >> j) & 1u) && popc32((uint32_t)mi.x | s1[j]) <= 4) N.pairs |= 1ull << (i * 8 + j);
-    }
-}
-
-// The next admissible pair of the lane's node: CutEnumerate's body for one
-// (i, j) -- FindCut, merge, CutFilter, truth table, MinimizeCutSupport,
-// CutFilter again, CutFindValue (rewrite.cu:268-294).
-__device__ __forceinline__ void lane_node_step(const EnumArgs &A, LaneNode &N) {
-    Slot(&S)[8] = N.S;
-    const int p = __ffsll((long long)N.pairs) - 1;
-    N.pairs &= N.pairs - 1;
-    const int i = p >> 3, j = p & 7;
-    const int64_t q = N.q;
-    RCut a, b;
-    load_rcut(A, (int64_t)N.u0 * 8 + i, A.cutM[(int64_t)N.u0 * 8 + i], a);
-    load_rcut(A, (int64_t)N.u1 * 8 + j, A.cutM[(int64_t)N.u1 * 8 + j], b);
-    // FindCut: first unused slot, else lowest value among >2-leaf, then
-    // 2-leaf, then smaller cuts (rewrite.cu:84-109)
-    int id = -1;
+            for (int i = 0; i < 8; i++) {
+                const int2 mi = M0[i];
+                if (!packed_used((uint32_t)mi.y)) continue;
 #pragma unroll
-    for (int k = 0; k < 8; k++)
-        if (id < 0 && !sl_used(S[k])) id = k;
-    if (id < 0) {
-        uint32_t best = 0xFFFFFFFFu;
-#pragma unroll
-        for (int k = 0; k < 8; k++) {
-            uint32_t n = sl_n(S[k]);
-            uint32_t cls = n > 2 ? 0u : (n == 2 ? 1u : 2u);
-            uint32_t key = (cls << 20) | (sl_value(S[k]) << 3) | (uint32_t)k;
-            best = key < best ? key : best;
+                for (int j = 0; j < 8; j++)
+                    if (((used1 >> j) & 1u) && popc32((uint32_t)mi.x | s1[j]) <= 4)
+                        pairs |= 1ull << (i * 8 + j);
+            }
         }
-        id = (int)(best & 7u);
     }
+    // every lane runs the warp's largest number of admissible pairs, in step;
+    // `continue` in the do-while below ends the lane's current pair
+    const int rounds = __reduce_max_sync(0xffffffffu, (unsigned)popc64(pairs));
+    for (int t = 0; t < rounds; t++) {
+        if (pairs) {
+            const int p = __ffsll((long long)pairs) - 1;
+            pairs &= pairs - 1;
+            const int i = p >> 3, j = p & 7;
+            do {
+                RCut a, b;
+                load_rcut(A, (int64_t)u0 * 8 + i, M0[i], a);
+                load_rcut(A, (int64_t)u1 * 8 + j, M1[j], b);
+                // FindCut: first unused slot, else lowest value among
+                // >2-leaf, then 2-leaf, then smaller cuts (rewrite.cu:84-109)
+                int id = -1;
 #pragma unroll
-    for (int k = 0; k < 8; k++)
-        if (k == id) sl_clear_used(S[k]);
-    RCut m;
-    if (!rc_merge(a, b, m)) return;
-    if (filter_slots(S, id, m.l, m.n, m.sign)) return;  // dropped: the slot stays free
-    m.tt = rc_truth(m, a, b, N.c0, N.c1);
-    const bool mini = rc_minimize(m);
-    m.value = 0;
-    Cut pc;
-    pc.tt = m.tt;
-    pc.nLeaves = m.n;
-    pc.used = 1;
-    pc.value = 0;
-    uint32_t a0, a1;
-    rc_pack_aux(m, a0, a1);
-    A.cutA[q * 8 + id] = make_int2((int)a0, (int)a1);
+                for (int k = 0; k < 8; k++)
+                    if (id < 0 && !sl_used(S[k])) id = k;
+                if (id < 0) {
+                    uint32_t best = 0xFFFFFFFFu;
 #pragma unroll
-    for (int k = 0; k < 8; k++)
-        if (k == id) {
-            S[k].l[0] = m.l[0];
-            S[k].l[1] = m.l[1];
-            S[k].l[2] = m.l[2];
-            S[k].l[3] = m.l[3];
-            S[k].sign = m.sign;
-            S[k].pk = cut_pack(pc);
+                    for (int k = 0; k < 8; k++) {
+                        uint32_t n = sl_n(S[k]);
+                        uint32_t cls = n > 2 ? 0u : (n == 2 ? 1u : 2u);
+                        uint32_t key = (cls << 20) | (sl_value(S[k]) << 3) | (uint32_t)k;
+                        best = key < best ? key : best;
+                    }
+                    id = (int)(best & 7u);
+                }
+#pragma unroll
+                for (int k = 0; k < 8; k++)
+                    if (k == id) sl_clear_used(S[k]);
+                RCut m;
+                if (!rc_merge(a, b, m)) continue;
+                if (filter_slots(S, id, m.l, m.n, m.sign)) continue;  // dropped: slot stays free
+                m.tt = rc_truth(m, a, b, c0, c1);
+                const bool mini = rc_minimize(m);
+                m.value = 0;
+                Cut pc;
+                pc.tt = m.tt;
+                pc.nLeaves = m.n;
+                pc.used = 1;
+                pc.value = 0;
+                uint32_t a0, a1;
+                rc_pack_aux(m, a0, a1);
+                A.cutA[q * 8 + id] = make_int2((int)a0, (int)a1);
+#pragma unroll
+                for (int k = 0; k < 8; k++)
+                    if (k == id) {
+                        S[k].l[0] = m.l[0];
+                        S[k].l[1] = m.l[1];
+                        S[k].l[2] = m.l[2];
+                        S[k].l[3] = m.l[3];
+                        S[k].sign = m.sign;
+                        S[k].pk = cut_pack(pc);
+                    }
+                bool keep = true;
+                if (mini) keep = !filter_slots(S, id, m.l, m.n, m.sign);
+                pc.value = rc_value(m);
+                pc.used = keep ? 1u : 0u;
+#pragma unroll
+                for (int k = 0; k < 8; k++)
+                    if (k == id) S[k].pk = cut_pack(pc);
+                if (m.n < 2) pairs = 0;  // enumeration of this node stops (rewrite.cu:291)
+            } while (false);
         }
-    bool keep = true;
-    if (mini) keep = !filter_slots(S, id, m.l, m.n, m.sign);
-    pc.value = rc_value(m);
-    pc.used = keep ? 1u : 0u;
-#pragma unroll
-    for (int k = 0; k < 8; k++)
-        if (k == id) S[k].pk = cut_pack(pc);
-    if (m.n < 2) N.pairs = 0;  // enumeration of this node stops (rewrite.cu:291)
-}
-
-// Writes the lane's node's 8 slots and publishes it.
-__device__ __forceinline__ void lane_node_end(const EnumArgs &A, const LaneNode &N) {
-    const int64_t q = N.q;
+        __syncwarp();
+    }
+    if (!valid) return;
 #pragma unroll
     for (int k = 0; k < 8; k++) {
-        A.cutL[q * 8 + k] = make_int4(N.S[k].l[0], N.S[k].l[1], N.S[k].l[2], N.S[k].l[3]);
-        A.cutM[q * 8 + k] = make_int2((int)N.S[k].sign, (int)N.S[k].pk);
+        A.cutL[q * 8 + k] = make_int4(S[k].l[0], S[k].l[1], S[k].l[2], S[k].l[3]);
+        A.cutM[q * 8 + k] = make_int2((int)S[k].sign, (int)S[k].pk);
     }
     __threadfence();
     st_release(&A.done[q], 1);
-}
-
-// The nodes [base, base + cnt) of one wide level, one node per lane at a
-// time.  Every round each lane with a node replays one admissible pair; a
-// lane whose node has no pair left publishes it and takes the chunk's next
-// node, so lanes stay busy while the chunk lasts instead of idling until
-// the warp's busiest node is done (admissible pairs per node vary about
-// twofold within a warp).  Nodes of one level never read each other, so a
-// lane never waits on another lane of its warp.
-__device__ __forceinline__ void enum_chunk_thread(const EnumArgs &A, int64_t base, int cnt, int lane) {
-    const unsigned F = 0xffffffffu;
-    LaneNode N;
-    bool active = lane < cnt;
-    if (active) lane_node_begin(A, base + lane, N);
-    int next = 32;  // the chunk's next unclaimed node, the same on every lane
-    while (true) {
-        if (active && !N.pairs) {
-            lane_node_end(A, N);
-            active = false;
-        }
-        const unsigned need = __ballot_sync(F, !active);
-        if (need && next < cnt) {
-            const int idx = next + __popc(need & ((1u << lane) - 1u));
-            if (!active && idx < cnt) {
-                lane_node_begin(A, base + idx, N);
-                active = true;
-            }
-            next += __popc(need);
-        }
-        if (!__any_sync(F, active)) break;
-        if (active && N.pairs) lane_node_step(A, N);
-        __syncwarp();
-    }
 }
 
 // Levels are cut into chunks that never cross a level: a wide level into
@@ -533,9 +494,8 @@ __global__ void __launch_bounds__(kEnumBlock, 3) k_enumerate(EnumArgs A) {
         const int64_t base = A.nL0 + A.lvlStart[lo];
         const int64_t k = c - A.chunkStart[lo];
         if (w >= A.wideMin) {
-            const int64_t first = k * A.chunkNodes;
-            const int cnt = (int)(w - first < A.chunkNodes ? w - first : A.chunkNodes);
-            enum_chunk_thread(A, base + first, cnt, lane);
+            const int64_t q = base + k * 32 + lane;
+            enum_node_thread(A, q, q < base + w);
         } else {
             enum_node_warp(A, base + k, lane);
         }
@@ -548,11 +508,11 @@ __global__ void k_level_count(int64_t nL0, int64_t N, const int *wlev, int *lvlC
         agg_add(lvlCnt, wlev[q], 1);
 }
 
-__global__ void k_level_chunks(int n, const int *lvlCnt, int wideMin, int chunkNodes, int *cc) {
+__global__ void k_level_chunks(int n, const int *lvlCnt, int wideMin, int *cc) {
     int stride = gridDim.x * blockDim.x;
     for (int l = blockIdx.x * blockDim.x + threadIdx.x; l < n; l += stride) {
         const int w = lvlCnt[l];
-        cc[l] = w >= wideMin ? (w + chunkNodes - 1) / chunkNodes : w;
+        cc[l] = w >= wideMin ? (w + 31) / 32 : w;
     }
 }
 
@@ -579,15 +539,13 @@ int rw_enumerate(ExecCtx &X, RwWork &w) {
     if (!lvlCnt || !lvlStart || !cc || !chunkStart) return X.fail(CULS_E_OOM, "rw: scratch arena exhausted (levels)");
     if ((rc = X.check(cudaMemsetAsync(lvlCnt, 0, sizeof(int) * L, s), "memset"))) return rc;
     k_level_count<<<X.grid(N - w.nL0), kBlock, 0, s>>>(w.nL0, N, w.wlev, lvlCnt);
-    k_level_chunks<<<grid_1d(L, kBlock, X.sms * 16), kBlock, 0, s>>>(L - 1, lvlCnt, X.tune->enumWideMin,
-                                                                   X.tune->enumChunkNodes, cc);
+    k_level_chunks<<<grid_1d(L, kBlock, X.sms * 16), kBlock, 0, s>>>(L - 1, lvlCnt, X.tune->enumWideMin, cc);
     if ((rc = X.check(scan_exclusive(lvlCnt, lvlStart, L - 1, nullptr, *X.ar, s), "scan"))) return rc;
     if ((rc = X.check(scan_exclusive(cc, chunkStart, L - 1, chunkStart + L - 1, *X.ar, s), "scan"))) return rc;
     k_enum_init<<<X.grid(N), kBlock, 0, s>>>(N, w.wlev, w.wl, w.lidLow, w.ref, w.cutL, w.cutM, cutA, done);
     // lvlStart counts AND nodes only: the AND positions of W start at nL0
-    EnumArgs A{w.nL0,     N,       lvlCnt,  lvlStart, chunkStart, w.maxLevel,  X.tune->enumWideMin,
-               X.tune->enumChunkNodes, w.w0, w.w1, w.ref, w.lidLow, w.cutL, w.cutM, cutA, done,
-               X.counters, w.warpPairs, X.status};
+    EnumArgs A{w.nL0, N,       lvlCnt, lvlStart, chunkStart, w.maxLevel, X.tune->enumWideMin, w.w0, w.w1,
+               w.ref, w.lidLow, w.cutL, w.cutM, cutA,       done,       X.counters, w.warpPairs, X.status};
     X.mark(kMkEnumK0);
     k_enumerate<<<(unsigned)(X.sms * X.tune->enumBlocksPerSm), kEnumBlock, 0, s>>>(A);
     X.mark(kMkEnumK1);

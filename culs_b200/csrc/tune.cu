@@ -6,8 +6,7 @@
 // workload's level widths and depths, so it is chosen by timing rw's cut
 // enumeration (device events around the kernel) on clones of a sample of
 // the workload: first the width threshold at the default grid, then the
-// grid at the chosen threshold, then the chunk a warp takes from a
-// one-node-per-thread level.
+// grid at the chosen threshold.
 #include <cfloat>
 
 #include "engine.cuh"
@@ -60,18 +59,6 @@ int Engine::autotune(const Batch &sample, int rounds) {
         if (rc) break;
         Tune t = best;
         t.enumBlocksPerSm = b;
-        float ms;
-        if ((rc = measure(t, ms))) break;
-        if (ms < bestMs) {
-            bestMs = ms;
-            best = t;
-        }
-    }
-    const int chunks[] = {32, 64, 128, 256};
-    for (int c : chunks) {
-        if (rc) break;
-        Tune t = best;
-        t.enumChunkNodes = c;
         float ms;
         if ((rc = measure(t, ms))) break;
         if (ms < bestMs) {

@@ -209,14 +209,11 @@ int culs_fetch_aiger(culs_ctx *ctx, int64_t job, uint8_t *buf, size_t cap, size_
  * CULS_PARAM_ENUM_WIDE_MIN: cut-enumeration levels with at least this many
  * AND nodes run one node per thread, narrower ones one node per warp
  * (default 16384).  CULS_PARAM_ENUM_BLOCKS_PER_SM: persistent enumeration
- * blocks per SM (default 8).  CULS_PARAM_ENUM_CHUNK_NODES: AND nodes a warp
- * takes at a time from a one-node-per-thread level, a multiple of 32 from 32
- * to 1024 (default 128).  culs_autotune times rw's enumeration on
+ * blocks per SM (default 8).  culs_autotune times rw's enumeration on
  * clones of `sample` (left unchanged) for candidate values, `rounds` times
  * each, and keeps the fastest in the context.  No reference counterpart. */
 #define CULS_PARAM_ENUM_WIDE_MIN 1
 #define CULS_PARAM_ENUM_BLOCKS_PER_SM 2
-#define CULS_PARAM_ENUM_CHUNK_NODES 3
 int culs_set_param(culs_ctx *ctx, int which, int64_t value);
 int culs_get_param(culs_ctx *ctx, int which, int64_t *value);
 int culs_autotune(culs_ctx *ctx, const culs_graph *sample, int rounds);
