@@ -10,10 +10,12 @@ A step is one `rw; st` over the workload's graphs:
   c3  one 10M-AND layered AIG, 4,096 PIs/POs, 2,000 layers, 80% window-3 /
       20% far fanins
   c2  64x64 array multiplier; c1  5,000-AND 40-layer AIG (parity cases)
-  c5  served mode: Poisson arrivals (--load x measured capacity) of jobs
-      drawn from 64 c4-family graphs of 500-2M ANDs and 64 n x n
-      multipliers (n 8-128), submitted one by one through culs_submit;
-      reports throughput and p50/p99 submit-to-done latency
+  c5  served mode: Poisson arrivals (0.25, 0.5, 0.75 and --load x measured
+      batch capacity; --jobs jobs per run, --repeats runs per load) of jobs
+      drawn from 512 c4-family graphs of 500-2M ANDs and 512 n x n
+      multipliers (n 8-128), submitted one by one through culs_submit under
+      a 150 GB admission budget; reports throughput and p50/p99
+      submit-to-done latency (the default c4 line carries a short run)
 `value` times device-resident steps (a device clone of the input, rw, st);
 `e2e` times the public C-ABI path from host arrays: upload, rw, st,
 download; `e2e_aiger` the same from binary AIGER files' bytes to files'
@@ -302,10 +304,10 @@ def plain_path(ctx, graphs, budget_s=8.0, e2e=False):
                       (", upload + rw;st + download, wall clock" if e2e else ", device-resident, CUDA events")}
 
 
-def served_pool(seed=5, count=128, gen=None):
+def served_pool(seed=5, count=1024, gen=None):
     """Job pool of the served workload: half seeded c4-family graphs with AND
     counts log-uniform in 500-2M, half n x n array multipliers, n uniform in
-    8-128."""
+    8-128.  Jobs are drawn from the pool with repetition."""
     if gen is None:
         import culs_b200 as gen
     rng = np.random.default_rng(seed)
@@ -314,23 +316,16 @@ def served_pool(seed=5, count=128, gen=None):
     return pool
 
 
-def served_arm(args, group):
-    """Served mode: jobs drawn from the pool arrive as a Poisson process at a
-    fraction of the measured batch capacity; each is submitted through the C
-    ABI (culs_submit), waited for and fetched on another thread.  Reports
-    throughput and submit-to-done latency percentiles (wall clock, the
-    latency a caller sees) at --load, and the same at 0.25 and 0.5 of
-    capacity in `load_sweep`."""
-    import threading
-    import culs_b200 as C
-    ctx = C.Context(device=group.local)
-    pool = served_pool()
-    # capacity: the whole pool as one batch (upload, rw;st, download from
-    # host arrays), after one untimed pass, the median of three.  (A burst
-    # through the served path is not a stable yardstick: how many jobs the
-    # first worker finds queued depends on thread timing.)
+SERVE_BUDGET = 150 * 10**9  # the served workload's HBM admission budget, bytes
+
+
+def served_capacity(ctx, pool, runs=3):
+    """Jobs per second when the whole pool runs as one batch from host arrays
+    (upload, rw;st, download), median of `runs` after one untimed pass.  (A
+    burst through the served path is not a stable yardstick: how many jobs a
+    free worker finds queued depends on thread timing.)"""
     caps = []
-    for r in range(4):
+    for r in range(runs + 1):
         t0 = time.perf_counter()
         d = ctx.upload_batch(pool)
         ctx.rw_st(d)
@@ -338,77 +333,108 @@ def served_arm(args, group):
         d.free()
         if r:
             caps.append(len(pool) / (time.perf_counter() - t0))
-    cap_jobs_s = float(np.median(caps))
-    ctx.serve_start(workers=args.workers)
-    njobs = max(args.steps, 1) * 400
+    return float(np.median(caps)), caps
 
-    def run_load(load, seed):
-        """Poisson arrivals at load x capacity; returns (AND nodes/s, sorted
-        latencies in ms, job picks)."""
-        rng = np.random.default_rng(seed)
-        rate = load * cap_jobs_s
-        picks = rng.integers(0, len(pool), njobs)
-        gaps = rng.exponential(1.0 / rate, njobs)
-        lat, nodes, done_t = [], [0], [0.0]
-        q = []
-        cv = threading.Condition()
 
-        def collector():
-            for k in range(njobs):
-                with cv:
-                    while len(q) <= k:
-                        cv.wait()
-                    j = q[k]
-                ctx.wait(j)
-                out, ms = ctx.fetch(j)
-                lat.append(ms)
-                nodes[0] += pool[picks[k]].nAnds
-            done_t[0] = time.perf_counter()
+def served_load(ctx, pool, rate, njobs, seed):
+    """Poisson arrivals at `rate` jobs/s of `njobs` jobs drawn from the pool,
+    each submitted through the C ABI (culs_submit) on this thread, waited for
+    and fetched on another.  Returns (AND nodes/s from the first submission
+    to the last fetch, sorted submit-to-done latencies in ms, picks)."""
+    import threading
+    rng = np.random.default_rng(seed)
+    picks = rng.integers(0, len(pool), njobs)
+    gaps = rng.exponential(1.0 / rate, njobs)
+    lat, nodes, done_t = [], [0], [0.0]
+    q = []
+    cv = threading.Condition()
 
-        th = threading.Thread(target=collector)
-        th.start()
-        t0 = time.perf_counter()
-        due = t0
+    def collector():
         for k in range(njobs):
-            due += gaps[k]
-            d = due - time.perf_counter()
-            if d > 0:
-                time.sleep(d)
-            j = ctx.submit(pool[picks[k]])
             with cv:
-                q.append(j)
-                cv.notify()
-        th.join()
-        return nodes[0] / (done_t[0] - t0), np.sort(np.array(lat)), picks
+                while len(q) <= k:
+                    cv.wait()
+                j = q[k]
+            ctx.wait(j)
+            out, ms = ctx.fetch(j)
+            lat.append(ms)
+            nodes[0] += pool[picks[k]].nAnds
+        done_t[0] = time.perf_counter()
 
+    th = threading.Thread(target=collector)
+    th.start()
+    t0 = time.perf_counter()
+    due = t0
+    for k in range(njobs):
+        due += gaps[k]
+        d = due - time.perf_counter()
+        if d > 0:
+            time.sleep(d)
+        j = ctx.submit(pool[picks[k]])
+        with cv:
+            q.append(j)
+            cv.notify()
+    th.join()
+    return nodes[0] / (done_t[0] - t0), np.sort(np.array(lat)), picks
+
+
+def served_session(ctx, pool, loads, njobs, repeats, workers, budget=SERVE_BUDGET, seed=5):
+    """Served mode at each offered load (a fraction of the batch capacity),
+    `repeats` runs of `njobs` jobs each: the median and the range of p50,
+    p99 and throughput per load."""
+    cap, caps = served_capacity(ctx, pool)
+    ctx.serve_start(admit_bytes=budget, workers=workers)
     sweep = []
-    for i, load in enumerate(sorted(set([0.25, 0.5, args.load]))):
-        v, lt, pk = run_load(load, 5 + i)
-        sweep.append({"load_vs_capacity": load, "offered_jobs_per_s": load * cap_jobs_s, "value": v,
-                      "p50_ms": float(np.percentile(lt, 50)), "p99_ms": float(np.percentile(lt, 99))})
-        if load == args.load:
-            value, lat, picks = v, lt, pk
-    rate = args.load * cap_jobs_s
-    ctx.serve_stop()
-    plain = plain_path(ctx, [pool[i] for i in picks], budget_s=8.0, e2e=True)
-    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+    try:
+        for i, load in enumerate(loads):
+            runs = []
+            for r in range(repeats):
+                v, lt, _ = served_load(ctx, pool, load * cap, njobs, seed + 100 * i + r)
+                runs.append({"value": v, "p50_ms": float(np.percentile(lt, 50)),
+                             "p99_ms": float(np.percentile(lt, 99)), "mean_ms": float(lt.mean()),
+                             "max_ms": float(lt[-1])})
+            med = {k: float(np.median([x[k] for x in runs])) for k in ("value", "p50_ms", "p99_ms")}
+            sweep.append({"load_vs_capacity": load, "offered_jobs_per_s": load * cap, "jobs": njobs,
+                          "repeats": repeats, **med,
+                          "p50_range_ms": [min(x["p50_ms"] for x in runs), max(x["p50_ms"] for x in runs)],
+                          "p99_range_ms": [min(x["p99_ms"] for x in runs), max(x["p99_ms"] for x in runs)],
+                          "runs": runs})
+    finally:
+        ctx.serve_stop()
+    return {"capacity_jobs_per_s": cap, "capacity_runs": caps, "budget_bytes": budget, "workers": workers,
+            "pool_graphs": len(pool), "pool_and_nodes": int(sum(g.nAnds for g in pool)), "sweep": sweep,
+            "timing": "wall clock, submit to done"}
+
+
+def served_arm(args, group):
+    """Served mode (`--workload c5`): jobs drawn from the 1,024-graph pool
+    arrive as a Poisson process at 0.25, 0.5 and 0.75 of the measured batch
+    capacity (and --load), `--jobs` jobs per run, `--repeats` runs per load,
+    under the 150 GB admission budget; reports throughput and p50/p99
+    submit-to-done latency per load, and the plain one-at-a-time path on the
+    same jobs."""
+    import culs_b200 as C
+    ctx = C.Context(device=group.local)
+    pool = served_pool()
+    loads = sorted(set([0.25, 0.5, 0.75, args.load]))
+    srv = served_session(ctx, pool, loads, args.jobs, args.repeats, args.workers)
+    at = [x for x in srv["sweep"] if x["load_vs_capacity"] == args.load][0]
+    rng = np.random.default_rng(5)
+    plain = plain_path(ctx, [pool[i] for i in rng.integers(0, len(pool), 400)], budget_s=8.0, e2e=True)
+    line = {"metric": METRIC, "value": at["value"], "unit": UNIT, "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "int32",
             "data": "synthetic (seeded generators; CULS ships no benchmark inputs)",
-            "config": {"workload": WORKLOAD_DESC["c5"], "jobs": njobs, "pool_graphs": len(pool),
-                       "offered_jobs_per_s": rate, "load_vs_capacity": args.load,
-                       "capacity_jobs_per_s": cap_jobs_s, "capacity_runs": caps,
-                       "timing": "wall clock, submit to fetch",
-                       "parallelism": f"single GPU, dynamic batching, {args.workers} batches at once"},
-            "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
-                           "mean": float(lat.mean()), "max": float(lat[-1])},
-            "plain_single_graph_path": plain,
-            "served_vs_plain": value / plain["value"] if plain["value"] else None,
-            "load_sweep": sweep,
-            "e2e": {"value": value, "unit": UNIT,
-                    "h2d_bytes_per_step": None, "d2h_bytes_per_step": None},
+            "config": {"workload": WORKLOAD_DESC["c5"], "jobs_per_run": args.jobs, "pool_graphs": len(pool),
+                       "load_vs_capacity": args.load, "budget_bytes": SERVE_BUDGET,
+                       "parallelism": f"single GPU, {args.workers} workers, continuous admission"},
+            "latency_ms": {"p50": at["p50_ms"], "p99": at["p99_ms"]},
+            "served": srv, "plain_single_graph_path": plain,
+            "served_vs_plain": at["value"] / plain["value"] if plain["value"] else None,
+            "e2e": {"value": at["value"], "unit": UNIT, "h2d_bytes_per_step": None, "d2h_bytes_per_step": None},
             "gpu_launches": ctx.kernel_launches()}
     print(json.dumps(line), flush=True)
+    ctx.close()
     return 0
 
 
@@ -590,16 +616,30 @@ def our_arm(args, group):
         par = parity_digest(dw, args.workload)
     line["parity"] = par
     bad = group.sum(par["mismatches"] if par else 0)
+    dw.free()
+    d0.free()
     if group.rank == 0:
         if group.world == 1 and len(graphs) > 1:
             plain = plain_path(ctx, graphs)
             line["plain_single_graph_path"] = plain
             line["batched_vs_plain"] = value / plain["value"] if plain["value"] else None
             line["single_graph_c2"] = single_graph_c2(ctx)
+            if not args.no_served and args.workload == "c4":
+                # a short served-mode run (the c5 workload's job mix, 256
+                # pool graphs, 2,000 jobs at half the batch capacity, one
+                # run) so the default line carries p50/p99 latency
+                pool = served_pool(count=256)
+                srv = served_session(ctx, pool, [0.5], 2000, 1, args.workers)
+                x = srv["sweep"][0]
+                line["served"] = {"workload": WORKLOAD_DESC["c5"], "pool_graphs": len(pool), "jobs": x["jobs"],
+                                  "load_vs_capacity": 0.5, "offered_jobs_per_s": x["offered_jobs_per_s"],
+                                  "value": x["value"], "unit": UNIT, "p50_ms": x["p50_ms"], "p99_ms": x["p99_ms"],
+                                  "budget_bytes": srv["budget_bytes"], "workers": srv["workers"],
+                                  "capacity_jobs_per_s": srv["capacity_jobs_per_s"],
+                                  "timing": srv["timing"]}
+                del pool
         line["cpu_baseline"] = cpu_baseline(args.workload, graphs) if group.world == 1 else None
         print(json.dumps(line), flush=True)
-    dw.free()
-    d0.free()
     ctx.close()
     return 1 if bad else 0
 
@@ -612,7 +652,11 @@ def main():
     ap.add_argument("--workload", default="c4", choices=["c4", "c4m", "c3", "c3m", "c2", "c1", "c5"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--load", type=float, default=0.75, help="c5: offered load as a fraction of measured capacity")
-    ap.add_argument("--workers", type=int, default=2, help="c5: batches the served mode runs at once")
+    ap.add_argument("--workers", type=int, default=4, help="c5: batches the served mode runs at once")
+    ap.add_argument("--jobs", type=int, default=20000, help="c5: jobs per run")
+    ap.add_argument("--repeats", type=int, default=3, help="c5: runs per offered load")
+    ap.add_argument("--no-served", action="store_true",
+                    help="c4: leave out the short served-mode run of the default line")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

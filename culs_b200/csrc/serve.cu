@@ -211,10 +211,15 @@ void Server::worker(Engine &eng, std::mutex &engMu) {
             std::unique_lock<std::mutex> lk(mu_);
             cvWork_.wait(lk, [&] { return stop_ || !queue_.empty(); });
             if (queue_.empty()) return;  // stop requested and nothing left
-            // admission: arrival order, the head's flags, within the budget
-            // (the head is always admitted; the engine refuses it if it alone
-            // exceeds the context's budget)
+            // admission: arrival order, the head's flags and size class,
+            // within the budget (the head is always admitted; the engine
+            // refuses it if it alone exceeds the context's budget).  A batch
+            // lasts as long as its deepest graph, and depth grows with size,
+            // so a batch takes only jobs within kSizeRatio of the head's AND
+            // count: small jobs then do not wait on a large one's critical
+            // path, and the jobs left in the queue go to the next free worker.
             const ServeJob *head = jobs_[queue_.front()].get();
+            const int64_t hs = 1 + (int64_t)head->nAnds;
             size_t bytes = 0;
             std::deque<int64_t> rest;
             while (!queue_.empty()) {
@@ -223,7 +228,10 @@ void Server::worker(Engine &eng, std::mutex &engMu) {
                 ServeJob *j = jobs_[id].get();
                 const size_t need = kBytesPerObj * (1 + (size_t)j->nPIs + j->nAnds);
                 const bool fits = batch.empty() || (bytes + need <= admit_ && (int)batch.size() < maxBatch_);
-                if (j->rwFlags == head->rwFlags && j->stFlags == head->stFlags && j->aiger == head->aiger && fits) {
+                const int64_t js = 1 + (int64_t)j->nAnds;
+                const bool alike = js <= hs * kSizeRatio && hs <= js * kSizeRatio;
+                if (j->rwFlags == head->rwFlags && j->stFlags == head->stFlags && j->aiger == head->aiger && fits &&
+                    alike) {
                     batch.push_back(j);
                     bytes += need;
                     j->state = kRunning;

@@ -1,10 +1,11 @@
 // Served mode: AIGs submitted one by one are rewritten in dynamic batches.
 //
 // The reference runs one AIG per process invocation.  A server takes jobs
-// (copied at submission, so the caller may free its arrays), and a worker
-// thread repeatedly takes the queued jobs in arrival order -- those with the
-// head job's flags, as long as their estimated device footprint stays within
-// the admission budget -- and runs them as one batch through the engine
+// (copied at submission, so the caller may free its arrays), and each of
+// several worker threads, as soon as it is free, takes the queued jobs in
+// arrival order -- those with the head job's flags and of a size like the
+// head's, as long as their estimated device footprint stays within its share
+// of the admission budget -- and runs them as one batch through its engine
 // (upload, rw, st, download) under the context's lock, so served jobs and
 // direct calls on the same context never overlap on the device.  Each job
 // records its submit-to-done latency.
@@ -42,6 +43,9 @@ class Server {
     // Device bytes the admission rule charges per object of a batch (arena
     // of rw plus the graph arrays and their spares).
     static constexpr size_t kBytesPerObj = 720;
+    // A batch takes only jobs whose AND count is within this factor of its
+    // first job's (the batch runs as long as its deepest graph).
+    static constexpr int64_t kSizeRatio = 8;
 
     // workers > 1 adds engines of the server's own (stream, arena, staging)
     // on the same device, so batches overlap on the GPU: a batch waits on its

@@ -160,15 +160,17 @@ int culs_rw_st(culs_ctx *ctx, culs_graph *g, uint32_t rwFlags, uint32_t stFlags)
 int culs_rw_st_batch(culs_ctx *ctx, culs_graph *const *gs, int count, uint32_t rwFlags, uint32_t stFlags);
 
 /* ------------------------------------------------------------ served mode
- * AIGs submitted one by one are rewritten (`rw; st`) in dynamic batches by a
- * worker thread of the context: it takes queued jobs in arrival order (those
- * with the first job's flags) while their estimated device footprint stays
- * within admitBytes (0: the context's HBM budget) and maxBatch (<= 0: no
- * limit), runs them as one batch, and holds every result until fetched.
- * `workers` (<= 0: 2) batches run at once, each on an engine of its own
- * (the first is the context's), splitting the admission budget: a batch
- * waits on its deepest graph while most of the GPU would sit idle.  Jobs
- * and direct calls on the same context never overlap on its engine.
+ * AIGs submitted one by one are rewritten (`rw; st`) in dynamic batches by
+ * `workers` (<= 0: 4) worker threads of the context, each on an engine of its
+ * own (the first is the context's), splitting the admission budget
+ * admitBytes (0: the context's HBM budget).  A worker, as soon as it is free,
+ * takes the queued jobs in arrival order -- those with the first job's flags
+ * and an AND count within 8x of its -- while their estimated device
+ * footprint stays within its share and maxBatch (<= 0: no limit), runs them
+ * as one batch, and holds every result until fetched.  Batches of several
+ * workers overlap on the GPU: a batch waits on its deepest graph while most
+ * of the GPU would sit idle.  Jobs and direct calls on the same context
+ * never overlap on its engine.
  * No counterpart in the reference (one AIG per process invocation).
  *
  * culs_submit copies the graph (the caller may free its arrays) and returns
