@@ -97,6 +97,13 @@ struct Batch {
     cudaError_t reserve(int64_t nObj, int64_t nPO, int G);
     cudaError_t reserve_spare(int64_t nObj, int64_t nPO);
     void swap_spare();
+    // Objects per level summed over the graphs (+1): the number of nodes a
+    // level-ordered dataflow pass over the batch can work on at once.
+    int64_t flow_width() const {
+        int64_t w = 1;
+        for (const DevGraph &g : hg) w += (1 + (int64_t)g.nPIs + g.nAnds) / ((int64_t)g.nLevels + 1);
+        return w;
+    }
     // Copies the current graph into the kept buffers and sets keep.
     cudaError_t keep_current(cudaStream_t s);
     // Makes the kept graph current (the current one is discarded) and clears

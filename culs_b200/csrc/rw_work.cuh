@@ -60,6 +60,7 @@ struct RwWork {
     int64_t nL0 = 0;  // constants and PIs: W positions [0, nL0)
     int64_t nPO = 0;
     int maxLevel = 0;
+    int64_t width = 1;  // Batch::flow_width of the batch: nodes a level-ordered pass can work on at once
     unsigned long long *warpPairs = nullptr;  // device counter (RwStats::warpPairs)
     bool useZeros = false;
     DevGraph *dg = nullptr;  // device graph table (cpos = constant's W position)

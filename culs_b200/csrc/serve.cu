@@ -12,13 +12,19 @@ Server::Server(Engine &eng, std::mutex &engMu, size_t admitBytes, int maxBatch, 
     : eng_(eng), engMu_(engMu), maxBatch_(maxBatch > 0 ? maxBatch : 1 << 20) {
     workers = workers < 1 ? 1 : workers;
     admit_ = admitBytes / (size_t)workers;  // every worker's batch within its share
-    for (int w = 1; w < workers; w++) {
+    // every worker has an engine of its own (stream, arena, staging) whose
+    // HBM budget is its share of the admission budget, so the workers
+    // together stay within it whatever the context's own engine holds
+    for (int w = 0; w < workers; w++) {
         auto e = std::make_unique<Engine>();
-        if (e->init(eng.budget() / (size_t)workers) != CULS_OK) break;  // fewer workers
+        if (e->init(admit_) != CULS_OK) break;  // fewer workers
         own_.push_back(std::move(e));
         ownMu_.push_back(std::make_unique<std::mutex>());
     }
-    th_ = std::thread([this] { worker(eng_, engMu_); });
+    if (own_.empty()) {  // no room for an engine of its own: the context's
+        th_ = std::thread([this] { worker(eng_, engMu_); });
+        return;
+    }
     for (size_t i = 0; i < own_.size(); i++) {
         Engine *e = own_[i].get();
         std::mutex *m = ownMu_[i].get();

@@ -47,9 +47,11 @@ class Server {
     // first job's (the batch runs as long as its deepest graph).
     static constexpr int64_t kSizeRatio = 8;
 
-    // workers > 1 adds engines of the server's own (stream, arena, staging)
-    // on the same device, so batches overlap on the GPU: a batch waits on its
-    // deepest graph's critical path, during which most SMs would sit idle.
+    // Every worker runs on an engine of the server's own (stream, arena,
+    // staging) on the context's device, with its share of the admission
+    // budget as HBM budget; workers' batches overlap on the GPU: a batch
+    // waits on its deepest graph's critical path, during which most SMs
+    // would sit idle.
     Server(Engine &eng, std::mutex &engMu, size_t admitBytes, int maxBatch, int workers = 1);
     ~Server();  // finishes every queued job, then stops the worker
 
@@ -80,7 +82,7 @@ class Server {
 
     Engine &eng_;
     std::mutex &engMu_;
-    std::vector<std::unique_ptr<Engine>> own_;  // engines of workers 2..n
+    std::vector<std::unique_ptr<Engine>> own_;  // the workers' engines
     std::vector<std::unique_ptr<std::mutex>> ownMu_;
     std::vector<std::thread> extra_;
     size_t admit_;
