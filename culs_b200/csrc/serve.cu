@@ -13,11 +13,13 @@ Server::Server(Engine &eng, std::mutex &engMu, size_t admitBytes, int maxBatch, 
     workers = workers < 1 ? 1 : workers;
     admit_ = admitBytes / (size_t)workers;  // every worker's batch within its share
     // every worker has an engine of its own (stream, arena, staging) whose
-    // HBM budget is its share of the admission budget, so the workers
-    // together stay within it whatever the context's own engine holds
+    // HBM budget is its share of the admission budget (at least 1 GiB, room
+    // for the arena's fixed part), so the workers together stay near it
+    // whatever the context's own engine holds
+    const size_t engBudget = std::max<size_t>(admit_, (size_t)1 << 30);
     for (int w = 0; w < workers; w++) {
         auto e = std::make_unique<Engine>();
-        if (e->init(admit_) != CULS_OK) break;  // fewer workers
+        if (e->init(engBudget) != CULS_OK) break;  // fewer workers
         own_.push_back(std::move(e));
         ownMu_.push_back(std::make_unique<std::mutex>());
     }
