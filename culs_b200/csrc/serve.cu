@@ -14,9 +14,10 @@ Server::Server(Engine &eng, std::mutex &engMu, size_t admitBytes, int maxBatch, 
     admit_ = admitBytes / (size_t)workers;  // every worker's batch within its share
     // every worker has an engine of its own (stream, arena, staging) whose
     // HBM budget is its share of the admission budget (at least 1 GiB, room
-    // for the arena's fixed part), so the workers together stay near it
-    // whatever the context's own engine holds
-    const size_t engBudget = std::max<size_t>(admit_, (size_t)1 << 30);
+    // for the arena's fixed part, and never more than the context's budget),
+    // so the workers together stay near it whatever the context's own engine
+    // holds
+    const size_t engBudget = std::min<size_t>(eng.budget(), std::max<size_t>(admit_, (size_t)1 << 30));
     for (int w = 0; w < workers; w++) {
         auto e = std::make_unique<Engine>();
         if (e->init(engBudget) != CULS_OK) break;  // fewer workers

@@ -163,7 +163,8 @@ int culs_rw_st_batch(culs_ctx *ctx, culs_graph *const *gs, int count, uint32_t r
  * AIGs submitted one by one are rewritten (`rw; st`) in dynamic batches by
  * `workers` (<= 0: 4) worker threads of the context, each on an engine of its
  * own whose HBM budget is its share of the admission budget admitBytes (0:
- * the context's HBM budget), or 1 GiB if that is more.  A worker, as soon as it is free,
+ * the context's HBM budget), or 1 GiB if that is more, and at most the
+ * context's HBM budget.  A worker, as soon as it is free,
  * takes the queued jobs in arrival order -- those with the first job's flags
  * and an AND count within 8x of its -- while their estimated device
  * footprint stays within its share and maxBatch (<= 0: no limit), runs them
