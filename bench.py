@@ -389,14 +389,14 @@ def served_load(ctx, pool, rate, njobs, seed):
     return nodes[0] / (done_t[0] - t0), np.sort(np.array(lat)), picks
 
 
-def served_session(device, pool, loads, njobs, repeats, workers, budget=SERVE_BUDGET, seed=5):
+def served_session(device, pool, loads, njobs, repeats, workers, budget=SERVE_BUDGET, seed=5, max_batch=0):
     """Served mode at each offered load (a fraction of the batch capacity),
     `repeats` runs of `njobs` jobs each, on a fresh context: the median and
     the range of p50, p99 and throughput per load."""
     import culs_b200 as C
     cap, caps = served_capacity(device, pool)
     ctx = C.Context(device=device)
-    ctx.serve_start(admit_bytes=budget, workers=workers)
+    ctx.serve_start(admit_bytes=budget, workers=workers, max_batch=max_batch)
     sweep = []
     try:
         for i, load in enumerate(loads):
@@ -416,6 +416,7 @@ def served_session(device, pool, loads, njobs, repeats, workers, budget=SERVE_BU
         ctx.serve_stop()
         ctx.close()
     return {"capacity_jobs_per_s": cap, "capacity_runs": caps, "budget_bytes": budget, "workers": workers,
+            "max_batch": max_batch,
             "pool_graphs": len(pool), "pool_and_nodes": int(sum(g.nAnds for g in pool)), "sweep": sweep,
             "timing": "wall clock, submit to done"}
 
@@ -430,7 +431,7 @@ def served_arm(args, group):
     import culs_b200 as C
     pool = served_pool()
     loads = sorted(set([0.25, 0.5, 0.75, args.load]))
-    srv = served_session(group.local, pool, loads, args.jobs, args.repeats, args.workers)
+    srv = served_session(group.local, pool, loads, args.jobs, args.repeats, args.workers, max_batch=args.max_batch)
     ctx = C.Context(device=group.local)
     at = [x for x in srv["sweep"] if x["load_vs_capacity"] == args.load][0]
     rng = np.random.default_rng(5)
@@ -671,6 +672,7 @@ def main():
     ap.add_argument("--workers", type=int, default=4, help="c5: batches the served mode runs at once")
     ap.add_argument("--jobs", type=int, default=20000, help="c5: jobs per run")
     ap.add_argument("--repeats", type=int, default=3, help="c5: runs per offered load")
+    ap.add_argument("--max-batch", type=int, default=0, help="c5: jobs per served batch at most (0: no cap)")
     ap.add_argument("--no-served", action="store_true",
                     help="c4: leave out the short served-mode run of the default line")
     args = ap.parse_args()

@@ -8,6 +8,8 @@
 // and the PIs), POs hold local literals.  A single graph is a batch of one.
 #pragma once
 
+#include <algorithm>
+
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -176,6 +178,10 @@ class Engine {
     cudaStream_t stream() const { return s_; }
     size_t budget() const { return budget_; }
     int device() const { return device_; }  // the CUDA device the engine lives on
+    // Sizes every grid of this engine for 1/share of the device's SMs, so
+    // that `share` engines running at once (the served workers) overlap on
+    // the GPU instead of queueing behind one another's persistent kernels.
+    void set_sm_share(int share) { sms_ = std::max(8, num_sms() / std::max(1, share)); }
     size_t arenaHighWater() const { return ar_.high_water(); }
     int kernelLaunches() const { return launches_; }
     void setProfile(bool on) { prof_ = on; }

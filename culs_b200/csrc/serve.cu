@@ -21,6 +21,7 @@ Server::Server(Engine &eng, std::mutex &engMu, size_t admitBytes, int maxBatch, 
     for (int w = 0; w < workers; w++) {
         auto e = std::make_unique<Engine>();
         if (e->init(engBudget) != CULS_OK) break;  // fewer workers
+        e->set_sm_share(workers);
         own_.push_back(std::move(e));
         ownMu_.push_back(std::make_unique<std::mutex>());
     }
