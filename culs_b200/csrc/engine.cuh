@@ -182,6 +182,11 @@ class Engine {
     // that `share` engines running at once (the served workers) overlap on
     // the GPU instead of queueing behind one another's persistent kernels.
     void set_sm_share(int share) { sms_ = std::max(8, num_sms() / std::max(1, share)); }
+    // Grows the scratch arena and the pinned staging up front for batches of
+    // up to nObj objects, so that serving them needs no allocation (freeing
+    // device or pinned memory synchronises the whole device, stalling every
+    // other engine's work).
+    int prepare(int64_t nObj);
     size_t arenaHighWater() const { return ar_.high_water(); }
     int kernelLaunches() const { return launches_; }
     void setProfile(bool on) { prof_ = on; }

@@ -66,6 +66,12 @@ void run_parallel(int runs, F fn) {
 
 }  // namespace
 
+int Engine::prepare(int64_t nObj) {
+    int rc = ensure_arena((size_t)nObj * 640 + ((size_t)256 << 20));
+    if (rc == CULS_OK) rc = ensure_stage(3 * (size_t)nObj);
+    return rc;
+}
+
 int Engine::ensure_stage(size_t ints) {
     ints = std::max<size_t>(ints, 1);
     if (stage_ && stageCap_ >= ints) return 0;

@@ -22,6 +22,9 @@ Server::Server(Engine &eng, std::mutex &engMu, size_t admitBytes, int maxBatch, 
         auto e = std::make_unique<Engine>();
         if (e->init(engBudget) != CULS_OK) break;  // fewer workers
         e->set_sm_share(workers);
+        // room for a typical batch (at most 16M objects within the share) up
+        // front: growing it later would synchronise the whole device
+        e->prepare(std::min<int64_t>((int64_t)(engBudget / kBytesPerObj), (int64_t)16 << 20));
         own_.push_back(std::move(e));
         ownMu_.push_back(std::make_unique<std::mutex>());
     }
