@@ -29,13 +29,19 @@ Server::Server(Engine &eng, std::mutex &engMu, size_t admitBytes, int maxBatch, 
         ownMu_.push_back(std::make_unique<std::mutex>());
     }
     if (own_.empty()) {  // no room for an engine of its own: the context's
-        th_ = std::thread([this] { worker(eng_, engMu_); });
+        th_ = std::thread([this] { worker(eng_, engMu_, INT64_MAX); });
         return;
     }
-    for (size_t i = 0; i < own_.size(); i++) {
+    // the first half of the workers (those beyond two) serve small jobs
+    // only: a worker i < n/2 takes jobs below kSmallAnds * 8^i AND nodes, the
+    // others take any job.  Small jobs then never wait behind a batch that
+    // runs for a large graph's critical path.
+    const int n = (int)own_.size();
+    for (int i = 0; i < n; i++) {
         Engine *e = own_[i].get();
         std::mutex *m = ownMu_[i].get();
-        extra_.emplace_back([this, e, m] { worker(*e, *m); });
+        const int64_t cap = (n > 2 && i < n / 2) ? kSmallAnds << (3 * i) : INT64_MAX;
+        extra_.emplace_back([this, e, m, cap] { worker(*e, *m, cap); });
     }
 }
 
@@ -77,7 +83,7 @@ int Server::submit(const int32_t *f0, const int32_t *f1, const int32_t *outs, in
         queue_.push_back(job->id);
         jobs_[job->id] = std::move(job);
     }
-    cvWork_.notify_one();
+    cvWork_.notify_all();  // workers take different jobs
     return CULS_OK;
 }
 
@@ -122,7 +128,7 @@ int Server::submit_aiger(const uint8_t *data, size_t len, uint32_t rwFlags, uint
         queue_.push_back(job->id);
         jobs_[job->id] = std::move(job);
     }
-    cvWork_.notify_one();
+    cvWork_.notify_all();  // workers take different jobs
     return CULS_OK;
 }
 
@@ -216,14 +222,24 @@ int Server::cancel(int64_t id) {
     return CULS_OK;
 }
 
-void Server::worker(Engine &eng, std::mutex &engMu) {
+void Server::worker(Engine &eng, std::mutex &engMu, int64_t maxAnds) {
     cudaSetDevice(eng.device());  // the current device is per thread
+    // the first queued job this worker takes (below maxAnds AND nodes)
+    auto first = [&]() -> std::deque<int64_t>::iterator {
+        for (auto it = queue_.begin(); it != queue_.end(); ++it)
+            if (jobs_[*it]->nAnds < maxAnds) return it;
+        return queue_.end();
+    };
     while (true) {
         std::vector<ServeJob *> batch;
         {
             std::unique_lock<std::mutex> lk(mu_);
-            cvWork_.wait(lk, [&] { return stop_ || !queue_.empty(); });
+            cvWork_.wait(lk, [&] { return first() != queue_.end() || (stop_ && queue_.empty()); });
             if (queue_.empty()) return;  // stop requested and nothing left
+            // the jobs before the first one this worker takes stay queued,
+            // in order, for the other workers
+            std::deque<int64_t> skipped(queue_.begin(), first());
+            queue_.erase(queue_.begin(), first());
             // admission: arrival order, the head's flags and size class,
             // within the budget (the head is always admitted; the engine
             // refuses it if it alone exceeds the context's budget).  A batch
@@ -242,7 +258,7 @@ void Server::worker(Engine &eng, std::mutex &engMu) {
                 const size_t need = kBytesPerObj * (1 + (size_t)j->nPIs + j->nAnds);
                 const bool fits = batch.empty() || (bytes + need <= admit_ && (int)batch.size() < maxBatch_);
                 const int64_t js = 1 + (int64_t)j->nAnds;
-                const bool alike = js <= hs * kSizeRatio && hs <= js * kSizeRatio;
+                const bool alike = js <= hs * kSizeRatio && hs <= js * kSizeRatio && j->nAnds < maxAnds;
                 if (j->rwFlags == head->rwFlags && j->stFlags == head->stFlags && j->aiger == head->aiger && fits &&
                     alike) {
                     batch.push_back(j);
@@ -257,7 +273,14 @@ void Server::worker(Engine &eng, std::mutex &engMu) {
                 queue_.push_front(rest.back());
                 rest.pop_back();
             }
+            while (!skipped.empty()) {
+                queue_.push_front(skipped.back());
+                skipped.pop_back();
+            }
         }
+        // jobs this worker left to the others, or an emptied queue that
+        // workers waiting to stop must see
+        cvWork_.notify_all();
         // a host exception (an allocation) fails the batch's jobs, not the
         // worker thread and with it the process
         const int rc = guard_call(nullptr, [&]() -> int {

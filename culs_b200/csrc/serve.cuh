@@ -46,6 +46,9 @@ class Server {
     // A batch takes only jobs whose AND count is within this factor of its
     // first job's (the batch runs as long as its deepest graph).
     static constexpr int64_t kSizeRatio = 8;
+    // Workers reserved for small jobs take jobs below kSmallAnds * 8^i AND
+    // nodes (worker i of the first half, when there are more than two).
+    static constexpr int64_t kSmallAnds = 65536;
 
     // Every worker runs on an engine of the server's own (stream, arena,
     // staging) on the context's device, with its share of the admission
@@ -76,7 +79,7 @@ class Server {
     const std::string &lastError() const { return err_; }
 
   private:
-    void worker(Engine &eng, std::mutex &engMu);
+    void worker(Engine &eng, std::mutex &engMu, int64_t maxAnds);
     void run_batch(Engine &eng, std::mutex &engMu, std::vector<ServeJob *> &batch);
     void run_aiger(Engine &eng, std::mutex &engMu, std::vector<ServeJob *> &batch);
 
