@@ -181,7 +181,12 @@ class Engine {
     // Sizes every grid of this engine for 1/share of the device's SMs, so
     // that `share` engines running at once (the served workers) overlap on
     // the GPU instead of queueing behind one another's persistent kernels.
-    void set_sm_share(int share) { sms_ = std::max(8, num_sms() / std::max(1, share)); }
+    // Persistent kernels get one resident wave of blocks on that share (the
+    // enumeration's blocks fit 3 to an SM).
+    void set_sm_share(int share) {
+        sms_ = std::max(8, num_sms() / std::max(1, share));
+        tune_.enumBlocksPerSm = std::min(tune_.enumBlocksPerSm, 3);
+    }
     // Grows the scratch arena and the pinned staging up front for batches of
     // up to nObj objects, so that serving them needs no allocation (freeing
     // device or pinned memory synchronises the whole device, stalling every

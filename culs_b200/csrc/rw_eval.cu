@@ -275,7 +275,9 @@ int rw_evaluate(ExecCtx &X, RwWork &w, const Batch &b) {
     w.bestOut = X.ar->get<uint8_t>(N);
     uint8_t *candFlag = X.ar->get<uint8_t>(N);
     w.cand = X.ar->get<int>(N);
-    const unsigned evalGrid = X.grid(N, kEvalBlock);
+    // one resident wave: 8 blocks an SM (registers and shared memory); a
+    // second wave of a grid-stride kernel would only start as the first ends
+    const unsigned evalGrid = grid_1d(N, kEvalBlock, X.sms * 8);
     int *scratch = X.ar->get<int>((size_t)2 * kLibSlots * evalGrid * kEvalBlock);
     int *mffcNodes = X.ar->get<int>((size_t)evalGrid * (kEvalBlock / 32) * kWarpNodes * 8 * 8);
     if (!slots || !dOff || !w.bestCut || !w.bestOut || !candFlag || !w.cand || !scratch || !mffcNodes)
