@@ -403,6 +403,13 @@ int culs_set_param(culs_ctx *ctx, int which, int64_t value) {
                 if (value < 1 || value > 64) return CULS_E_INVALID;
                 t.enumBlocksPerSm = (int)value;
                 return CULS_OK;
+            case CULS_PARAM_SM_SHARE:
+                if (value < 1 || value > 64) return CULS_E_INVALID;
+                ctx->eng.set_sm_share((int)value);
+                return CULS_OK;
+            case CULS_PARAM_HIGH_PRIORITY:
+                if (value != 0 && value != 1) return CULS_E_INVALID;
+                return set_err(ctx, ctx->eng.set_high_priority(value != 0));
             default:
                 return CULS_E_INVALID;
         }
@@ -417,6 +424,8 @@ int culs_get_param(culs_ctx *ctx, int which, int64_t *value) {
         switch (which) {
             case CULS_PARAM_ENUM_WIDE_MIN: *value = t.enumWideMin; return CULS_OK;
             case CULS_PARAM_ENUM_BLOCKS_PER_SM: *value = t.enumBlocksPerSm; return CULS_OK;
+            case CULS_PARAM_SM_SHARE: *value = ctx->eng.sm_share(); return CULS_OK;
+            case CULS_PARAM_HIGH_PRIORITY: *value = ctx->eng.high_priority() ? 1 : 0; return CULS_OK;
             default: return CULS_E_INVALID;
         }
     });

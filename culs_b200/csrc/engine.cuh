@@ -184,9 +184,17 @@ class Engine {
     // Persistent kernels get one resident wave of blocks on that share (the
     // enumeration's blocks fit 3 to an SM).
     void set_sm_share(int share) {
-        sms_ = std::max(8, num_sms() / std::max(1, share));
-        tune_.enumBlocksPerSm = std::min(tune_.enumBlocksPerSm, 3);
+        share_ = std::max(1, share);
+        sms_ = std::max(8, num_sms() / share_);
+        if (share_ > 1) tune_.enumBlocksPerSm = std::min(tune_.enumBlocksPerSm, 3);
     }
+    int sm_share() const { return share_; }
+    // Recreates the engine's stream at the device's highest stream priority
+    // (high) or the default one: the block scheduler then starts this
+    // engine's blocks before pending blocks of lower-priority streams.  Only
+    // between calls (the stream is drained first).
+    int set_high_priority(bool high);
+    bool high_priority() const { return highPrio_; }
     // Grows the scratch arena and the pinned staging up front for batches of
     // up to nObj objects, so that serving them needs no allocation (freeing
     // device or pinned memory synchronises the whole device, stalling every
@@ -251,6 +259,8 @@ class Engine {
     Arena ar_;
     int launches_ = 0;
     int sms_ = 148;
+    int share_ = 1;
+    bool highPrio_ = false;
     bool prof_ = false;
     Tune tune_;
     std::shared_ptr<DevPool> pool_;

@@ -356,6 +356,20 @@ int Engine::init(size_t hbmBudget) {
     return 0;
 }
 
+int Engine::set_high_priority(bool high) {
+    int least = 0, greatest = 0;
+    int rc = check(cudaDeviceGetStreamPriorityRange(&least, &greatest), "stream priorities");
+    if (rc) return rc;
+    if ((rc = sync())) return rc;
+    cudaStream_t ns = nullptr;
+    if ((rc = check(cudaStreamCreateWithPriority(&ns, cudaStreamNonBlocking, high ? greatest : least), "stream")))
+        return rc;
+    cudaStreamDestroy(s_);
+    s_ = ns;
+    highPrio_ = high;
+    return 0;
+}
+
 int Engine::ensure_arena(size_t bytes) {
     bytes = (bytes + (64u << 20)) & ~(size_t)((1u << 20) - 1);
     if (bytes <= ar_.capacity()) return 0;
