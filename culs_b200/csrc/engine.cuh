@@ -194,6 +194,10 @@ class Engine {
     // engine's blocks before pending blocks of lower-priority streams.  Only
     // between calls (the stream is drained first).
     int set_high_priority(bool high);
+    // Runs the engine's work on stream s, owned by the caller (a stream of
+    // an SM partition of `sms` SMs, partition.cuh), with every grid sized for
+    // those SMs.  Only between calls.
+    int adopt_stream(cudaStream_t s, int sms);
     bool high_priority() const { return highPrio_; }
     // Grows the scratch arena and the pinned staging up front for batches of
     // up to nObj objects, so that serving them needs no allocation (freeing
@@ -261,6 +265,7 @@ class Engine {
     int sms_ = 148;
     int share_ = 1;
     bool highPrio_ = false;
+    bool ownStream_ = true;  // s_ was created by this engine
     bool prof_ = false;
     Tune tune_;
     std::shared_ptr<DevPool> pool_;

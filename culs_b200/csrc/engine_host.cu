@@ -272,7 +272,7 @@ Engine::~Engine() {
     if (stage_) cudaFreeHost(stage_);
     for (auto &e : ev_)
         if (e) cudaEventDestroy(e);
-    if (s_) cudaStreamDestroy(s_);
+    if (s_ && ownStream_) cudaStreamDestroy(s_);
 }
 
 int Engine::fail(int code, const std::string &msg) {
@@ -364,9 +364,22 @@ int Engine::set_high_priority(bool high) {
     cudaStream_t ns = nullptr;
     if ((rc = check(cudaStreamCreateWithPriority(&ns, cudaStreamNonBlocking, high ? greatest : least), "stream")))
         return rc;
-    cudaStreamDestroy(s_);
+    if (ownStream_) cudaStreamDestroy(s_);
     s_ = ns;
+    ownStream_ = true;
     highPrio_ = high;
+    return 0;
+}
+
+int Engine::adopt_stream(cudaStream_t s, int sms) {
+    int rc = sync();
+    if (rc) return rc;
+    if (ownStream_) cudaStreamDestroy(s_);
+    s_ = s;
+    ownStream_ = false;
+    sms_ = std::max(8, sms);
+    share_ = std::max(1, num_sms() / sms_);
+    tune_.enumBlocksPerSm = std::min(tune_.enumBlocksPerSm, 3);
     return 0;
 }
 

@@ -18,10 +18,15 @@ Server::Server(Engine &eng, std::mutex &engMu, size_t admitBytes, int maxBatch, 
     // so the workers together stay near it whatever the context's own engine
     // holds
     const size_t engBudget = std::min<size_t>(eng.budget(), std::max<size_t>(admit_, (size_t)1 << 30));
+    if (workers > 1 && !make_sm_partitions(eng.device(), workers, parts_, nullptr)) parts_.clear();
     for (int w = 0; w < workers; w++) {
         auto e = std::make_unique<Engine>();
         if (e->init(engBudget) != CULS_OK) break;  // fewer workers
-        e->set_sm_share(workers);
+        if (!parts_.empty()) {
+            if (e->adopt_stream(parts_[w].stream, parts_[w].sms) != CULS_OK) break;
+        } else {
+            e->set_sm_share(workers);
+        }
         // room for a typical batch (at most 16M objects within the share) up
         // front: growing it later would synchronise the whole device
         e->prepare(std::min<int64_t>((int64_t)(engBudget / kBytesPerObj), (int64_t)16 << 20));
@@ -54,6 +59,8 @@ Server::~Server() {
     if (th_.joinable()) th_.join();
     for (auto &t : extra_)
         if (t.joinable()) t.join();
+    own_.clear();  // the engines, before the partitions their streams belong to
+    destroy_sm_partitions(parts_);
 }
 
 int Server::submit(const int32_t *f0, const int32_t *f1, const int32_t *outs, int32_t nPIs, int32_t nPOs,

@@ -23,6 +23,7 @@
 #include <vector>
 
 #include "engine.cuh"
+#include "partition.cuh"
 
 namespace culs {
 
@@ -54,7 +55,9 @@ class Server {
     // staging) on the context's device, with its share of the admission
     // budget as HBM budget; workers' batches overlap on the GPU: a batch
     // waits on its deepest graph's critical path, during which most SMs
-    // would sit idle.
+    // would sit idle.  With several workers each runs on a disjoint SM
+    // partition of the GPU (a green context, partition.cuh), or, where the
+    // driver cannot partition, sizes its grids for its share of the SMs.
     Server(Engine &eng, std::mutex &engMu, size_t admitBytes, int maxBatch, int workers = 1);
     ~Server();  // finishes every queued job, then stops the worker
 
@@ -85,6 +88,7 @@ class Server {
 
     Engine &eng_;
     std::mutex &engMu_;
+    std::vector<SmPartition> parts_;             // the workers' SM partitions (empty: shared SMs)
     std::vector<std::unique_ptr<Engine>> own_;  // the workers' engines
     std::vector<std::unique_ptr<std::mutex>> ownMu_;
     std::vector<std::thread> extra_;
