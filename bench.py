@@ -669,7 +669,7 @@ def main():
     ap.add_argument("--workload", default="c4", choices=["c4", "c4m", "c3", "c3m", "c2", "c1", "c5"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--load", type=float, default=0.75, help="c5: offered load as a fraction of measured capacity")
-    ap.add_argument("--workers", type=int, default=4, help="c5: batches the served mode runs at once")
+    ap.add_argument("--workers", type=int, default=2, help="c5: batches the served mode runs at once")
     ap.add_argument("--jobs", type=int, default=20000, help="c5: jobs per run")
     ap.add_argument("--repeats", type=int, default=3, help="c5: runs per offered load")
     ap.add_argument("--max-batch", type=int, default=0, help="c5: jobs per served batch at most (0: no cap)")

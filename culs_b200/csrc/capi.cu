@@ -292,7 +292,7 @@ int culs_serve_start(culs_ctx *ctx, size_t admitBytes, int maxBatch, int workers
         std::lock_guard<std::mutex> lk(ctx->srvMu);
         if (ctx->srv) return CULS_E_INVALID;
         if (admitBytes == 0) admitBytes = ctx->eng.budget();
-        if (workers <= 0) workers = 4;
+        if (workers <= 0) workers = 2;
         int dev = 0;
         cudaGetDevice(&dev);
         cudaSetDevice(ctx->eng.device());  // the server's own engines live beside the context's

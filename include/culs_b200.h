@@ -161,7 +161,7 @@ int culs_rw_st_batch(culs_ctx *ctx, culs_graph *const *gs, int count, uint32_t r
 
 /* ------------------------------------------------------------ served mode
  * AIGs submitted one by one are rewritten (`rw; st`) in dynamic batches by
- * `workers` (<= 0: 4) worker threads of the context, each on an engine of its
+ * `workers` (<= 0: 2) worker threads of the context, each on an engine of its
  * own whose HBM budget is its share of the admission budget admitBytes (0:
  * the context's HBM budget), or 1 GiB if that is more, and at most the
  * context's HBM budget.  A worker, as soon as it is free,
@@ -169,8 +169,11 @@ int culs_rw_st_batch(culs_ctx *ctx, culs_graph *const *gs, int count, uint32_t r
  * and an AND count within 8x of its -- while their estimated device
  * footprint stays within its share and maxBatch (<= 0: no limit), runs them
  * as one batch, and holds every result until fetched.  Batches of several
- * workers overlap on the GPU: a batch waits on its deepest graph while most
- * of the GPU would sit idle.  Jobs and direct calls on the same context
+ * workers overlap on the GPU, each worker on a disjoint partition of the SMs
+ * (a green context) where the driver supports it: a batch waits on its
+ * deepest graph while most of the GPU would sit idle.  With more than two
+ * workers, the first half serve small jobs only (below 65,536 * 8^i AND
+ * nodes for worker i).  Jobs and direct calls on the same context
  * never overlap on its engine.
  * No counterpart in the reference (one AIG per process invocation).
  *
