@@ -1076,6 +1076,298 @@ static Graph dedup_cpu(const Graph &g) {
     return o;
 }
 
+// ---------------------------------------------------------------- balance
+// AIG balancing `b` (src/algorithms/balance.cu:912-1382, called by
+// AIGMan::balance, src/aig_manager.cu:682-737), sortDecId = 1 (the `b`
+// default: inputs sorted by decreasing level, then decreasing literal).
+// Sequential restatement of the reference's two phases:
+//  1. cover finding, level by level from the POs (balance.cu:953-1029):
+//     the next level is every AND input of the covers of this level, in
+//     increasing id order; a node's cover is its supergate, collected by the
+//     DFS of localCoverTravToTable (balance.cu:666-751), and its "last
+//     appear level" the last level it is listed on;
+//  2. reconstruction, deepest covers first (balance.cu:1157-1248): covers of
+//     one level in increasing node id, in chunks of 32,768; all covers of a
+//     chunk pair their two lowest inputs in lockstep steps against one table
+//     of built nodes (existing pairs are reused, new ones get id counter +
+//     cover index, the smallest id of a key wins), and finally nodes are
+//     renumbered in id order (balance.cu:1271-1300).
+// The reference is deterministic here: duplicate keys inside a step resolve
+// by atomicMin and every other step is order independent.
+static const int kBalMaxCover = 1024;   // MAX_LOCAL_COVER_SIZE
+static const int kBalStack = 128;       // DFS_COVER_STACK_SIZE
+static const int kBalChunk = 32768;     // iterLen
+static const unsigned kBalEmpty = 0xFFFFFFFFu;
+
+// checkTrivialAndCases + TableLookup of the reconstruction
+// (src/hash_table/hash_table.h:435-449, balance.cu:85-110): literal of the
+// AND of lit1 and lit2 if it is trivial or already built, else kBalEmpty.
+static unsigned bal_lookup(int l1, int l2, const std::unordered_map<uint64_t, unsigned> &tab) {
+    if (l1 == l2) return (unsigned)l1;
+    if (l1 == (l2 ^ 1)) return 1u;  // AigConst0 (AIGMan literal 1 = FALSE)
+    if (l1 == 0) return (unsigned)l2;  // AigConst1
+    if (l2 == 0) return (unsigned)l1;
+    if (l1 == 1 || l2 == 1) return 1u;
+    if (l1 > l2) std::swap(l1, l2);
+    auto it = tab.find(((uint64_t)(uint32_t)l1 << 32) | (uint32_t)l2);
+    return it == tab.end() ? kBalEmpty : it->second << 1;
+}
+
+static Graph balance_core(const Graph &g, std::string *err) {
+    const int nPIs = g.nPIs, nObjs = g.nObjs, nPOs = g.nPOs;
+    Graph r;
+    r.nPIs = nPIs;
+    r.nPOs = nPOs;
+    std::vector<int> nfo(nObjs, 0);  // fanouts incl. PO references (aig_manager.cu:203-221)
+    for (int v = nPIs + 1; v < nObjs; v++) {
+        nfo[lid(g.f0[v])]++;
+        nfo[lid(g.f1[v])]++;
+    }
+    for (int o : g.outs) nfo[lid(o)]++;
+    // ---- phase 1: covers
+    std::vector<int> covLen(nObjs, -1), lastLevel(nObjs, -1);
+    std::vector<std::vector<int>> cover(nObjs);
+    std::vector<int> list;
+    {
+        std::vector<char> seen(nObjs, 0);
+        for (int o : g.outs) {  // checkCoverTravEnd: AND drivers, first occurrence
+            int v = lid(o);
+            if (v > nPIs && !seen[v]) {
+                seen[v] = 1;
+                list.push_back(v);
+            }
+        }
+    }
+    if (list.empty()) {  // no AND node drives a PO: no AND node is kept
+        r.nObjs = nPIs + 1;
+        r.f0.assign(r.nObjs, -1);
+        r.f1.assign(r.nObjs, -1);
+        r.outs = g.outs;
+        return r;
+    }
+    int levelCount = 0;
+    std::vector<char> status(nObjs);
+    while (!list.empty()) {
+        std::fill(status.begin(), status.end(), 0);
+        for (int v : list) {
+            lastLevel[v] = levelCount;
+            if (covLen[v] < 0) {
+                // localCoverTravToTable (balance.cu:666-751)
+                std::vector<int> &cv = cover[v];
+                int stk[kBalStack];
+                int top = -1;
+                stk[++top] = 2 * v;
+                bool constFalse = false;
+                while (top >= 0) {
+                    const int cur = stk[top--];
+                    bool same = false;
+                    for (int x : cv) {
+                        if (x == cur) {
+                            same = true;
+                            break;
+                        }
+                        if (x == (cur ^ 1)) {
+                            constFalse = true;
+                            break;
+                        }
+                    }
+                    if (constFalse) break;
+                    if (same) continue;
+                    const int id = lid(cur);
+                    if (cur != 2 * v && ((cur & 1) || id <= nPIs || nfo[id] > 1 || top + 2 >= kBalStack ||
+                                         (int)cv.size() + 2 * (top + 1) + 1 >= kBalMaxCover)) {
+                        cv.push_back(cur);
+                        continue;
+                    }
+                    stk[++top] = g.f1[id];
+                    stk[++top] = g.f0[id];
+                }
+                if (constFalse) cv.clear();
+                covLen[v] = (int)cv.size();
+            }
+            if (covLen[v] == 0) continue;  // constant false: inputs not followed
+            for (int x : cover[v])
+                if (lid(x) > nPIs) status[lid(x)] = 1;
+        }
+        list.clear();
+        for (int v = 0; v < nObjs; v++)
+            if (status[v]) list.push_back(v);
+        levelCount++;
+    }
+    // ---- phase 2: reconstruction
+    std::vector<int> covers;  // cover roots by (last level, id)
+    for (int v = 0; v < nObjs; v++)
+        if (covLen[v] >= 0) covers.push_back(v);
+    std::stable_sort(covers.begin(), covers.end(), [&](int a, int b) { return lastLevel[a] < lastLevel[b]; });
+    std::vector<int> newLit(nObjs, -1);  // per cover root: its reconstructed literal
+    std::unordered_map<uint64_t, unsigned> tab;  // key (lit0 < lit1) -> new id
+    std::unordered_map<unsigned, unsigned> lev;  // new id -> level
+    auto level_of = [&](int lit) -> int {
+        const unsigned id = (unsigned)lid(lit);
+        if ((int)id <= nPIs) return 0;
+        auto it = lev.find(id);
+        if (it == lev.end()) {
+            if (err) *err = "balance: level of a built node missing";
+            return 0;
+        }
+        return (int)it->second;
+    };
+    long long newIdCounter = nPIs + 1;
+    std::vector<size_t> lvEnd(levelCount + 1, 0);  // covers of level L: [lvEnd[L-1], lvEnd[L])
+    for (int v : covers) lvEnd[lastLevel[v]]++;
+    for (int L = 1; L < levelCount; L++) lvEnd[L] += lvEnd[L - 1];
+    for (int L = levelCount - 1; L >= 0; L--) {
+        const size_t pos = L ? lvEnd[L - 1] : 0, end = lvEnd[L];
+        for (size_t c0 = pos; c0 < end; c0 += kBalChunk) {
+            const int n = (int)std::min<size_t>(kBalChunk, end - c0);
+            // prepareReconstructArrays (balance.cu:272-426), sortDecId = 1
+            std::vector<std::vector<std::pair<int, int>>> arr(n);  // (literal, level)
+            for (int i = 0; i < n; i++) {
+                const int v = covers[c0 + i];
+                for (int x : cover[v]) {
+                    int nl;
+                    if (lid(x) <= nPIs)
+                        nl = x;
+                    else
+                        nl = newLit[lid(x)] ^ (x & 1);
+                    arr[i].push_back({nl, level_of(nl)});
+                }
+                std::sort(arr[i].begin(), arr[i].end(), [](const std::pair<int, int> &a, const std::pair<int, int> &b) {
+                    return a.second == b.second ? a.first > b.first : a.second > b.second;
+                });
+            }
+            // steps (balance.cu:1185-1234)
+            std::vector<int> mask(n);
+            std::vector<uint64_t> keys(n);
+            std::vector<unsigned> vals(n), lvls(n);
+            while (true) {
+                int maxMask = 0;
+                for (int i = 0; i < n; i++) {
+                    auto &a = arr[i];
+                    const int len = (int)a.size();
+                    mask[i] = 0;
+                    if (len <= 1) continue;
+                    // sharedNodeDrivenPermute (balance.cu:187-247)
+                    int left = 0;
+                    if (len >= 3) {
+                        left = len - 2;
+                        const int border = a[left].second;
+                        for (left--; left >= 0 && a[left].second == border; left--) {
+                        }
+                        left++;
+                    }
+                    const int right = len - 2;
+                    if (left < right) {
+                        const int l1 = a[right + 1].first, l2 = a[right].first;
+                        for (int k = right; k >= left; k--) {
+                            const int l3 = a[k].first;
+                            if (bal_lookup(l1, l3, tab) != kBalEmpty) {
+                                if (l3 != l2) std::swap(a[k], a[right]);
+                                break;
+                            }
+                        }
+                    }
+                    // prepareDataToInsert (balance.cu:113-184)
+                    int l1 = a[len - 1].first, l2 = a[len - 2].first;
+                    const int lv1 = a[len - 1].second, lv2 = a[len - 2].second;
+                    a.resize(len - 2);
+                    const unsigned got = bal_lookup(l1, l2, tab);
+                    if (got != kBalEmpty) {
+                        mask[i] = 2;
+                        vals[i] = got;
+                        lvls[i] = (unsigned)level_of((int)got);
+                    } else {
+                        if (l1 > l2) std::swap(l1, l2);
+                        mask[i] = 1;
+                        keys[i] = ((uint64_t)(uint32_t)l1 << 32) | (uint32_t)l2;
+                        vals[i] = (unsigned)(newIdCounter + i);
+                        lvls[i] = (unsigned)std::max(lv1, lv2) + 1;
+                    }
+                    maxMask = std::max(maxMask, mask[i]);
+                }
+                if (maxMask == 0) break;
+                // insert_batch_update_min_masked + retrieve_batch_masked
+                for (int i = 0; i < n; i++)
+                    if (mask[i] == 1) {
+                        auto it = tab.find(keys[i]);
+                        if (it == tab.end())
+                            tab[keys[i]] = vals[i];
+                        else
+                            it->second = std::min(it->second, vals[i]);
+                    }
+                unsigned maxId = 0;
+                for (int i = 0; i < n; i++)
+                    if (mask[i] == 1) {
+                        vals[i] = tab[keys[i]];
+                        maxId = std::max(maxId, vals[i]);
+                    }
+                if (maxId != 0) newIdCounter = (long long)maxId + 1;
+                for (int i = 0; i < n; i++)
+                    if (mask[i] == 1) {
+                        auto it = lev.find(vals[i]);
+                        if (it == lev.end())
+                            lev[vals[i]] = lvls[i];
+                        else
+                            it->second = std::min(it->second, lvls[i]);
+                    }
+                // addBackLocalArrays (balance.cu:429-467)
+                for (int i = 0; i < n; i++) {
+                    if (mask[i] == 0) continue;
+                    const int lit = mask[i] == 2 ? (int)vals[i] : (int)(vals[i] << 1);
+                    auto &a = arr[i];
+                    bool dup = false;
+                    for (auto &e : a)
+                        if (e.first == lit) {
+                            dup = true;
+                            break;
+                        }
+                    if (dup) continue;
+                    a.push_back({lit, (int)lvls[i]});
+                    for (int k = (int)a.size() - 1; k > 0 && a[k].second > a[k - 1].second; k--) std::swap(a[k], a[k - 1]);
+                }
+            }
+            // recordReconstructedCovers (balance.cu:469-491)
+            for (int i = 0; i < n; i++) {
+                const int v = covers[c0 + i];
+                newLit[v] = arr[i].empty() ? 1 : arr[i][0].first;
+            }
+        }
+    }
+    // renumbering in id order (balance.cu:1266-1300)
+    std::vector<std::pair<unsigned, uint64_t>> built;
+    built.reserve(tab.size());
+    for (auto &kv : tab) built.push_back({kv.second, kv.first});
+    std::sort(built.begin(), built.end());
+    std::unordered_map<unsigned, int> outId;
+    for (size_t k = 0; k < built.size(); k++) outId[built[k].first] = nPIs + 1 + (int)k;
+    auto map_lit = [&](unsigned lit) -> int {
+        const unsigned id = lit >> 1;
+        if ((int)id <= nPIs) return (int)lit;
+        return 2 * outId[id] + (int)(lit & 1);
+    };
+    r.nObjs = nPIs + 1 + (int)built.size();
+    r.f0.assign(r.nObjs, -1);
+    r.f1.assign(r.nObjs, -1);
+    for (size_t k = 0; k < built.size(); k++) {
+        const uint64_t key = built[k].second;
+        r.f0[nPIs + 1 + k] = map_lit((unsigned)(key >> 32));
+        r.f1[nPIs + 1 + k] = map_lit((unsigned)(key & 0xFFFFFFFFu));
+    }
+    // processPO (balance.cu:882-910)
+    r.outs.resize(nPOs);
+    for (int i = 0; i < nPOs; i++) {
+        const int o = g.outs[i];
+        if (lid(o) <= nPIs) {
+            r.outs[i] = o;
+            continue;
+        }
+        const int nl = newLit[lid(o)];
+        r.outs[i] = map_lit((unsigned)nl) ^ (o & 1);
+    }
+    r.nLevels = -1;  // the balance does not compute levels (aig_manager.cu:727)
+    return r;
+}
+
 struct Oracle {
     Lib lib;
     Graph g;
@@ -1176,6 +1468,23 @@ int orc_rw(void *h, int fUseZeros, int dedupMode) {
 int orc_st(void *h, int fCPU) {
     Oracle *o = (Oracle *)h;
     o->g = fCPU ? orc::strash_cpu(o->g) : orc::strash_gpu(o->g);
+    o->keepRw = false;
+    return 0;
+}
+
+// AIGMan::balance(sortDecId = 1, updateLevel) (src/aig_manager.cu:682-737):
+// balance, then a GPU strash when updateLevel (the `b` command).  Returns
+// -1 when the restatement met an inconsistency.
+int orc_b(void *h, int updateLevel) {
+    Oracle *o = (Oracle *)h;
+    if (o->g.nObjs - 1 - o->g.nPIs == 0) return 0;
+    std::string err;
+    orc::Graph r = orc::balance_core(o->g, &err);
+    if (!err.empty()) {
+        o->err = err;
+        return -1;
+    }
+    o->g = updateLevel ? orc::strash_gpu(r) : r;
     o->keepRw = false;
     return 0;
 }

@@ -47,6 +47,7 @@ def _load():
         lib.orc_set_graph.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ip, ip, ip]
         lib.orc_rw.argtypes = [vp, ctypes.c_int, ctypes.c_int]
         lib.orc_st.argtypes = [vp, ctypes.c_int]
+        lib.orc_b.argtypes = [vp, ctypes.c_int]
         lib.orc_get_sizes.argtypes = [vp, ip, ip, ip, ip]
         lib.orc_get_graph.argtypes = [vp, ip, ip, ip]
         lib.orc_dump_sizes.argtypes = [vp, ip, ip]
@@ -116,6 +117,12 @@ class Oracle:
 
     def st(self, cpu=False):
         self.lib.orc_st(self.h, int(cpu))
+
+    def b(self, update_level=True):
+        """`b` (balance, sortDecId 1), followed by a GPU-style strash when
+        update_level (the command's behaviour)."""
+        if self.lib.orc_b(self.h, int(update_level)) != 0:
+            raise RuntimeError("oracle balance: inconsistent state")
 
     def graph(self) -> Graph:
         a = [ctypes.c_int() for _ in range(4)]

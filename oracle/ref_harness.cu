@@ -10,8 +10,9 @@
 //       (command handlers src/command_manager.cpp:32-128).
 //   rw_harness chain <in.aig> <out.aig> <script>
 //       a command sequence on one AIGMan, script = comma-separated tokens
-//       rw | rwz | rwc | rwzc | st: AIGMan::rewrite(zeros = 'z',
-//       fGPUDeduplicate = no 'c') or AIGMan::strash(false, true), printing
+//       rw | rwz | rwc | rwzc | st | b | bn: AIGMan::rewrite(zeros = 'z',
+//       fGPUDeduplicate = no 'c'), AIGMan::strash(false, true), or
+//       AIGMan::balance(1, updateLevel = true for b, false for bn), printing
 //       the AND count and level after each, then AIGMan::saveFile.
 //   rw_harness dump <in.aig> <prefix>
 //       the first half of rw::CPUSolver::Rewrite (src/algorithms/
@@ -129,6 +130,10 @@ static int run_chain(const char *in, const char *out, const char *script) {
     while (std::getline(ss, tok, ',')) {
         if (tok == "st") {
             man.strash(false, true);
+        } else if (tok == "b") {
+            man.balance(1, true);  // the `b` command: balance, then strash
+        } else if (tok == "bn") {
+            man.balance(1, false);  // balance as resyn2 calls it, no strash
         } else if (tok.rfind("rw", 0) == 0) {
             const bool zeros = tok.find('z') != std::string::npos;
             const bool gpuDedup = tok.find('c') == std::string::npos;
