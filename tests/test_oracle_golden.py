@@ -18,7 +18,7 @@ import aigcanon
 from oracle.oracle import Graph, Oracle
 
 GOLDEN = Path(__file__).resolve().parent / "golden"
-CASES = sorted(p.stem for p in GOLDEN.glob("*.npz") if p.stem != "chains")
+CASES = sorted(p.stem for p in GOLDEN.glob("*.npz") if p.stem not in ("chains", "balance"))
 
 
 def load(name):
