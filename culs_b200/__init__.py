@@ -35,6 +35,7 @@ ERRORS = {-1: "CULS_E_INVALID", -2: "CULS_E_OOM", -3: "CULS_E_BUDGET", -4: "CULS
 RW_ZEROS, RW_GPU_DEDUP, RW_DUMP = 1, 2, 4
 SERVE_BYTES_PER_OBJ = 720  # device bytes the served mode's admission charges per object
 ST_CPU = 1
+B_NO_STRASH = 1
 STAT_NAMES = ["replaced", "replaced_pos", "replaced_zero", "reverted", "compromised", "pre_eval", "small_cut",
               "new_idx", "expected", "new_nodes", "candidates", "enum_warp_pairs"]
 DUMPS = ["reorder_f0", "reorder_f1", "reorder_out", "cuts", "selected", "replace", "new_f0", "new_f1", "choice"]
@@ -94,6 +95,7 @@ _lib.culs_fetch_aiger.argtypes = [_vp, ctypes.c_int64, _vp, ctypes.c_size_t, cty
 _lib.culs_graph_download.argtypes = [_vp, _vp, ctypes.c_int, _ip, _ip, _ip]
 _lib.culs_rw.argtypes = [_vp, _vp, ctypes.c_uint32]
 _lib.culs_st.argtypes = [_vp, _vp, ctypes.c_uint32]
+_lib.culs_b.argtypes = [_vp, _vp, ctypes.c_uint32]
 _lib.culs_rw_st.argtypes = [_vp, _vp, ctypes.c_uint32, ctypes.c_uint32]
 _lib.culs_rw_stats.argtypes = [_vp, ctypes.POINTER(ctypes.c_int64), ctypes.c_int]
 _lib.culs_dump_size.restype = ctypes.c_int64
@@ -259,6 +261,11 @@ class Context:
 
     def st(self, d, cpu=False):
         self._err(_lib.culs_st(self.h, d.h, ST_CPU if cpu else 0), "st")
+
+    def b(self, d, update_level=True):
+        """`b`: balance (sortDecId 1) every graph of d, then strash unless
+        update_level is False (the balance as resyn2 calls it)."""
+        self._err(_lib.culs_b(self.h, d.h, 0 if update_level else B_NO_STRASH), "b")
 
     def rw_st(self, d, zeros=False, gpu_dedup=True, cpu_st=False):
         f = (RW_ZEROS if zeros else 0) | (RW_GPU_DEDUP if gpu_dedup else 0)
@@ -502,6 +509,11 @@ class AIGMan:
 
     def strash(self, fCPU=False):
         self.ctx.st(self.dev, cpu=fCPU)
+
+    def balance(self, sortDecId=1, updateLevel=True):
+        if sortDecId != 1:
+            raise CulsError(CULS_E_INVALID, "balance: only sortDecId 1 (the `b` default) is provided")
+        self.ctx.b(self.dev, update_level=updateLevel)
 
     def printStats(self):
         s = self.dev.stats()

@@ -247,6 +247,14 @@ int culs_st(culs_ctx *ctx, culs_graph *g, uint32_t flags) {
     });
 }
 
+int culs_b(culs_ctx *ctx, culs_graph *g, uint32_t flags) {
+    return culs::guard_call(ctx ? &ctx->err : &g_err, [&]() -> int {
+        if (!ctx || !g || (flags & ~CULS_B_NO_STRASH)) return CULS_E_INVALID;
+        std::lock_guard<std::mutex> lk(ctx->mu);
+        return set_err(ctx, ctx->eng.balance(g->b, (flags & CULS_B_NO_STRASH) == 0));
+    });
+}
+
 int culs_rw_st(culs_ctx *ctx, culs_graph *g, uint32_t rwFlags, uint32_t stFlags) {
     return culs::guard_call(ctx ? &ctx->err : &g_err, [&]() -> int {
         int rc = culs_rw(ctx, g, rwFlags);

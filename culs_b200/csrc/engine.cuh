@@ -173,6 +173,9 @@ class Engine {
     int batch_depth(Batch &b);
     int rw(Batch &b, bool useZeros, bool gpuDedup, RwStats *stats, RwDump *dump);
     int st(Batch &b, bool cpuOrder);
+    // AIG balancing (`b`, sortDecId 1) of every graph of b, then a strash
+    // when updateLevel (balance.cu).
+    int balance(Batch &b, bool updateLevel);
     int sync();
 
     cudaStream_t stream() const { return s_; }
@@ -227,6 +230,8 @@ class Engine {
     int ensure_arena(size_t bytes);
     int ensure_stage(size_t ints);  // pinned host staging of at least `ints` int32
     ExecCtx ctx();
+    int balance_graph(const int *F0, const int *F1, const int *PO, int nPIs, int nPO, int nObj, int *F0n, int *F1n,
+                      int *POn, int *nAndsOut);
     void apply_spin_limit();
 
     // stage helpers

@@ -124,6 +124,16 @@ struct Shell {
         account(t0, t0, t1);
     }
 
+    void b() {
+        if (!loaded) return;
+        auto t0 = Clock::now();
+        int rc = culs_b(ctx, g, 0);
+        if (rc == CULS_OK) rc = culs_sync(ctx);
+        auto t1 = Clock::now();
+        report(rc, "b");
+        account(t0, t0, t1);
+    }
+
     void st(bool cpu) {
         if (!loaded) return;
         auto t0 = Clock::now();
@@ -185,9 +195,17 @@ void run_command(Shell &sh, const std::string &line) {
         bool seen[1] = {false};
         ok = parse_flags(lit, "c", seen);
         if (ok) sh.st(seen[0]);
-    } else if (cmd == "b" || cmd == "balance" || cmd == "rf" || cmd == "refactor" || cmd == "rs" ||
-               cmd == "resub" || cmd == "resyn2" || cmd == "resyn2rs" || cmd == "r2rs") {
-        printf("Command %s is not part of this library (rw and st only), ignored.\n", cmd.c_str());
+    } else if (cmd == "b" || cmd == "balance") {
+        bool seen[1] = {false};
+        ok = parse_flags(lit, "s", seen);
+        if (ok && seen[0]) {
+            printf("balance -s (seeded shuffle of equal-level inputs) is not provided, ignored.\n");
+            return;
+        }
+        if (ok) sh.b();
+    } else if (cmd == "rf" || cmd == "refactor" || cmd == "rs" || cmd == "resub" || cmd == "resyn2" ||
+               cmd == "resyn2rs" || cmd == "r2rs") {
+        printf("Command %s is not part of this library (rw, st and b only), ignored.\n", cmd.c_str());
         return;
     } else {
         printf("Command %s not registered, ignored.\n", cmd.c_str());

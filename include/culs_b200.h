@@ -148,6 +148,17 @@ int culs_rw(culs_ctx *ctx, culs_graph *g, uint32_t flags);
 /* `st` on every graph of the handle: AIGMan::strash(fCPU)
  * (src/aig/strash.cu:317-503, handler src/command_manager.cpp:115-128). */
 int culs_st(culs_ctx *ctx, culs_graph *g, uint32_t flags);
+/* `b` on every graph of the handle: AIGMan::balance(sortDecId = 1,
+ * updateLevel = true) (CULS src/aig_manager.cu:682-737 over
+ * balancePerformV2, src/algorithms/balance.cu:912-1382; handler
+ * src/command_manager.cpp:61-79): supergates rebuilt as balanced trees, then
+ * a strash.  With CULS_B_NO_STRASH the strash is left out, as resyn2 calls
+ * the balance (src/command_manager.cpp:151) -- the handle then reports the
+ * graph's depth as its level.  `b -s` (sortDecId 0, a seeded shuffle of
+ * equal-level inputs) is not provided: CULS_E_INVALID for any other flag.
+ * Drops the rewrite manager's kept graph. */
+#define CULS_B_NO_STRASH 1u
+int culs_b(culs_ctx *ctx, culs_graph *g, uint32_t flags);
 /* `rw; st` in one call (the rewrite-then-strash step of the reference's
  * scripts), on one graph or a whole batch. */
 int culs_rw_st(culs_ctx *ctx, culs_graph *g, uint32_t rwFlags, uint32_t stFlags);
