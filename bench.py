@@ -661,6 +661,24 @@ def our_arm(args, group):
     return 1 if bad else 0
 
 
+def once(args):
+    """One `rw; st` of the workload on a device-resident clone, nothing timed
+    or printed but a one-line summary: the command the committed ncu
+    summaries (profiles/) were captured from."""
+    import culs_b200 as C
+    ctx = C.Context()
+    graphs = make_workload(args.workload, 0)
+    d0 = ctx.upload_batch(graphs)
+    d = ctx.clone(d0)
+    ctx.rw_st(d)
+    ctx.sync()
+    print(json.dumps({"once": WORKLOAD_DESC.get(args.workload, args.workload), "graphs": len(graphs),
+                      "and_nodes": sum(g.nAnds for g in graphs),
+                      "and_nodes_out": sum(d.stats(i)["nAnds"] for i in range(len(d)))}), flush=True)
+    ctx.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -675,9 +693,13 @@ def main():
     ap.add_argument("--max-batch", type=int, default=0, help="c5: jobs per served batch at most (0: no cap)")
     ap.add_argument("--no-served", action="store_true",
                     help="c4: leave out the short served-mode run of the default line")
+    ap.add_argument("--once", action="store_true",
+                    help="one device-resident rw;st of the workload and exit (for profiler captures)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.once:
+        return once(args)
     group = Group()
     try:
         if args.impl == "reference":
