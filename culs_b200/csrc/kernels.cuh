@@ -159,14 +159,15 @@ __device__ __forceinline__ bool queue_round_end(bool fin, bool progressed, int64
 
 // Blocks for a persistent dataflow kernel over a batch `width` nodes wide
 // (Batch::flow_width): enough for about sixteen levels' worth of nodes in
-// flight at itemsPerBlock nodes per block, at least 8, at most `full`.  A
+// flight at itemsPerBlock nodes per block, at least minBlocks (one per SM:
+// a narrow graph's waits still spread over the SMs), at most `full`.  A
 // narrow, deep batch then leaves the rest of the GPU to other streams (the
 // served mode runs several batches at once) instead of filling every SM with
 // blocks that wait on its critical path.  Any grid is correct: chunks are
 // claimed in order by running blocks.
-inline unsigned flow_blocks(int64_t width, int itemsPerBlock, unsigned full) {
+inline unsigned flow_blocks(int64_t width, int itemsPerBlock, unsigned full, int minBlocks) {
     int64_t b = (16 * width + itemsPerBlock - 1) / itemsPerBlock;
-    if (b < 8) b = 8;
+    if (b < minBlocks) b = minBlocks;
     return (unsigned)(b < (int64_t)full ? b : (int64_t)full);
 }
 

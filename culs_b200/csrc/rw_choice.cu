@@ -188,6 +188,20 @@ __global__ void __launch_bounds__(kChoiceBlock) k_choice(ChoiceArgs A, int G) {
             na = A.recA[i + 1];
             nb = A.recB[i + 1];
         }
+        if (i + 1 < e && (na.z >> 1) >= 0) {
+            // the next candidate's first loads, into L1 while this one runs
+            // (a prefetch carries no value, so later stores cannot make it stale)
+            const int nn = na.z >> 1, nq = na.y;
+            asm volatile("prefetch.global.L1 [%0];" ::"l"(A.L0 + nn));
+            asm volatile("prefetch.global.L1 [%0];" ::"l"(A.L1 + nn));
+            asm volatile("prefetch.global.L1 [%0];" ::"l"(A.del + nn));
+            asm volatile("prefetch.global.L1 [%0];" ::"l"(A.L0 + nq));
+            asm volatile("prefetch.global.L1 [%0];" ::"l"(A.L1 + nq));
+            asm volatile("prefetch.global.L1 [%0];" ::"l"(A.del + nb.x));
+            asm volatile("prefetch.global.L1 [%0];" ::"l"(A.del + nb.y));
+            asm volatile("prefetch.global.L1 [%0];" ::"l"(A.del + nb.z));
+            asm volatile("prefetch.global.L1 [%0];" ::"l"(A.del + nb.w));
+        }
         const int c = a.x, q = a.y, rep = a.z;
         const int newIdx = rep >> 1;
         if (newIdx < 0) {
@@ -319,6 +333,9 @@ int rw_choice(ExecCtx &X, Batch &b, RwWork &w, RwStats *stats) {
     if ((rc = X.check(scan_exclusive(gCount, gStart, G, nullptr, ar, s), "scan"))) return rc;
     ChoiceArgs A{w.nL0, w.dg,   w.L0,   w.L1,     w.ref,    w.del,       recA,   recB,  gStart,
                  gCount, w.useZeros ? 1 : 0,    stack,  (int)stackCap,       w.choice, dstats, X.status};
+    // the walk's working set is the graph's fanins, flags and counts: the
+    // smallest shared-memory carveout leaves the most L1 for it
+    cudaFuncSetAttribute(k_choice, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
     k_choice<<<(G + kChoiceBlock - 1) / kChoiceBlock, kChoiceBlock, 0, s>>>(A, G);
     X.launched(1);
     unsigned long long hs[8], warpPairs = 0;

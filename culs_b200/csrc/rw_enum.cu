@@ -550,7 +550,7 @@ int rw_enumerate(ExecCtx &X, RwWork &w) {
     // a wide batch fills the GPU; a narrow one runs about sixteen levels'
     // worth of chunks at a time (32 nodes a warp on wide levels, 1 on narrow)
     const int perBlock = (kEnumBlock / 32) * (w.width >= X.tune->enumWideMin ? 32 : 1);
-    k_enumerate<<<flow_blocks(w.width, perBlock, (unsigned)(X.sms * X.tune->enumBlocksPerSm)), kEnumBlock, 0, s>>>(A);
+    k_enumerate<<<flow_blocks(w.width, perBlock, (unsigned)(X.sms * X.tune->enumBlocksPerSm), X.sms), kEnumBlock, 0, s>>>(A);
     X.mark(kMkEnumK1);
     X.launched(6);
     if ((rc = X.check(cudaGetLastError(), "enumerate launch"))) return rc;

@@ -196,7 +196,7 @@ int rw_front(ExecCtx &X, Batch &b, RwWork &w) {
     ChunkSched sched;
     if ((rc = build_chunk_sched(X, b, kBlock, sched))) return rc;
     k_front_load<<<X.grid(N), kBlock, 0, s>>>(N, G, b.dg, b.F0, b.F1, gidIn, a0, a1, lp, done);
-    k_front_levelize<<<flow_blocks(w.width, kBlock, (unsigned)(X.sms * 8)), kBlock, 0, s>>>(sched, a0, a1, lp, done, cnt + 0, cnt + 1, X.status);
+    k_front_levelize<<<flow_blocks(w.width, kBlock, (unsigned)(X.sms * 8), X.sms), kBlock, 0, s>>>(sched, a0, a1, lp, done, cnt + 0, cnt + 1, X.status);
     k_front_keys<<<X.grid(N), kBlock, 0, s>>>(N, lp, keys, vals);
     X.launched(3);
     if ((rc = X.check(cudaMemcpyAsync(X.hostSmall, cnt, sizeof(int) * 8, cudaMemcpyDeviceToHost, s), "d2h"))) return rc;

@@ -574,7 +574,7 @@ int Engine::strash_core(Batch &b, int64_t M, const int *L0, const int *L1, const
         return fail(CULS_E_OOM, "strash: scratch arena exhausted");
     int *qc = counters_;  // [0]=head [1]=tail [2]=done [3]=count [4]=maxLevel [5]=counter
     const unsigned gridM = grid_1d(std::max<int64_t>(M, nPO), kBlock, sms_ * 16);
-    const unsigned gridQ = flow_blocks(b.flow_width(), kBlock, (unsigned)(sms_ * 8));
+    const unsigned gridQ = flow_blocks(b.flow_width(), kBlock, (unsigned)(sms_ * 8), sms_);
 
     // 1. liveness
     check(cudaMemsetAsync(dead, 0, (size_t)M + 1, s), "memset");
@@ -905,7 +905,7 @@ int Engine::batch_depth(Batch &b) {
     if ((rc = check(cudaMemsetAsync(dead, 0, (size_t)N + 1, s), "memset"))) return rc;
     k_depth_prep<<<X.grid(N), kBlock, 0, s>>>(N, G, b.dg, b.F0, b.F1, L0, L1, gid);
     k_live_flags<<<X.grid(N), kBlock, 0, s>>>(N, L0, dead, live, done);
-    k_st_levelize<<<flow_blocks(b.flow_width(), kBlock, (unsigned)(sms_ * 8)), kBlock, 0, s>>>(sched, L0, L1, live, gid, level, done, graphLevels, qc + 5,
+    k_st_levelize<<<flow_blocks(b.flow_width(), kBlock, (unsigned)(sms_ * 8), sms_), kBlock, 0, s>>>(sched, L0, L1, live, gid, level, done, graphLevels, qc + 5,
                                                           qc + 4, status_);
     launches_ += 3;
     std::vector<int> hl(G);

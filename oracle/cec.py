@@ -1,0 +1,109 @@
+"""Combinational equivalence check of two AIGs by SAT sweeping with z3.
+
+TEST INFRASTRUCTURE.  ABC's `cec` (which BASELINE.json's north_star names)
+cannot be built here: the reference's ABC submodule is empty.  This is the
+substitute the survey planned, reported under its own name ("z3 SAT-sweeping
+CEC"), not as ABC:
+
+1. both AIGs (AIGMan convention: literal 0 = TRUE) share their PIs and are
+   simulated on random 64-bit patterns, every node of both;
+2. every node of the second AIG whose simulation signature equals that of a
+   node of the first (or its complement) is a candidate pair;
+3. one incremental z3 solver holds the Tseitin encoding of both AIGs; the
+   candidate pairs are proved in topological order of the second AIG, each
+   proved pair added as an equality (so later proofs see both cones merged,
+   which keeps each query local), a refuted pair simply left out;
+4. the outputs are equivalent when, for every PO pair, z3 finds no input
+   assignment that tells them apart (UNSAT).
+
+Returns a dict: equivalent (True only when every PO pair is proved), the
+counts of candidate pairs proved and refuted, the PO pairs proved, and the
+time taken.
+"""
+import time
+
+import numpy as np
+
+
+def _simulate_all(g, words, seed):
+    """Values of every object of g (AIGMan literals) under `words` x 64
+    random patterns: uint64 array [nObjs, words] (object 0 = TRUE)."""
+    n = len(g.fanin0)
+    rng = np.random.default_rng(seed)
+    val = np.zeros((n, words), np.uint64)
+    val[0] = np.uint64(0xFFFFFFFFFFFFFFFF)
+    val[1:g.nPIs + 1] = rng.integers(0, 2 ** 64, (g.nPIs, words), dtype=np.uint64)
+    f0 = np.asarray(g.fanin0)
+    f1 = np.asarray(g.fanin1)
+    full = np.uint64(0xFFFFFFFFFFFFFFFF)
+    for v in range(g.nPIs + 1, n):
+        a, b = int(f0[v]), int(f1[v])
+        x = val[a >> 1] ^ (full if a & 1 else np.uint64(0))
+        y = val[b >> 1] ^ (full if b & 1 else np.uint64(0))
+        val[v] = x & y
+    return val
+
+
+def cec(a, b, words=8, seed=1, max_pairs=None):
+    import z3
+    t0 = time.time()
+    if a.nPIs != b.nPIs or len(a.outs) != len(b.outs):
+        return {"equivalent": False, "reason": "interfaces differ", "seconds": time.time() - t0}
+    va = _simulate_all(a, words, seed)
+    vb = _simulate_all(b, words, seed)
+    full = np.uint64(0xFFFFFFFFFFFFFFFF)
+    s = z3.Solver()
+    pis = [z3.BoolVal(True)] + [z3.Bool(f"i{k}") for k in range(1, a.nPIs + 1)]
+
+    def encode(g, tag):
+        xs = list(pis) + [None] * (len(g.fanin0) - g.nPIs - 1)
+        for v in range(g.nPIs + 1, len(g.fanin0)):
+            x = z3.Bool(f"{tag}{v}")
+            l0, l1 = int(g.fanin0[v]), int(g.fanin1[v])
+            p = xs[l0 >> 1] if not l0 & 1 else z3.Not(xs[l0 >> 1])
+            q = xs[l1 >> 1] if not l1 & 1 else z3.Not(xs[l1 >> 1])
+            s.add(x == z3.And(p, q))
+            xs[v] = x
+        return xs
+
+    xa = encode(a, "a")
+    xb = encode(b, "b")
+
+    def lit(xs, l):
+        return xs[l >> 1] if not l & 1 else z3.Not(xs[l >> 1])
+
+    # candidate pairs: signature of a node of b equal to a node of a (or its complement)
+    sig = {}
+    for v in range(len(a.fanin0)):
+        sig.setdefault(va[v].tobytes(), (v, 0))
+    for v in range(len(a.fanin0)):
+        sig.setdefault((va[v] ^ full).tobytes(), (v, 1))
+    proved = refuted = 0
+    for v in range(b.nPIs + 1, len(b.fanin0)):
+        c = sig.get(vb[v].tobytes())
+        if c is None:
+            continue
+        if max_pairs is not None and proved + refuted >= max_pairs:
+            break
+        u, comp = c
+        ea = xa[u] if not comp else z3.Not(xa[u])
+        s.push()
+        s.add(ea != xb[v])
+        r = s.check()
+        s.pop()
+        if r == z3.unsat:
+            s.add(ea == xb[v])
+            proved += 1
+        else:
+            refuted += 1
+    po_proved = 0
+    for oa, ob in zip(a.outs, b.outs):
+        s.push()
+        s.add(lit(xa, int(oa)) != lit(xb, int(ob)))
+        r = s.check()
+        s.pop()
+        if r == z3.unsat:
+            po_proved += 1
+    return {"equivalent": po_proved == len(a.outs), "pos": len(a.outs), "pos_proved": po_proved,
+            "pairs_proved": proved, "pairs_refuted": refuted, "seconds": round(time.time() - t0, 2),
+            "method": "z3 SAT-sweeping CEC (simulation candidates, incremental proofs)"}

@@ -1,0 +1,52 @@
+"""Proves `rw; st` and `b` equivalence-preserving on the single-graph
+configurations with the z3 SAT-sweeping CEC (oracle/cec.py, the substitute
+for ABC `cec`, which cannot be built here), and records the outcome in
+tests/golden/cec.json.  Runs on the CPU (minutes):
+
+    python tests/golden/run_cec.py
+
+The graphs checked are the oracle's results, which the GPU tests show equal
+to the CUDA path's node for node (tests/test_gpu_parity.py,
+tests/test_balance.py), so the proof covers both.
+"""
+import json
+import sys
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parents[2]
+sys.path.insert(0, str(ROOT))
+sys.path.insert(0, str(ROOT / "tests"))
+import culs_b200 as C  # noqa: E402  (generators only)
+from oracle.cec import cec  # noqa: E402
+from oracle.oracle import Oracle  # noqa: E402
+from util import to_oracle  # noqa: E402
+
+CASES = {
+    "c1_layered5k (configs[0])": lambda: C.gen_layered(1, 64, 32, 5000, 40, 4, 0.0, True),
+    "c2_mult64 (configs[1])": lambda: C.gen_multiplier(64),
+}
+
+
+def run(g, ops):
+    o = Oracle()
+    o.set_graph(to_oracle(g))
+    for op in ops:
+        op(o)
+    return o.graph()
+
+
+def main():
+    out = {}
+    for name, make in CASES.items():
+        g = make()
+        for flow, ops in [("rw;st", [lambda o: o.rw(), lambda o: o.st()]), ("b", [lambda o: o.b()])]:
+            r = run(g, ops)
+            res = cec(to_oracle(g), r, words=32)
+            res.update({"and_in": g.nAnds, "and_out": r.nAnds, "level_out": r.nLevels})
+            out[f"{name} {flow}"] = res
+            print(name, flow, res, flush=True)
+    (Path(__file__).resolve().parent / "cec.json").write_text(json.dumps(out, indent=1) + "\n")
+
+
+if __name__ == "__main__":
+    main()
