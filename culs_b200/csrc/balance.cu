@@ -30,7 +30,7 @@
 // are invisible.  A chunk needs at most (longest cover - 1) steps, known on
 // the host from phase 1, so steps are launched back to back.
 //
-// Phase 3 renumbers the built nodes in id order (balance.cu:1266-1300) and
+// Phase 3 renumbers the built nodes in id order (balance.cu:1285-1318) and
 // maps the POs (balance.cu:882-910).  Graphs of a batch are balanced one
 // after another; `b` then strashes the batch (AIGMan::balance with
 // updateLevel).
@@ -46,7 +46,7 @@ namespace {
 
 constexpr int kBalMaxCover = 1024;  // MAX_LOCAL_COVER_SIZE, balance.cu:17
 constexpr int kBalStack = 128;      // DFS_COVER_STACK_SIZE, balance.cu:18
-constexpr int kBalChunk = 32768;    // iterLen, balance.cu:1122
+constexpr int kBalChunk = 32768;    // iterLen, balance.cu:1125
 constexpr int kBalLocal = 32;       // leaves a DFS keeps in registers
 constexpr int kBalBigThreads = 2048;  // threads (each with a 1,024-leaf buffer) for the large covers
 constexpr int kBalLevelsPerSync = 16;
@@ -625,7 +625,7 @@ int Engine::balance_graph(const int *F0, const int *F1, const int *PO, int nPIs,
         return fail(CULS_E_OOM, "balance: arena exhausted");
     k_bal_init_tables<<<grid_1d(std::max<int64_t>(rCap, lCap), kBlock, sms_ * 16), kBlock, 0, s>>>(T, rCap, lCap);
     {
-        // the counter before the first step: nPIs + 1 (balance.cu:1154)
+        // the counter before the first step: nPIs + 1 (balance.cu:1167)
         const int init[8] = {0, 0, 0, nPIs + 1, 0, 0, 0, 0};
         check(cudaMemcpyAsync(C.ctr, init, sizeof init, cudaMemcpyHostToDevice, s), "h2d");
     }

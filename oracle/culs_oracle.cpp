@@ -1081,17 +1081,17 @@ static Graph dedup_cpu(const Graph &g) {
 // AIGMan::balance, src/aig_manager.cu:682-737), sortDecId = 1 (the `b`
 // default: inputs sorted by decreasing level, then decreasing literal).
 // Sequential restatement of the reference's two phases:
-//  1. cover finding, level by level from the POs (balance.cu:953-1029):
+//  1. cover finding, level by level from the POs (balance.cu:970-1039):
 //     the next level is every AND input of the covers of this level, in
 //     increasing id order; a node's cover is its supergate, collected by the
 //     DFS of localCoverTravToTable (balance.cu:666-751), and its "last
 //     appear level" the last level it is listed on;
-//  2. reconstruction, deepest covers first (balance.cu:1157-1248): covers of
+//  2. reconstruction, deepest covers first (balance.cu:1175-1283): covers of
 //     one level in increasing node id, in chunks of 32,768; all covers of a
 //     chunk pair their two lowest inputs in lockstep steps against one table
 //     of built nodes (existing pairs are reused, new ones get id counter +
 //     cover index, the smallest id of a key wins), and finally nodes are
-//     renumbered in id order (balance.cu:1271-1300).
+//     renumbered in id order (balance.cu:1285-1318).
 // The reference is deterministic here: duplicate keys inside a step resolve
 // by atomicMin and every other step is order independent.
 static const int kBalMaxCover = 1024;   // MAX_LOCAL_COVER_SIZE
@@ -1236,7 +1236,7 @@ static Graph balance_core(const Graph &g, std::string *err) {
                     return a.second == b.second ? a.first > b.first : a.second > b.second;
                 });
             }
-            // steps (balance.cu:1185-1234)
+            // steps (balance.cu:1207-1262)
             std::vector<int> mask(n);
             std::vector<uint64_t> keys(n);
             std::vector<unsigned> vals(n), lvls(n);
@@ -1333,7 +1333,7 @@ static Graph balance_core(const Graph &g, std::string *err) {
             }
         }
     }
-    // renumbering in id order (balance.cu:1266-1300)
+    // renumbering in id order (balance.cu:1285-1318)
     std::vector<std::pair<unsigned, uint64_t>> built;
     built.reserve(tab.size());
     for (auto &kv : tab) built.push_back({kv.second, kv.first});
