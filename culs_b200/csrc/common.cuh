@@ -53,6 +53,15 @@ CULS_DEV int ld_acquire(const int *p) {
     return v;
 }
 CULS_DEV void st_release(int *p, int v) { asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory"); }
+// Relaxed GPU-scope accesses, for a word that is itself the published value
+// (a level): the reader uses nothing else the writer stored before it, so
+// coherence of the one word is all the ordering needed.
+CULS_DEV int ld_relaxed(const int *p) {
+    int v;
+    asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+CULS_DEV void st_relaxed(int *p, int v) { asm volatile("st.relaxed.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory"); }
 CULS_DEV int ld_cg(const int *p) { return __ldcg(p); }
 CULS_DEV int4 ld_cg(const int4 *p) { return __ldcg(p); }
 CULS_DEV int2 ld_cg(const int2 *p) { return __ldcg(p); }
@@ -88,6 +97,8 @@ inline unsigned long long at_cas(unsigned long long *p, unsigned long long cmp, 
 }
 inline int ld_acquire(const int *p) { return *p; }
 inline void st_release(int *p, int v) { *p = v; }
+inline int ld_relaxed(const int *p) { return *p; }
+inline void st_relaxed(int *p, int v) { *p = v; }
 inline int ld_cg(const int *p) { return *p; }
 inline void set_status(int *status, int code) {
     if (*status == 0) *status = code;
@@ -121,6 +132,31 @@ CULS_HD bool wait_ge(const int *flag, int target, int *status) {
         }
         backoff(it);
         if (ld_acquire(flag) >= target) return true;
+    }
+}
+
+// Waits until the word *w is at least `floor` and returns it in *val: the
+// same bounds as wait_ge, with relaxed loads, for a word that carries its
+// own payload (see ld_relaxed).
+CULS_HD bool wait_word(const int *w, int floor, int *status, int *val) {
+    int v = ld_relaxed(w);
+    if (v >= floor) {
+        *val = v;
+        return true;
+    }
+    const int64_t lim = spin_limit(status);
+    for (int64_t it = 1;; ++it) {
+        if ((it & 31) == 1 && ld_cg(status) != kDevOk) return false;
+        if (it >= lim) {
+            set_status(status, kDevWaitTimeout);
+            return false;
+        }
+        backoff(it);
+        v = ld_relaxed(w);
+        if (v >= floor) {
+            *val = v;
+            return true;
+        }
     }
 }
 

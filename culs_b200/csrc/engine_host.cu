@@ -317,6 +317,7 @@ ExecCtx Engine::ctx() {
     X.hostSmall = hostSmall_;
     X.lib = lib_;
     X.sms = sms_;
+    X.clusters = ownStream_;
     X.launches = &launches_;
     X.err = &err_;
     X.ev = prof_ ? ev_ : nullptr;

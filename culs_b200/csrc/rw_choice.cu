@@ -3,9 +3,10 @@
 // rewrite.h:118-124,208-220) moved onto the GPU.
 //
 // Choice: one thread per graph walks that graph's candidates in id order and
-// replays install / FastDelete with explicit stacks that follow the
-// reference's recursion step by step (FastDelete's order of reference-count
-// updates matters when a cone reaches a node along two paths).  The walk is
+// replays FastDelete with an explicit stack that follows the reference's
+// recursion step by step (its order of reference-count updates matters when
+// a cone reaches a node along two paths: a node can be deleted twice) and
+// install with a worklist (its outcome does not depend on the order).  The walk is
 // a chain of dependent memory accesses, so it is written to shorten that
 // chain: each candidate's record (node, replacement, cut leaves) is gathered
 // beforehand in graph order and read one candidate ahead; the loads a
@@ -13,7 +14,9 @@
 // frame carries its node's two fanins, the top frame lives in registers and
 // the next ones in shared memory; reference-count updates whose old value is
 // not needed are fire-and-forget atomics (a thread's own later loads of the
-// same word observe them).
+// same word observe them).  A single graph of up to 65,536 objects runs on a
+// thread-block cluster instead, with its arrays in the blocks' distributed
+// shared memory (k_choice_cluster).
 //
 // Redundancy removal chases buffer chains.  The reference does it in one
 // sequential sweep in which a node's fanins, once rewritten, can make it
@@ -23,8 +26,13 @@
 // because a node's outcome depends only on nodes with smaller ids.
 #include <algorithm>
 #include <climits>
+#include <cstdlib>
+
+#include <cooperative_groups.h>
 
 #include "rw_work.cuh"
+
+namespace cg = cooperative_groups;
 
 namespace culs {
 
@@ -48,94 +56,180 @@ struct ChoiceArgs {
     int *status;
 };
 
-// frame {node, step | count << 2, fanin0 literal, fanin1 literal}; frames
-// below kChoiceFrames in shared memory, deeper ones in the graph's global
-// stack
+// The graph arrays the walk reads and writes.  GlobalMem: the arrays in HBM
+// (one thread per graph of a batch).  ClusterMem: for a single graph small
+// enough, the same arrays copied into the distributed shared memory of a
+// thread-block cluster, object x at offset x & mask of block x >> shift, so
+// that every access of the walk's dependent chain is a shared-memory access
+// of this SM or a neighbour instead of an L2 round trip.  Only one thread
+// walks, so the reference-count updates need no atomicity there; they stay
+// atomics because a fire-and-forget `red` does not stall the thread.
+struct GlobalMem {
+    int *L0, *L1, *ref;
+    uint8_t *del;
+    __device__ __forceinline__ int l0(int x) const { return L0[x]; }
+    __device__ __forceinline__ int l1(int x) const { return L1[x]; }
+    __device__ __forceinline__ int dl(int x) const { return del[x]; }
+    __device__ __forceinline__ int rf(int x) const { return ref[x]; }
+    __device__ __forceinline__ void set_del(int x, int v) const { del[x] = (uint8_t)v; }
+    __device__ __forceinline__ void set_fanins(int x, int a, int b) const {
+        L0[x] = a;
+        L1[x] = b;
+    }
+    __device__ __forceinline__ void rf_add(int x, int d) const { atomicAdd(ref + x, d); }
+    __device__ __forceinline__ int rf_add_old(int x, int d) const { return atomicAdd(ref + x, d); }
+    // del (or ref) and both fanins of x
+    __device__ __forceinline__ void dab(int x, int &d, int &a, int &b) const {
+        d = del[x];
+        a = L0[x];
+        b = L1[x];
+    }
+    __device__ __forceinline__ void rab(int x, int &r, int &a, int &b) const {
+        r = ref[x];
+        a = L0[x];
+        b = L1[x];
+    }
+    __device__ __forceinline__ void ab(int x, int &a, int &b) const {
+        a = L0[x];
+        b = L1[x];
+    }
+    static constexpr bool kPrefetch = true;
+};
+
+struct ClusterMem {
+    int4 *rec;  // this block's slice of {L0, L1, ref, del}; every block of the cluster has it at the same offset
+    int shift, mask;
+    __device__ __forceinline__ int4 *at(int x) const {
+        return cg::this_cluster().map_shared_rank(rec + (x & mask), (unsigned)(x >> shift));
+    }
+    __device__ __forceinline__ int l0(int x) const { return at(x)->x; }
+    __device__ __forceinline__ int l1(int x) const { return at(x)->y; }
+    __device__ __forceinline__ int dl(int x) const { return at(x)->w; }
+    __device__ __forceinline__ int rf(int x) const { return at(x)->z; }
+    __device__ __forceinline__ void set_del(int x, int v) const { at(x)->w = v; }
+    __device__ __forceinline__ void set_fanins(int x, int a, int b) const {
+        *reinterpret_cast<int2 *>(at(x)) = make_int2(a, b);
+    }
+    __device__ __forceinline__ void rf_add(int x, int d) const { atomicAdd(&at(x)->z, d); }
+    __device__ __forceinline__ int rf_add_old(int x, int d) const { return atomicAdd(&at(x)->z, d); }
+    __device__ __forceinline__ void dab(int x, int &d, int &a, int &b) const {
+        const int4 r = *at(x);
+        d = r.w;
+        a = r.x;
+        b = r.y;
+    }
+    __device__ __forceinline__ void rab(int x, int &f, int &a, int &b) const {
+        const int4 r = *at(x);
+        f = r.z;
+        a = r.x;
+        b = r.y;
+    }
+    __device__ __forceinline__ void ab(int x, int &a, int &b) const {
+        const int2 r = *reinterpret_cast<const int2 *>(at(x));
+        a = r.x;
+        b = r.y;
+    }
+    static constexpr bool kPrefetch = false;
+};
+
+// Stack frames: FastDelete's {node, step | count << 2, fanin0 literal,
+// fanin1 literal}, install's {node, fanin0 literal, fanin1 literal, 0};
+// frames below kChoiceFrames in shared memory (sh[sp * stride]), deeper ones
+// in the graph's global stack.  The scalars the walk reads at every node are copies held here: read
+// through the argument block, they would be reloaded after every store the
+// compiler cannot tell apart from it.
+template <class Mem>
 struct GraphCtx {
     const ChoiceArgs *A;
+    Mem m;
     int trueLit;
-    int4 (*sh)[kChoiceBlock];
-    int lane;
+    int4 *sh;
+    int stride;
     int4 *stk;
+    int64_t nL0;
+    int stackCap;
+    int *status;
     __device__ __forceinline__ void push(int sp, int4 f) const {
         if (sp < kChoiceFrames)
-            sh[sp][lane] = f;
+            sh[sp * stride] = f;
         else
             stk[sp] = f;
     }
-    __device__ __forceinline__ int4 pop(int sp) const { return sp < kChoiceFrames ? sh[sp][lane] : stk[sp]; }
+    __device__ __forceinline__ int4 pop(int sp) const { return sp < kChoiceFrames ? sh[sp * stride] : stk[sp]; }
 };
 
-__device__ __forceinline__ int ch_red(const GraphCtx &C, int x, int l0, int l1) {
-    return x >= C.A->nL0 && (l0 == l1 || l0 == C.trueLit);
+template <class Mem>
+__device__ __forceinline__ int ch_red(const GraphCtx<Mem> &C, int x, int l0, int l1) {
+    return x >= C.nL0 && (l0 == l1 || l0 == C.trueLit);
 }
-__device__ __forceinline__ void ref_add(int *ref, int x, int d) { atomicAdd(ref + x, d); }
 
-// A pushed frame's two fanins are read together: their (del or ref, L0,
-// L1).  L0 and L1 do not change during install / FastDelete, and del / ref
-// of the second fanin change only inside the first fanin's subtree, so the
-// second fanin is read again only when its frame resumes after that
-// subtree.
+// A pushed FastDelete frame's two fanins are read together: their (ref, L0,
+// L1).  L0 and L1 do not change during FastDelete, and the ref of the second
+// fanin changes only inside the first fanin's subtree, so the second fanin
+// is read again only when its frame resumes after that subtree.
 
-// install lambda, rewrite.cu:835-847; rootDel, r0, r1 = del, L0, L1 of root
-__device__ int ch_install(const GraphCtx &C, int root, int rootDel, int r0, int r1) {
-    const ChoiceArgs &A = *C.A;
+// install lambda, rewrite.cu:835-847; rootDel, r0, r1 = del, L0, L1 of root.
+// Whether a node is installed depends only on the deletion flags, which the
+// walk clears as it reaches nodes, and install reads no reference count, so
+// every visiting order installs the same nodes, makes the same increments
+// and returns the same count: a worklist (a node's deleted fanins are
+// cleared and queued when the node is taken) instead of the recursion.
+template <class Mem>
+__device__ int ch_install(const GraphCtx<Mem> &C, int root, int rootDel, int r0, int r1) {
+    const Mem &m = C.m;
     if (!rootDel) return 0;
-    A.del[root] = 0;
-    int4 f = make_int4(root, (1 - ch_red(C, root, r0, r1)) << 2, r0, r1);
-    int d0 = A.del[r0 >> 1], a0 = A.L0[r0 >> 1], b0 = A.L1[r0 >> 1];
-    int d1 = A.del[r1 >> 1], a1 = A.L0[r1 >> 1], b1 = A.L1[r1 >> 1];
-    int sp = 0;
+    m.set_del(root, 0);
+    int cnt = 0, sp = 0;
+    int x = root, l0 = r0, l1 = r1;
     while (true) {
-        const int step = f.y & 3;
-        if (step < 2) {
-            const int child = (step == 0 ? f.z : f.w) >> 1;
-            const int d = step == 0 ? d0 : d1, c0 = step == 0 ? a0 : a1, c1 = step == 0 ? b0 : b1;
-            f.y++;
-            if (d) {
-                if (sp + 1 >= A.stackCap) {
-                    set_status(A.status, kDevStackOverflow);
-                    return 0;
-                }
-                A.del[child] = 0;
-                C.push(sp++, f);
-                f = make_int4(child, (1 - ch_red(C, child, c0, c1)) << 2, c0, c1);
-                d0 = A.del[c0 >> 1], a0 = A.L0[c0 >> 1], b0 = A.L1[c0 >> 1];
-                d1 = A.del[c1 >> 1], a1 = A.L0[c1 >> 1], b1 = A.L1[c1 >> 1];
+        cnt += 1 - ch_red(C, x, l0, l1);
+        const int c0 = l0 >> 1, c1 = l1 >> 1;
+        int d0, a0, b0, d1, a1, b1;
+        m.dab(c0, d0, a0, b0);
+        m.dab(c1, d1, a1, b1);
+        m.rf_add(c0, 1);
+        m.rf_add(c1, 1);
+        if (d1 && c1 != c0) {
+            if (sp + 1 >= C.stackCap) {
+                set_status(C.status, kDevStackOverflow);
+                return 0;
             }
-            continue;
+            m.set_del(c1, 0);
+            C.push(sp++, make_int4(c1, a1, b1, 0));
         }
-        ref_add(A.ref, f.z >> 1, 1);
-        ref_add(A.ref, f.w >> 1, 1);
-        const int cnt = f.y >> 2;
-        if (sp == 0) return cnt;
-        f = C.pop(--sp);
-        f.y += cnt << 2;
-        if ((f.y & 3) == 1) {  // resumes at fanin 1 after fanin 0's subtree
-            const int c = f.w >> 1;
-            d1 = A.del[c], a1 = A.L0[c], b1 = A.L1[c];
+        if (d0) {
+            m.set_del(c0, 0);
+            x = c0, l0 = a0, l1 = b0;
+        } else if (sp > 0) {
+            const int4 f = C.pop(--sp);
+            x = f.x, l0 = f.y, l1 = f.z;
+        } else {
+            return cnt;
         }
     }
 }
 
 // FastDelete's two reference-count decrements of a frame's fanins, whose
 // returned values give the fanins' counts; L0 / L1 of both fanins
-__device__ __forceinline__ void fd_open(const ChoiceArgs &A, int l0, int l1, int &v0, int &a0, int &b0, int &v1, int &a1,
+template <class Mem>
+__device__ __forceinline__ void fd_open(const Mem &m, int l0, int l1, int &v0, int &a0, int &b0, int &v1, int &a1,
                                         int &b1) {
     const int c0 = l0 >> 1, c1 = l1 >> 1;
-    const int o0 = atomicAdd(A.ref + c0, -1);
-    const int o1 = atomicAdd(A.ref + c1, -1);
-    a0 = A.L0[c0], b0 = A.L1[c0], a1 = A.L0[c1], b1 = A.L1[c1];
+    const int o0 = m.rf_add_old(c0, -1);
+    const int o1 = m.rf_add_old(c1, -1);
+    m.ab(c0, a0, b0);
+    m.ab(c1, a1, b1);
     v1 = o1 - 1;
     v0 = c0 == c1 ? v1 : o0 - 1;  // one node twice: both decrements precede the first check
 }
 
 // FastDelete, rewrite.h:208-220; r0, r1 = L0, L1 of root
-__device__ int ch_fast_delete(const GraphCtx &C, int root, int r0, int r1) {
-    const ChoiceArgs &A = *C.A;
-    if (root < A.nL0) return 0;
+template <class Mem>
+__device__ int ch_fast_delete(const GraphCtx<Mem> &C, int root, int r0, int r1) {
+    const Mem &m = C.m;
+    if (root < C.nL0) return 0;
     int v0, a0, b0, v1, a1, b1;
-    fd_open(A, r0, r1, v0, a0, b0, v1, a1, b1);
+    fd_open(m, r0, r1, v0, a0, b0, v1, a1, b1);
     int4 f = make_int4(root, 1 | ((1 - ch_red(C, root, r0, r1)) << 2), r0, r1);
     int sp = 0;
     while (true) {
@@ -144,51 +238,54 @@ __device__ int ch_fast_delete(const GraphCtx &C, int root, int r0, int r1) {
             const int child = (step == 1 ? f.z : f.w) >> 1;
             const int r = step == 1 ? v0 : v1, c0 = step == 1 ? a0 : a1, c1 = step == 1 ? b0 : b1;
             f.y++;
-            if (r == 0 && child >= A.nL0) {
-                if (sp + 1 >= A.stackCap) {
-                    set_status(A.status, kDevStackOverflow);
+            if (r == 0 && child >= C.nL0) {
+                if (sp + 1 >= C.stackCap) {
+                    set_status(C.status, kDevStackOverflow);
                     return 0;
                 }
-                fd_open(A, c0, c1, v0, a0, b0, v1, a1, b1);
+                fd_open(m, c0, c1, v0, a0, b0, v1, a1, b1);
                 C.push(sp++, f);
                 f = make_int4(child, 1 | ((1 - ch_red(C, child, c0, c1)) << 2), c0, c1);
             }
             continue;
         }
-        A.del[f.x] = 1;
+        m.set_del(f.x, 1);
         const int cnt = f.y >> 2;
         if (sp == 0) return cnt;
         f = C.pop(--sp);
         f.y += cnt << 2;
         if ((f.y & 3) == 2) {  // resumes at fanin 1 after fanin 0's subtree
             const int c = f.w >> 1;
-            v1 = A.ref[c], a1 = A.L0[c], b1 = A.L1[c];
+            m.rab(c, v1, a1, b1);
         }
     }
 }
 
-__global__ void __launch_bounds__(kChoiceBlock) k_choice(ChoiceArgs A, int G) {
-    __shared__ int4 sh[kChoiceFrames][kChoiceBlock];
-    int g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= G) return;
+// The choice loop over graph g's candidates in id order (rewrite.cu:849-897).
+template <class Mem>
+__device__ void choice_graph(const GraphCtx<Mem> &C, int g) {
+    const ChoiceArgs &A = *C.A;
+    const Mem &m = C.m;
+    const int4 *recA = A.recA, *recB = A.recB;
+    int *choice = A.choice;
+    const bool useZeros = A.useZeros != 0;
     const int cpos = A.dg[g].cpos;
-    GraphCtx C{&A, 2 * cpos + 1, sh, (int)threadIdx.x, A.stack + (int64_t)g * A.stackCap};
     unsigned long long replaced = 0, pos = 0, zero = 0, reverted = 0, comp = 0, noRep = 0, selfRef = 0;
     long long expected = 0;
     int i = A.gStart[g];
     const int e = i + A.gCount[g];
     int4 na = make_int4(-1, -1, -1, -1), nb = na;
     if (i < e) {
-        na = A.recA[i];
-        nb = A.recB[i];
+        na = recA[i];
+        nb = recB[i];
     }
     for (; i < e; i++) {
         const int4 a = na, lv = nb;
         if (i + 1 < e) {
-            na = A.recA[i + 1];
-            nb = A.recB[i + 1];
+            na = recA[i + 1];
+            nb = recB[i + 1];
         }
-        if (i + 1 < e && (na.z >> 1) >= 0) {
+        if (Mem::kPrefetch && i + 1 < e && (na.z >> 1) >= 0) {
             // the next candidate's first loads, into L1 while this one runs
             // (a prefetch carries no value, so later stores cannot make it stale)
             const int nn = na.z >> 1, nq = na.y;
@@ -206,48 +303,47 @@ __global__ void __launch_bounds__(kChoiceBlock) k_choice(ChoiceArgs A, int G) {
         const int newIdx = rep >> 1;
         if (newIdx < 0) {
             noRep++;
-            A.choice[c] = kChNoReplace;
+            choice[c] = kChNoReplace;
             continue;
         }
         // everything read before this candidate's first store
-        const int n0 = A.L0[newIdx], n1 = A.L1[newIdx];
-        const int dn = A.del[newIdx];
-        const int dl = A.del[lv.x] | A.del[lv.y] | A.del[lv.z] | A.del[lv.w];
-        const int q0 = A.L0[q], q1 = A.L1[q];
+        int n0, n1, dn, q0, q1;
+        m.dab(newIdx, dn, n0, n1);
+        const int dl = m.dl(lv.x) | m.dl(lv.y) | m.dl(lv.z) | m.dl(lv.w);
+        m.ab(q, q0, q1);
         if (newIdx == q || (n1 >> 1) == q) {
             selfRef++;
-            A.choice[c] = kChSelfRef;
+            choice[c] = kChSelfRef;
             continue;
         }
         if (dl) {
             comp++;
-            A.choice[c] = kChCompromised;
+            choice[c] = kChCompromised;
             continue;
         }
         int added = ch_install(C, newIdx, dn, n0, n1);
-        ref_add(A.ref, newIdx, 1);
+        m.rf_add(newIdx, 1);
         int saved = ch_fast_delete(C, q, q0, q1);
-        ref_add(A.ref, newIdx, -1);
-        if (saved - added > 0 || (saved == added && A.useZeros)) {
+        m.rf_add(newIdx, -1);
+        if (saved - added > 0 || (saved == added && useZeros)) {
             replaced++;
             if (saved - added > 0)
                 pos++;
             else
                 zero++;
             expected += saved - added;
-            A.del[q] = 0;
-            A.L0[q] = C.trueLit;
-            A.L1[q] = rep;
-            ref_add(A.ref, cpos, 1);
-            ref_add(A.ref, newIdx, 1);
-            A.choice[c] = kChCommitted;
+            m.set_del(q, 0);
+            m.set_fanins(q, C.trueLit, rep);
+            m.rf_add(cpos, 1);
+            m.rf_add(newIdx, 1);
+            choice[c] = kChCommitted;
         } else {
             reverted++;
-            ch_install(C, q, A.del[q], q0, q1);
-            ref_add(A.ref, q, 1);
-            if (A.ref[newIdx] == 0) ch_fast_delete(C, newIdx, n0, n1);
-            ref_add(A.ref, q, -1);
-            A.choice[c] = kChReverted;
+            ch_install(C, q, m.dl(q), q0, q1);
+            m.rf_add(q, 1);
+            if (m.rf(newIdx) == 0) ch_fast_delete(C, newIdx, n0, n1);
+            m.rf_add(q, -1);
+            choice[c] = kChReverted;
         }
     }
     atomicAdd(&A.stats[0], replaced);
@@ -258,6 +354,55 @@ __global__ void __launch_bounds__(kChoiceBlock) k_choice(ChoiceArgs A, int G) {
     atomicAdd(&A.stats[5], noRep);
     atomicAdd(&A.stats[6], selfRef);
     atomicAdd(&A.stats[7], (unsigned long long)expected);
+}
+
+__global__ void __launch_bounds__(kChoiceBlock) k_choice(ChoiceArgs A, int G) {
+    __shared__ int4 sh[kChoiceFrames * kChoiceBlock];
+    int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= G) return;
+    GraphCtx<GlobalMem> C{&A,           GlobalMem{A.L0, A.L1, A.ref, A.del}, 2 * A.dg[g].cpos + 1,
+                          sh + threadIdx.x, kChoiceBlock, A.stack + (int64_t)g * A.stackCap,
+                          A.nL0,        A.stackCap,   A.status};
+    choice_graph(C, g);
+}
+
+constexpr int kClusterBlock = 256;
+constexpr int kClusterMaxBlocks = 8;  // the portable cluster size
+constexpr int kClusterMaxShift = 13;  // objects per block: 8192 16-byte records, 128 KB of shared memory
+
+// One graph (G = 1) on a cluster: its M objects' {L0, L1, ref, del} records
+// are copied into the blocks' shared memory, thread 0 of block 0 walks the
+// candidates on them (one 16-byte load gives a node's flag or count and
+// both fanins), and every block writes its slice back.  The blocks that do
+// not walk wait at the cluster barrier.
+__global__ void __launch_bounds__(kClusterBlock) k_choice_cluster(ChoiceArgs A, int64_t M, int shift) {
+    extern __shared__ __align__(16) unsigned char dyn[];
+    __shared__ int4 sh[kChoiceFrames];
+    const int per = 1 << shift;
+    int4 *rec = reinterpret_cast<int4 *>(dyn);
+    cg::cluster_group cl = cg::this_cluster();
+    const int64_t base = (int64_t)cl.block_rank() << shift;
+    for (int k = threadIdx.x; k < per; k += blockDim.x) {
+        const int64_t x = base + k;
+        if (x < M) rec[k] = make_int4(A.L0[x], A.L1[x], A.ref[x], A.del[x]);
+    }
+    cl.sync();
+    if (cl.block_rank() == 0 && threadIdx.x == 0) {
+        GraphCtx<ClusterMem> C{&A,    ClusterMem{rec, shift, per - 1}, 2 * A.dg[0].cpos + 1, sh, 1, A.stack,
+                               A.nL0, A.stackCap,                      A.status};
+        choice_graph(C, 0);
+    }
+    cl.sync();
+    for (int k = threadIdx.x; k < per; k += blockDim.x) {
+        const int64_t x = base + k;
+        if (x < M) {
+            const int4 r = rec[k];
+            A.L0[x] = r.x;
+            A.L1[x] = r.y;
+            A.ref[x] = r.z;
+            A.del[x] = (uint8_t)r.w;
+        }
+    }
 }
 
 // the choice's record of the i-th candidate in graph order: {c, q, rep, -}
@@ -333,10 +478,41 @@ int rw_choice(ExecCtx &X, Batch &b, RwWork &w, RwStats *stats) {
     if ((rc = X.check(scan_exclusive(gCount, gStart, G, nullptr, ar, s), "scan"))) return rc;
     ChoiceArgs A{w.nL0, w.dg,   w.L0,   w.L1,     w.ref,    w.del,       recA,   recB,  gStart,
                  gCount, w.useZeros ? 1 : 0,    stack,  (int)stackCap,       w.choice, dstats, X.status};
-    // the walk's working set is the graph's fanins, flags and counts: the
-    // smallest shared-memory carveout leaves the most L1 for it
-    cudaFuncSetAttribute(k_choice, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
-    k_choice<<<(G + kChoiceBlock - 1) / kChoiceBlock, kChoiceBlock, 0, s>>>(A, G);
+    // a single graph that fits: the cluster walk (not on an SM partition,
+    // whose SMs need not hold a whole cluster)
+    const int64_t M = w.N + w.nNew;  // extent of L0, L1, ref, del
+    bool onCluster = false;
+    if (G == 1 && X.clusters && M <= ((int64_t)kClusterMaxBlocks << kClusterMaxShift) && !getenv("CULS_CHOICE_GLOBAL")) {
+        int shift = 8;
+        while (((int64_t)kClusterMaxBlocks << shift) < M) shift++;
+        const int blocks = (int)((M + (1 << shift) - 1) >> shift);
+        const size_t smem = sizeof(int4) << shift;
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)blocks);
+        cfg.blockDim = dim3(kClusterBlock);
+        cfg.dynamicSmemBytes = smem;
+        cfg.stream = s;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = (unsigned)blocks;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        int fits = 0;
+        if (cudaFuncSetAttribute(k_choice_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) ==
+                cudaSuccess &&
+            cudaOccupancyMaxActiveClusters(&fits, k_choice_cluster, &cfg) == cudaSuccess && fits > 0) {
+            onCluster = cudaLaunchKernelEx(&cfg, k_choice_cluster, A, M, shift) == cudaSuccess;
+        }
+        (void)cudaGetLastError();  // a configuration the device refuses leaves no error behind
+    }
+    if (!onCluster) {
+        // the walk's working set is the graph's fanins, flags and counts: the
+        // smallest shared-memory carveout leaves the most L1 for it
+        cudaFuncSetAttribute(k_choice, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
+        k_choice<<<(G + kChoiceBlock - 1) / kChoiceBlock, kChoiceBlock, 0, s>>>(A, G);
+    }
     X.launched(1);
     unsigned long long hs[8], warpPairs = 0;
     if ((rc = X.check(cudaMemcpyAsync(hs, dstats, sizeof hs, cudaMemcpyDeviceToHost, s), "d2h"))) return rc;

@@ -215,13 +215,30 @@ __device__ __forceinline__ void fetch_slot(int src, int4 L, int2 M, int2 X, RCut
     rc_unpack_aux(x0, x1, c);
 }
 
+// Position of the k-th (from 0) set bit of m; m has more than k set bits.
+__device__ __forceinline__ int select_bit64(uint64_t m, int k) {
+    int p = 0;
+#pragma unroll
+    for (int w = 32; w >= 1; w >>= 1) {
+        const int c = __popcll(m & ((1ull << w) - 1ull));
+        const bool up = k >= c;
+        k -= up ? c : 0;
+        m = up ? m >> w : m;
+        p += up ? w : 0;
+    }
+    return p;
+}
+
 // A warp enumerates one node at a time: lanes 0-7 hold u0's cut slots and
-// lanes 8-15 u1's; every lane builds the candidates of pairs lane and
-// lane + 32 (pair bit i * 8 + j, the reference's i-major order); then the
-// warp replays CutEnumerate's slot policy over the admissible pairs in order
-// with the node's 8 slots on lanes 0-7 -- FindCut is a min over those lanes,
-// CutFilter two ballots -- and lanes 0-7 write the slots.  Same results as
-// the per-thread replay, with a node's latency cut to its sequential core.
+// lanes 8-15 u1's.  The admissible pairs (pair bit i * 8 + j, the
+// reference's i-major order; both slots used, at most four leaves by
+// signature) are found from the slots' signatures first and dealt out in
+// order, the k-th to lane k % 32, so a node with at most 32 of them -- most
+// nodes -- builds its candidates in one round.  Then the warp replays
+// CutEnumerate's slot policy over them in order with the node's 8 slots on
+// lanes 0-7 -- FindCut is a min over those lanes, CutFilter two ballots --
+// and lanes 0-7 write the slots.  Same results as the per-thread replay,
+// with a node's latency cut to its sequential core.
 __device__ __forceinline__ void enum_node_warp(const EnumArgs &A, int64_t q, int lane) {
     const unsigned F = 0xffffffffu;
     const int f0 = A.w0[q], f1 = A.w1[q];
@@ -255,23 +272,33 @@ __device__ __forceinline__ void enum_node_warp(const EnumArgs &A, int64_t q, int
             M = __ldcg(&A.cutM[idx]);
             X = __ldcg(&A.cutA[idx]);
         }
-        // candidates of pairs lane (i = lane / 8) and lane + 32
-        RCut a, b;
-        uint32_t ua, ub;
+        // admissible pairs from the signatures: pair lane (i = lane / 8)
+        // and pair lane + 32 (i = 4 + lane / 8), both with j = lane % 8
+        const uint32_t sA = (uint32_t)__shfl_sync(F, M.x, lane >> 3), pA = (uint32_t)__shfl_sync(F, M.y, lane >> 3);
+        const uint32_t sB = (uint32_t)__shfl_sync(F, M.x, 4 + (lane >> 3)),
+                       pB = (uint32_t)__shfl_sync(F, M.y, 4 + (lane >> 3));
+        const uint32_t sJ = (uint32_t)__shfl_sync(F, M.x, 8 + (lane & 7)),
+                       pJ = (uint32_t)__shfl_sync(F, M.y, 8 + (lane & 7));
+        const bool adm0 = packed_used(pA) && packed_used(pJ) && popc32(sA | sJ) <= 4;
+        const bool adm1 = packed_used(pB) && packed_used(pJ) && popc32(sB | sJ) <= 4;
+        const uint64_t pairs = (uint64_t)__ballot_sync(F, adm0) | ((uint64_t)__ballot_sync(F, adm1) << 32);
+        const int nPairs = __popcll(pairs);
+        // candidate k on lane k % 32: in k0 for k < 32, in k1 above
         Cand k0, k1;
-        fetch_slot(lane >> 3, L, M, X, a, ua);
-        fetch_slot(8 + (lane & 7), L, M, X, b, ub);
-        const bool adm0 = ua && ub && popc32(a.sign | b.sign) <= 4;
-        if (adm0) make_cand(a, b, c0, c1, k0);
-        fetch_slot(4 + (lane >> 3), L, M, X, a, ua);
-        const bool adm1 = ua && ub && popc32(a.sign | b.sign) <= 4;
-        if (adm1) make_cand(a, b, c0, c1, k1);
-        uint64_t pairs = (uint64_t)__ballot_sync(F, adm0) | ((uint64_t)__ballot_sync(F, adm1) << 32);
-        while (pairs) {
-            const int p = __ffsll((long long)pairs) - 1;
-            pairs &= pairs - 1;
+#pragma unroll
+        for (int r = 0; r < 2; r++) {
+            if (r * 32 >= nPairs) break;
+            const int k = r * 32 + lane;
+            const int p = k < nPairs ? select_bit64(pairs, k) : 0;
+            RCut a, b;
+            uint32_t ua, ub;
+            fetch_slot(p >> 3, L, M, X, a, ua);
+            fetch_slot(8 + (p & 7), L, M, X, b, ub);
+            if (k < nPairs) make_cand(a, b, c0, c1, r == 0 ? k0 : k1);
+        }
+        for (int k = 0; k < nPairs; k++) {
             Cand m;
-            fetch_cand(k0, k1, p >= 32, p & 31, m);
+            fetch_cand(k0, k1, k >= 32, k & 31, m);
             // Count the pair.  Besides the statistic, this atomic is
             // measured to make this loop run 3.4x faster on B200 (64x64
             // multiplier: 37.7 -> 11 ms; the instruction count drops 2.9x);
@@ -289,12 +316,7 @@ __device__ __forceinline__ void enum_node_warp(const EnumArgs &A, int64_t q, int
                     const uint32_t cls = n > 2 ? 0u : (n == 2 ? 1u : 2u);
                     key = (cls << 20) | (((spk >> 16) & 0x7FFu) << 3) | (uint32_t)lane;
                 }
-#pragma unroll
-                for (int o = 4; o; o >>= 1) {
-                    const uint32_t y = __shfl_xor_sync(F, key, o);
-                    key = y < key ? y : key;
-                }
-                id = (int)(__shfl_sync(F, key, 0) & 7u);
+                id = (int)(__reduce_min_sync(F, key) & 7u);
             }
             if (lane == id) spk &= ~(1u << 30);
             if (!m.ok) continue;

@@ -21,7 +21,7 @@ namespace culs {
 namespace {
 
 __global__ void k_front_load(int64_t N, int G, const DevGraph *dg, const int *F0, const int *F1, int *gidIn, int *a0,
-                             int *a1, int *lp, int *done) {
+                             int *a1, int *lp) {
     int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < N; p += stride) {
         int g = graph_of_pos(dg, G, (int)p);
@@ -31,7 +31,6 @@ __global__ void k_front_load(int64_t N, int G, const DevGraph *dg, const int *F0
         if (local <= dg[g].nPIs) {
             a0[p] = a1[p] = 2 * base;
             lp[p] = 0;
-            done[p] = 1;
         } else {
             int l0 = F0[p], l1 = F1[p];
             l0 = l0 < 2 ? 1 - l0 : l0;
@@ -39,16 +38,16 @@ __global__ void k_front_load(int64_t N, int G, const DevGraph *dg, const int *F0
             a0[p] = l0 + 2 * base;
             a1[p] = l1 + 2 * base;
             lp[p] = -1;
-            done[p] = 0;
         }
     }
 }
 
-// lp = 2*level + phase.  Fanins precede their node inside its graph, and the
+// lp = 2*level + phase, -1 until known: the word a node publishes and its
+// fanouts wait on.  Fanins precede their node inside its graph, and the
 // chunks are claimed in the interleaved schedule order (sched.cuh), so a
 // claimed chunk never waits on an unclaimed one.
 __global__ void __launch_bounds__(kBlock) k_front_levelize(ChunkSched S, const int *a0, const int *a1, int *lp,
-                                                            int *done, int *counter, int *maxLevel, int *status) {
+                                                            int *counter, int *maxLevel, int *status) {
     __shared__ int64_t s_begin, s_end;
     int myMax = 0;
     while (true) {
@@ -68,14 +67,12 @@ __global__ void __launch_bounds__(kBlock) k_front_levelize(ChunkSched S, const i
         if (p >= end || lp[p] != -1) continue;
         int f0 = a0[p], f1 = a1[p];
         int u0 = f0 >> 1, u1 = f1 >> 1;
-        if (!wait_ge(&done[u0], 1, status) || !wait_ge(&done[u1], 1, status)) continue;
-        int x0 = __ldcg(&lp[u0]), x1 = __ldcg(&lp[u1]);
+        int x0, x1;
+        if (!wait_word(&lp[u0], 0, status, &x0) || !wait_word(&lp[u1], 0, status, &x1)) continue;
         int lv = 1 + max(x0 >> 1, x1 >> 1);
         int ph = ((x0 & 1) ^ (f0 & 1)) & ((x1 & 1) ^ (f1 & 1));
-        __stcg(&lp[p], 2 * lv + ph);
+        st_relaxed(&lp[p], 2 * lv + ph);
         myMax = lv > myMax ? lv : myMax;
-        __threadfence();
-        st_release(&done[p], 1);
     }
     // every thread of the block leaves the loop at the same claim
     myMax = __reduce_max_sync(0xffffffffu, myMax);
@@ -195,8 +192,8 @@ int rw_front(ExecCtx &X, Batch &b, RwWork &w) {
     if ((rc = X.check(cudaMemsetAsync(cnt, 0, sizeof(int) * 8, s), "memset"))) return rc;
     ChunkSched sched;
     if ((rc = build_chunk_sched(X, b, kBlock, sched))) return rc;
-    k_front_load<<<X.grid(N), kBlock, 0, s>>>(N, G, b.dg, b.F0, b.F1, gidIn, a0, a1, lp, done);
-    k_front_levelize<<<flow_blocks(w.width, kBlock, (unsigned)(X.sms * 8), X.sms), kBlock, 0, s>>>(sched, a0, a1, lp, done, cnt + 0, cnt + 1, X.status);
+    k_front_load<<<X.grid(N), kBlock, 0, s>>>(N, G, b.dg, b.F0, b.F1, gidIn, a0, a1, lp);
+    k_front_levelize<<<flow_blocks(w.width, kBlock, (unsigned)(X.sms * 8), X.sms), kBlock, 0, s>>>(sched, a0, a1, lp, cnt + 0, cnt + 1, X.status);
     k_front_keys<<<X.grid(N), kBlock, 0, s>>>(N, lp, keys, vals);
     X.launched(3);
     if ((rc = X.check(cudaMemcpyAsync(X.hostSmall, cnt, sizeof(int) * 8, cudaMemcpyDeviceToHost, s), "d2h"))) return rc;

@@ -20,6 +20,7 @@ struct ExecCtx {
     int *hostSmall = nullptr; // 64 pinned host ints
     const RwLib *lib = nullptr;
     int sms = 148;
+    bool clusters = true;  // thread-block clusters may be launched on s (not on an SM-partition stream)
     int *launches = nullptr;
     std::string *err = nullptr;
     const Tune *tune = nullptr;  // launch and schedule parameters

@@ -18,9 +18,11 @@
 // order wins (the reference keeps whichever insertion lands first).
 //
 // B200 design: no per-frontier host loop.  Liveness is a reverse Kahn
-// worklist, levels a forward Kahn worklist over a fanout CSR, and hashing a
-// single in-order dataflow pass whose dependency waits are per-level
-// completion counters (bounded spins).
+// worklist, levels an in-order dataflow (a forward Kahn worklist over a
+// fanout CSR as the fallback), and hashing either a few full-width rounds
+// that iterate the mapping to its fixed point (batches whose table fits in
+// L2) or a single in-order dataflow pass whose dependency waits are
+// per-level completion counters (bounded spins).
 #include <algorithm>
 #include <cstdlib>
 #include <cstring>
@@ -191,7 +193,9 @@ __global__ void k_live_flags(int64_t M, const int *L0, const uint8_t *dead, uint
 // Levels of a graph-major batch whose positions are topological (`st`):
 // the in-order dataflow of the rw front over the interleaved chunk schedule
 // (sched.cuh), instead of a worklist over a fanout CSR.  Every AND node gets
-// its ASAP level; only live nodes count towards a graph's depth.
+// its ASAP level; only live nodes count towards a graph's depth.  An AND
+// node publishes its level (>= 1) in done[], the one word its fanouts wait
+// on and read.
 __global__ void __launch_bounds__(kBlock) k_st_levelize(ChunkSched S, const int *L0, const int *L1,
                                                          const uint8_t *liveFlag, const int *gid, int *level,
                                                          int *done, int *graphLevels, int *counter, int *maxLevel,
@@ -217,22 +221,15 @@ __global__ void __launch_bounds__(kBlock) k_st_levelize(ChunkSched S, const int 
         if (a < 0) continue;  // constant or PI: level 0, done preset
         const int u0 = a >> 1, u1 = L1[p] >> 1;
         int l0 = 0, l1 = 0;
-        if (L0[u0] >= 0) {
-            if (!wait_ge(&done[u0], 1, status)) continue;
-            l0 = __ldcg(&level[u0]);
-        }
-        if (L0[u1] >= 0) {
-            if (!wait_ge(&done[u1], 1, status)) continue;
-            l1 = __ldcg(&level[u1]);
-        }
+        if (L0[u0] >= 0 && !wait_word(&done[u0], 1, status, &l0)) continue;
+        if (L0[u1] >= 0 && !wait_word(&done[u1], 1, status, &l1)) continue;
         const int lv = 1 + (l0 > l1 ? l0 : l1);
+        st_relaxed(&done[p], lv);
         __stcg(&level[p], lv);
         if (liveFlag[p]) {
             agg_max(graphLevels, gid[p], lv);
             myMax = lv > myMax ? lv : myMax;
         }
-        __threadfence();
-        st_release(&done[p], 1);
     }
     // every thread of the block leaves the loop at the same claim
     myMax = __reduce_max_sync(0xffffffffu, myMax);
@@ -246,7 +243,8 @@ __global__ void __launch_bounds__(kBlock) k_st_levelize(ChunkSched S, const int 
 // leaves the node unresolved (done = 2), and the unresolved nodes form the
 // next pass's list.  Every wait is on a node whose chunk was claimed
 // earlier, so no pass can deadlock, and each pass resolves at least the
-// unresolved nodes whose fanins are all resolved.
+// unresolved nodes whose fanins are all resolved.  done[] is the word a node
+// publishes: 0 pending, 2 unresolved, level + 2 once resolved.
 __global__ void __launch_bounds__(kBlock) k_order_levelize(int64_t n, const int *list, const int *posOf, const int *L0,
                                                             const int *L1, const uint8_t *liveFlag, const int *gid,
                                                             int *level, int *done, int *graphLevels, int *counter,
@@ -273,31 +271,27 @@ __global__ void __launch_bounds__(kBlock) k_order_levelize(int64_t n, const int 
         for (int k = 0; k < 2 && ok; k++) {
             const int u = (k == 0 ? L0[v] : L1[v]) >> 1;
             if (L0[u] < 0) continue;  // constant or PI: level 0
-            int d = ld_acquire(&done[u]);
-            if (d == 0 && posOf[u] < pv) {
-                if (!wait_ge(&done[u], 1, status)) {
-                    ok = false;
-                    break;
-                }
-                d = ld_acquire(&done[u]);
-            }
-            if (d != 1) {
+            int d = ld_relaxed(&done[u]);
+            if (d == 0 && posOf[u] < pv && !wait_word(&done[u], 1, status, &d)) {
                 ok = false;
                 break;
             }
-            const int l = __ldcg(&level[u]);
+            if (d < 3) {  // pending behind this node in the order, or unresolved
+                ok = false;
+                break;
+            }
+            const int l = d - 2;
             lv = l > lv ? l : lv;
         }
         if (!ok) {
-            st_release(&done[v], 2);
+            st_relaxed(&done[v], 2);
             continue;
         }
         lv += 1;
+        st_relaxed(&done[v], lv + 2);
         __stcg(&level[v], lv);
         agg_max(graphLevels, gid[v], lv);
         myMax = lv > myMax ? lv : myMax;
-        __threadfence();
-        st_release(&done[v], 1);
     }
     myMax = __reduce_max_sync(0xffffffffu, myMax);
     if ((threadIdx.x & 31) == 0 && myMax > 0) atomicMax(maxLevel, myMax);
@@ -473,6 +467,105 @@ __global__ void __launch_bounds__(kDedupChunk) k_dedup(DedupArgs A) {
             __threadfence();
             atomicAdd(&A.lvlDone[lv], end - begin);
         }
+    }
+}
+
+// ------------------------------------------------- deduplication in rounds
+// The mapping k_dedup computes is the unique fixed point of one parallel
+// step: a node's key is its fanins' mapped literals (folded when trivial),
+// and it maps to the position of the lowest-ranked live node with the same
+// key.  (By induction over the levels: a node's key reads only lower
+// levels, so any fixed point equals the level-by-level result.)  Starting
+// from the identity, round r makes every node of level <= r final, and the
+// rounds stop at the first one that changes nothing -- after one round when
+// nothing merges, after a few when merges cascade, since a node's key
+// changes only when a fanin's mapping did.  Each round is two passes over
+// the live nodes with no dependency waits, so a deep, narrow graph costs a
+// few launches instead of one wait latency per level.
+
+struct RoundArgs {
+    int64_t nLive;
+    const int *srt, *rankOf, *posOfRank;
+    const int *L0, *L1;
+    const int *gid;
+    const DevGraph *dg;
+    AndTable tab;
+    const int *cur;  // per position: the literal an AND node maps to this round
+    int *nxt;        // the same after this round
+    int *slotT;      // per processing index: table slot, -1 when folded
+    int *mapEnc, *kl0, *kl1;
+    int foldTrivial, unique;
+    int *changed;
+    int *status;
+};
+
+__global__ void k_round_init(int64_t n, const int *srt, int *cur) {
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += stride) {
+        const int v = srt[t];
+        cur[v] = 2 * v;
+    }
+}
+
+// keys from this round's mapping: fold (as k_dedup does) or insert
+__global__ void k_round_insert(RoundArgs A) {
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < A.nLive; t += stride) {
+        const int v = A.srt[t];
+        int lits[2] = {A.L0[v], A.L1[v]};
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+            const int u = lits[k] >> 1;
+            if (A.L0[u] >= 0) lits[k] = A.cur[u] ^ (lits[k] & 1);
+        }
+        int l0 = lits[0], l1 = lits[1];
+        if (l0 > l1) {
+            const int x = l0;
+            l0 = l1;
+            l1 = x;
+        }
+        const int T = 2 * A.dg[A.gid[v]].cpos;  // AIGMan: constant TRUE
+        const int F = T + 1;
+        int triv = -1;
+        if (A.foldTrivial) {
+            if (l0 == l1)
+                triv = l0;
+            else if (l0 == (l1 ^ 1))
+                triv = F;
+            else if (l0 == T)
+                triv = l1;
+            else if (l1 == T)
+                triv = l0;
+            else if (l0 == F || l1 == F)
+                triv = F;
+        }
+        if (triv >= 0) {
+            A.mapEnc[v] = triv;
+            A.nxt[v] = triv;
+            A.slotT[t] = -1;
+            if (triv != A.cur[v]) *A.changed = 1;
+        } else {
+            const unsigned long long key = A.unique ? (1ull << 63) | (unsigned long long)(uint32_t)v
+                                                    : ((unsigned long long)(uint32_t)l0 << 32) | (uint32_t)l1;
+            const int slot = table_insert(A.tab, key, A.rankOf[v], A.status);
+            A.kl0[t] = l0;
+            A.kl1[t] = l1;
+            A.mapEnc[v] = slot >= 0 ? -(slot + 1) : 0;
+            A.slotT[t] = slot;
+        }
+    }
+}
+
+// every key's lowest rank is known: the inserted nodes map to its position
+__global__ void k_round_resolve(RoundArgs A) {
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < A.nLive; t += stride) {
+        const int slot = A.slotT[t];
+        if (slot < 0) continue;
+        const int v = A.srt[t];
+        const int m = 2 * A.posOfRank[A.tab.vals[slot]];
+        A.nxt[v] = m;
+        if (m != A.cur[v]) *A.changed = 1;
     }
 }
 
@@ -757,10 +850,50 @@ int Engine::strash_core(Batch &b, int64_t M, const int *L0, const int *L1, const
     uint8_t *wflags = ar_.get<uint8_t>(nLive + 1);
     int *wl = ar_.get<int>(nLive + 1);
     if (!tk || !tv || !mapEnc || !kl0 || !kl1 || !wflags || !wl) return fail(CULS_E_OOM, "strash: arena exhausted");
-    check(cudaMemsetAsync(tk, 0xFF, sizeof(unsigned long long) * cap, s), "memset");
-    check(cudaMemsetAsync(tv, 0x7F, sizeof(int) * cap, s), "memset");
     check(cudaMemsetAsync(qc + 5, 0, sizeof(int), s), "memset");
-    if (nLive > 0) {
+    // Rounds (k_round_*) for batches whose table stays in L2, where they
+    // replace one wait latency per level by a few full passes; the level
+    // dataflow (k_dedup) for larger ones, and whenever the rounds do not
+    // settle within kMaxRounds.  CULS_DEDUP_MODE=levels|rounds forces either
+    // (the tests run both on the same graphs).
+    constexpr int64_t kRoundsMaxLive = 4ll << 20;
+    constexpr int kMaxRounds = 24;
+    bool useRounds = nLive > 0 && nLive <= kRoundsMaxLive;
+    if (const char *env = getenv("CULS_DEDUP_MODE")) {
+        if (!strcmp(env, "levels")) useRounds = false;
+        if (!strcmp(env, "rounds")) useRounds = nLive > 0;
+    }
+    bool settled = false;
+    if (useRounds) {
+        int *cur = ar_.get<int>(M + 1), *nxt = ar_.get<int>(M + 1), *slotT = ar_.get<int>(nLive + 1);
+        if (!cur || !nxt || !slotT) return fail(CULS_E_OOM, "strash: arena exhausted");
+        const unsigned gl = grid_1d(nLive, kBlock, sms_ * 16);
+        if (prof_) this->mark(kMkDedupK0);
+        k_round_init<<<gl, kBlock, 0, s>>>(nLive, srt, cur);
+        launches_ += 1;
+        for (int r = 0; r < kMaxRounds; r++) {
+            check(cudaMemsetAsync(tk, 0xFF, sizeof(unsigned long long) * cap, s), "memset");
+            check(cudaMemsetAsync(tv, 0x7F, sizeof(int) * cap, s), "memset");
+            check(cudaMemsetAsync(qc + 16, 0, sizeof(int), s), "memset");
+            RoundArgs R{nLive,  srt,   rankOf, idOrder ? liveIdx : srt, L0, L1, gidA, b.dg, AndTable{tk, tv, cap - 1},
+                        cur,    nxt,   slotT,  mapEnc, kl0, kl1, foldTrivial ? 1 : 0, unique ? 1 : 0, qc + 16, status_};
+            k_round_insert<<<gl, kBlock, 0, s>>>(R);
+            k_round_resolve<<<gl, kBlock, 0, s>>>(R);
+            launches_ += 2;
+            check(cudaMemcpyAsync(hostSmall_ + 16, qc + 16, sizeof(int), cudaMemcpyDeviceToHost, s), "d2h");
+            if (int e = sync()) return e;
+            if (int e = check_status("strash hashing")) return e;
+            std::swap(cur, nxt);
+            if (hostSmall_[16] == 0) {
+                settled = true;
+                break;
+            }
+        }
+        if (prof_) this->mark(kMkDedupK1);
+    }
+    if (nLive > 0 && !settled) {
+        check(cudaMemsetAsync(tk, 0xFF, sizeof(unsigned long long) * cap, s), "memset");
+        check(cudaMemsetAsync(tv, 0x7F, sizeof(int) * cap, s), "memset");
         DedupArgs A{nLive,      srt,      rankOf,  idOrder ? liveIdx : srt,
                     L0,         L1,       level,   lvlCnt,
                     lvlStart,   chunkStart, maxLevel, lvlDone,
@@ -770,8 +903,11 @@ int Engine::strash_core(Batch &b, int64_t M, const int *L0, const int *L1, const
         if (prof_) this->mark(kMkDedupK0);
         k_dedup<<<gridQ, kBlock, 0, s>>>(A);
         if (prof_) this->mark(kMkDedupK1);
+        launches_ += 1;
+    }
+    if (nLive > 0) {
         k_winner_flags<<<grid_1d(nLive, kBlock, sms_ * 16), kBlock, 0, s>>>(nLive, srt, rankOf, mapEnc, tv, wflags);
-        launches_ += 2;
+        launches_ += 1;
     }
     check(compact_flags(wflags, nLive, wl, qc + 6, ar_, s), "compact");
     // In id order (CPU variants) the winners are ranked by position, not by

@@ -12,7 +12,9 @@ CEC"), not as ABC:
 3. one incremental z3 solver holds the Tseitin encoding of both AIGs; the
    candidate pairs are proved in topological order of the second AIG, each
    proved pair added as an equality (so later proofs see both cones merged,
-   which keeps each query local), a refuted pair simply left out;
+   which keeps each query local), a refuted pair left out and its
+   counterexample kept: every 64 counterexamples become one more simulation
+   word, which splits the candidate classes they refute;
 4. the outputs are equivalent when, for every PO pair, z3 finds no input
    assignment that tells them apart (UNSAT).
 
@@ -44,7 +46,28 @@ def _simulate_all(g, words, seed):
     return val
 
 
-def cec(a, b, words=8, seed=1, max_pairs=None):
+def _simulate_word(g, pi_word):
+    """One 64-bit word per object of g for the given PI word array."""
+    n = len(g.fanin0)
+    val = np.zeros(n, np.uint64)
+    val[0] = np.uint64(0xFFFFFFFFFFFFFFFF)
+    val[1:g.nPIs + 1] = pi_word
+    f0 = np.asarray(g.fanin0)
+    f1 = np.asarray(g.fanin1)
+    full = np.uint64(0xFFFFFFFFFFFFFFFF)
+    for v in range(g.nPIs + 1, n):
+        a, b = int(f0[v]), int(f1[v])
+        x = val[a >> 1] ^ (full if a & 1 else np.uint64(0))
+        y = val[b >> 1] ^ (full if b & 1 else np.uint64(0))
+        val[v] = x & y
+    return val
+
+
+def cec(a, b, words=8, seed=1, max_pairs=None, query_ms=20000, verbose=False):
+    """query_ms bounds each z3 query; a candidate whose query runs out is
+    left unmerged, a PO pair whose query runs out is left unproved.  Every
+    refuted candidate's counterexample is kept; each 64 of them become one
+    more simulation word, which splits the candidate classes they refute."""
     import z3
     t0 = time.time()
     if a.nPIs != b.nPIs or len(a.outs) != len(b.outs):
@@ -53,6 +76,7 @@ def cec(a, b, words=8, seed=1, max_pairs=None):
     vb = _simulate_all(b, words, seed)
     full = np.uint64(0xFFFFFFFFFFFFFFFF)
     s = z3.Solver()
+    s.set("timeout", query_ms)
     pis = [z3.BoolVal(True)] + [z3.Bool(f"i{k}") for k in range(1, a.nPIs + 1)]
 
     def encode(g, tag):
@@ -73,12 +97,17 @@ def cec(a, b, words=8, seed=1, max_pairs=None):
         return xs[l >> 1] if not l & 1 else z3.Not(xs[l >> 1])
 
     # candidate pairs: signature of a node of b equal to a node of a (or its complement)
-    sig = {}
-    for v in range(len(a.fanin0)):
-        sig.setdefault(va[v].tobytes(), (v, 0))
-    for v in range(len(a.fanin0)):
-        sig.setdefault((va[v] ^ full).tobytes(), (v, 1))
-    proved = refuted = 0
+    def build_sig():
+        sig = {}
+        for v in range(len(a.fanin0)):
+            sig.setdefault(va[v].tobytes(), (v, 0))
+        for v in range(len(a.fanin0)):
+            sig.setdefault((va[v] ^ full).tobytes(), (v, 1))
+        return sig
+
+    sig = build_sig()
+    cex = []  # counterexample input vectors, bit k of PI k
+    proved = refuted = unknown = 0
     for v in range(b.nPIs + 1, len(b.fanin0)):
         c = sig.get(vb[v].tobytes())
         if c is None:
@@ -90,12 +119,29 @@ def cec(a, b, words=8, seed=1, max_pairs=None):
         s.push()
         s.add(ea != xb[v])
         r = s.check()
+        if r == z3.sat:
+            m = s.model()
+            cex.append([z3.is_true(m.eval(pis[k], model_completion=True)) for k in range(1, a.nPIs + 1)])
         s.pop()
         if r == z3.unsat:
             s.add(ea == xb[v])
             proved += 1
-        else:
+        elif r == z3.sat:
             refuted += 1
+            if len(cex) == 64:  # one more simulation word from the counterexamples
+                bits = np.array(cex, bool)  # [64, nPIs]
+                w = np.zeros(a.nPIs, np.uint64)
+                for k in range(64):
+                    w |= bits[k].astype(np.uint64) << np.uint64(k)
+                va = np.concatenate([va, _simulate_word(a, w)[:, None]], axis=1)
+                vb = np.concatenate([vb, _simulate_word(b, w)[:, None]], axis=1)
+                sig = build_sig()
+                cex = []
+        else:
+            unknown += 1
+        if verbose and (proved + refuted + unknown) % 2000 == 0:
+            print(f"  cec {v}/{len(b.fanin0)}: proved {proved} refuted {refuted} unknown {unknown} "
+                  f"{time.time() - t0:.0f} s", flush=True)
     po_proved = 0
     for oa, ob in zip(a.outs, b.outs):
         s.push()
@@ -105,5 +151,6 @@ def cec(a, b, words=8, seed=1, max_pairs=None):
         if r == z3.unsat:
             po_proved += 1
     return {"equivalent": po_proved == len(a.outs), "pos": len(a.outs), "pos_proved": po_proved,
-            "pairs_proved": proved, "pairs_refuted": refuted, "seconds": round(time.time() - t0, 2),
+            "pairs_proved": proved, "pairs_refuted": refuted, "pairs_unknown": unknown,
+            "seconds": round(time.time() - t0, 2),
             "method": "z3 SAT-sweeping CEC (simulation candidates, incremental proofs)"}

@@ -4,7 +4,9 @@ in-order passes over a nearly topological order of the rewritten batch; the
 level-synchronous worklist, its fallback, runs alone when
 CULS_DEDUP_WORKLIST is set.  Both must give the same graphs, equal to the
 oracle, for GPU- and CPU-deduplicating rewrites and for a second rewrite
-that starts from the kept manager graph."""
+that starts from the kept manager graph.  The same holds for the two ways
+the hashing runs (CULS_DEDUP_MODE: fixed-point rounds or the level
+dataflow)."""
 import pytest
 
 import culs_b200 as C
@@ -53,3 +55,24 @@ def test_level_paths_agree(gpu_dedup, twice, monkeypatch):
     for i, g in enumerate(gs):
         assert same_graph(a[i], b[i]), i
         assert same_graph(a[i], oracle(g, gpu_dedup, twice)), i
+
+
+@pytest.mark.parametrize("gpu_dedup", [True, False])
+def test_hashing_rounds_equal_level_dataflow(gpu_dedup, monkeypatch):
+    """The hashing's fixed-point rounds (the default on batches whose table
+    fits in L2) and its level-by-level dataflow (the default on larger ones)
+    give the same graphs, equal to the oracle, on both the rewrite's
+    deduplication and `st`; a chain of `rw; rw; st` makes the second rewrite
+    start from a graph with merges left to cascade."""
+    gs = graphs()
+    ctx = C.Context()
+    try:
+        got = {}
+        for mode in ["rounds", "levels"]:
+            monkeypatch.setenv("CULS_DEDUP_MODE", mode)
+            got[mode] = run(ctx, gs, gpu_dedup, True)
+    finally:
+        ctx.close()
+    for i, g in enumerate(gs):
+        assert same_graph(got["rounds"][i], got["levels"][i]), i
+        assert same_graph(got["rounds"][i], oracle(g, gpu_dedup, True)), i
