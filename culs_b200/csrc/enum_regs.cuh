@@ -58,7 +58,9 @@ __device__ __forceinline__ T pick4(const T (&v)[4], int i) {
     return i == 0 ? v[0] : (i == 1 ? v[1] : (i == 2 ? v[2] : v[3]));
 }
 
-// MergeCutOrdered / MergeCut with the leaf attributes carried along.
+// MergeCutOrdered / MergeCut with the leaf attributes carried along: four
+// merge steps, each taking the smaller head leaf (both when equal), without
+// branches -- the lanes of the warp-wide enumeration merge different cuts.
 __device__ __forceinline__ bool rc_merge(const RCut &a0, const RCut &b0, RCut &o) {
     const bool sw = a0.n < b0.n;
     const RCut &a = sw ? b0 : a0;
@@ -67,39 +69,22 @@ __device__ __forceinline__ bool rc_merge(const RCut &a0, const RCut &b0, RCut &o
     const int na = (int)a.n, nb = (int)b.n;
 #pragma unroll
     for (int s = 0; s < 4; s++) {
-        o.l[s] = 0;
-        o.ref[s] = 0;
-        o.lid[s] = 0;
+        const bool ea = i >= na, eb = k >= nb;
+        const bool act = !(ea && eb);
+        const int ai = ea ? 0x7FFFFFFF : pick4(a.l, i);
+        const int bk = eb ? 0x7FFFFFFF : pick4(b.l, k);
+        const int take = eb ? 0 : (ea ? 1 : (ai < bk ? 0 : (ai > bk ? 1 : 2)));  // 0 = a, 1 = b, 2 = equal
+        o.l[s] = act ? (take == 1 ? bk : ai) : 0;
+        o.ref[s] = act ? (take == 1 ? pick4(b.ref, k) : pick4(a.ref, i)) : 0u;
+        o.lid[s] = act ? (take == 1 ? pick4(b.lid, k) : pick4(a.lid, i)) : 0u;
+        i += (act && take != 1) ? 1 : 0;
+        k += (act && take != 0) ? 1 : 0;
+        c = act ? s + 1 : c;
     }
-#pragma unroll
-    for (int s = 0; s < 4; s++) {
-        if (c != s) break;
-        // pick from a, from b, or from both
-        int ai = i < na ? pick4(a.l, i) : 0x7FFFFFFF;
-        int bk = k < nb ? pick4(b.l, k) : 0x7FFFFFFF;
-        if (i == na && k == nb) break;
-        int take;  // 0 = a, 1 = b, 2 = equal
-        if (k == nb)
-            take = 0;
-        else if (i == na)
-            take = 1;
-        else
-            take = ai < bk ? 0 : (ai > bk ? 1 : 2);
-        int leaf = take == 1 ? bk : ai;
-        uint32_t r = take == 1 ? pick4(b.ref, k) : pick4(a.ref, i);
-        uint32_t d = take == 1 ? pick4(b.lid, k) : pick4(a.lid, i);
-        o.l[s] = leaf;
-        o.ref[s] = r;
-        o.lid[s] = d;
-        if (take != 1) i++;
-        if (take != 0) k++;
-        c = s + 1;
-    }
-    if (i < na || k < nb) return false;
     o.n = (uint32_t)c;
     o.sign = a0.sign | b0.sign;
     o.used = 1;
-    return true;
+    return i >= na && k >= nb;
 }
 
 // CutTruthPhase over register leaves.
@@ -119,8 +104,8 @@ __device__ __forceinline__ int rc_phase(const RCut &x, const RCut &cut) {
 __device__ __forceinline__ uint32_t rc_truth(const RCut &cut, const RCut &a, const RCut &b, int ca, int cb) {
     uint32_t t0 = ca ? (~a.tt & 0xFFFFu) : a.tt;
     uint32_t t1 = cb ? (~b.tt & 0xFFFFu) : b.tt;
-    t0 = tt_stretch(t0, (int)a.n, rc_phase(a, cut));
-    t1 = tt_stretch(t1, (int)b.n, rc_phase(b, cut));
+    t0 = tt_stretch_flat(t0, (int)a.n, rc_phase(a, cut));
+    t1 = tt_stretch_flat(t1, (int)b.n, rc_phase(b, cut));
     return (t0 & t1) & 0xFFFFu;
 }
 
@@ -140,7 +125,7 @@ __device__ __forceinline__ bool rc_minimize(RCut &c) {
             ph |= 1 << i;
     }
     if (nl == (int)c.n) return false;
-    c.tt = tt_shrink(t, ph) & 0xFFFFu;
+    c.tt = tt_shrink_flat(t, ph) & 0xFFFFu;
     RCut o = c;
     int k = 0;
     uint32_t sign = 0;

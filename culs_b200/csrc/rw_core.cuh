@@ -226,6 +226,33 @@ CULS_HD uint32_t tt_stretch(uint32_t t, int nVar, int ph) {
     return t;
 }
 
+// tt_swap_adj with the variable known at compile time
+template <int V>
+CULS_HD uint32_t tt_swap_adj_c(uint32_t t) {
+    return V == 0   ? (t & 0x9999u) | ((t & 0x2222u) << 1) | ((t & 0x4444u) >> 1)
+           : V == 1 ? (t & 0xC3C3u) | ((t & 0x0C0Cu) << 2) | ((t & 0x3030u) >> 2)
+                    : (t & 0xF00Fu) | ((t & 0x00F0u) << 4) | ((t & 0x0F00u) >> 4);
+}
+
+// tt_stretch without branches, for the warp-wide enumeration (lanes with
+// different phases take one path): every swap the loops could make, in the
+// loops' order, applied when the loops would make it.  Equal to tt_stretch
+// whenever ph has nVar bits set, which holds for every call (a fanin cut's
+// leaves all appear in the merged cut).
+CULS_HD uint32_t tt_stretch_flat(uint32_t t, int nVar, int ph) {
+    int var = nVar - 1;
+#define CULS_SW(K, I)                                                          \
+    {                                                                          \
+        const uint32_t sw = tt_swap_adj_c<K>(t);                               \
+        t = (((ph >> (I)) & 1) && (K) >= var) ? sw : t;                        \
+    }
+    CULS_SW(0, 3) CULS_SW(1, 3) CULS_SW(2, 3) var -= (ph >> 3) & 1;
+    CULS_SW(0, 2) CULS_SW(1, 2) var -= (ph >> 2) & 1;
+    CULS_SW(0, 1)
+#undef CULS_SW
+    return t;
+}
+
 // CutTruthtable, src/algorithms/rewrite.cu:223-229
 CULS_HD uint32_t cut_truth(const Cut &cut, const Cut &a, const Cut &b, int ca, int cb) {
     uint32_t t0 = ca ? (~a.tt & 0xFFFFu) : a.tt;
@@ -243,6 +270,22 @@ CULS_HD uint32_t tt_shrink(uint32_t t, int ph) {
             for (int k = i - 1; k >= var; k--) t = tt_swap_adj(t, k);
             var++;
         }
+    return t;
+}
+
+// tt_shrink without branches (see tt_stretch_flat): equal to tt_shrink for
+// every phase.
+CULS_HD uint32_t tt_shrink_flat(uint32_t t, int ph) {
+    int var = (ph & 1);
+#define CULS_SW(K, I)                                                          \
+    {                                                                          \
+        const uint32_t sw = tt_swap_adj_c<K>(t);                               \
+        t = (((ph >> (I)) & 1) && (K) >= var) ? sw : t;                        \
+    }
+    CULS_SW(0, 1) var += (ph >> 1) & 1;
+    CULS_SW(1, 2) CULS_SW(0, 2) var += (ph >> 2) & 1;
+    CULS_SW(2, 3) CULS_SW(1, 3) CULS_SW(0, 3)
+#undef CULS_SW
     return t;
 }
 
