@@ -152,29 +152,26 @@ __device__ __forceinline__ void make_cand(const RCut &a, const RCut &b, int c0, 
     rc_pack_aux(m, c.a0, c.a1);
 }
 
-// Candidate `hi ? c1 : c0` of lane src, broadcast to the warp.
-__device__ __forceinline__ void fetch_cand(const Cand &c0, const Cand &c1, bool hi, int src, Cand &o) {
-    const unsigned F = 0xffffffffu;
-#define CULS_PICK(f) o.f = __shfl_sync(F, hi ? c1.f : c0.f, src)
-    CULS_PICK(x0);
-    CULS_PICK(x1);
-    CULS_PICK(x2);
-    CULS_PICK(x3);
-    CULS_PICK(xs);
-    CULS_PICK(xn);
-    CULS_PICK(y0);
-    CULS_PICK(y1);
-    CULS_PICK(y2);
-    CULS_PICK(y3);
-    CULS_PICK(ys);
-    CULS_PICK(yn);
-    CULS_PICK(ytt);
-    CULS_PICK(yval);
-    CULS_PICK(a0);
-    CULS_PICK(a1);
-    CULS_PICK(ok);
-    CULS_PICK(mini);
-#undef CULS_PICK
+// A candidate in shared memory: four 16-byte words, written once by the lane
+// that built it and read by the whole warp (a broadcast) when its turn in
+// the slot policy comes.
+__device__ __forceinline__ void put_cand(int4 *d, const Cand &c) {
+    d[0] = make_int4(c.x0, c.x1, c.x2, c.x3);
+    d[1] = make_int4(c.y0, c.y1, c.y2, c.y3);
+    d[2] = make_int4((int)c.xs, (int)(c.xn | (c.ok << 8) | (c.mini << 9)), (int)c.ys, (int)c.yn);
+    d[3] = make_int4((int)c.ytt, (int)c.yval, (int)c.a0, (int)c.a1);
+}
+
+__device__ __forceinline__ void get_cand(const int4 *d, Cand &c) {
+    const int4 w0 = d[0], w1 = d[1], w2 = d[2], w3 = d[3];
+    c.x0 = w0.x, c.x1 = w0.y, c.x2 = w0.z, c.x3 = w0.w;
+    c.y0 = w1.x, c.y1 = w1.y, c.y2 = w1.z, c.y3 = w1.w;
+    c.xs = (uint32_t)w2.x;
+    c.xn = (uint32_t)w2.y & 0xFFu;
+    c.ok = ((uint32_t)w2.y >> 8) & 1u;
+    c.mini = ((uint32_t)w2.y >> 9) & 1u;
+    c.ys = (uint32_t)w2.z, c.yn = (uint32_t)w2.w;
+    c.ytt = (uint32_t)w3.x, c.yval = (uint32_t)w3.y, c.a0 = (uint32_t)w3.z, c.a1 = (uint32_t)w3.w;
 }
 
 // CutFilter (rewrite.cu:178-193) with slot k on lane k (k < 8): visiting the
@@ -234,12 +231,13 @@ __device__ __forceinline__ int select_bit64(uint64_t m, int k) {
 // reference's i-major order; both slots used, at most four leaves by
 // signature) are found from the slots' signatures first and dealt out in
 // order, the k-th to lane k % 32, so a node with at most 32 of them -- most
-// nodes -- builds its candidates in one round.  Then the warp replays
+// nodes -- builds its candidates in one round; each lands in shared memory.
+// Then the warp replays
 // CutEnumerate's slot policy over them in order with the node's 8 slots on
 // lanes 0-7 -- FindCut is a min over those lanes, CutFilter two ballots --
 // and lanes 0-7 write the slots.  Same results as the per-thread replay,
 // with a node's latency cut to its sequential core.
-__device__ __forceinline__ void enum_node_warp(const EnumArgs &A, int64_t q, int lane) {
+__device__ __forceinline__ void enum_node_warp(const EnumArgs &A, int64_t q, int lane, int4 (*sc)[4]) {
     const unsigned F = 0xffffffffu;
     const int f0 = A.w0[q], f1 = A.w1[q];
     const int u0 = f0 >> 1, u1 = f1 >> 1, c0 = f0 & 1, c1 = f1 & 1;
@@ -283,8 +281,7 @@ __device__ __forceinline__ void enum_node_warp(const EnumArgs &A, int64_t q, int
         const bool adm1 = packed_used(pB) && packed_used(pJ) && popc32(sB | sJ) <= 4;
         const uint64_t pairs = (uint64_t)__ballot_sync(F, adm0) | ((uint64_t)__ballot_sync(F, adm1) << 32);
         const int nPairs = __popcll(pairs);
-        // candidate k on lane k % 32: in k0 for k < 32, in k1 above
-        Cand k0, k1;
+        // candidate k built by lane k % 32, kept in sc[k]
 #pragma unroll
         for (int r = 0; r < 2; r++) {
             if (r * 32 >= nPairs) break;
@@ -294,30 +291,32 @@ __device__ __forceinline__ void enum_node_warp(const EnumArgs &A, int64_t q, int
             uint32_t ua, ub;
             fetch_slot(p >> 3, L, M, X, a, ua);
             fetch_slot(8 + (p & 7), L, M, X, b, ub);
-            if (k < nPairs) make_cand(a, b, c0, c1, r == 0 ? k0 : k1);
+            if (k < nPairs) {
+                Cand c;
+                make_cand(a, b, c0, c1, c);
+                put_cand(sc[k], c);
+            }
         }
+        __syncwarp();
         for (int k = 0; k < nPairs; k++) {
             Cand m;
-            fetch_cand(k0, k1, k >= 32, k & 31, m);
+            get_cand(sc[k], m);
             // Count the pair.  Besides the statistic, this atomic is
             // measured to make this loop run 3.4x faster on B200 (64x64
             // multiplier: 37.7 -> 11 ms; the instruction count drops 2.9x);
             // a plain store or a compiler barrier in its place does not.
             if (lane == 0) atomicAdd(A.warpPairs, 1ull);
-            // FindCut (rewrite.cu:84-109)
+            // FindCut (rewrite.cu:84-109): the first free slot, else the
+            // lowest (class, value, index); both computed, one kept
             const unsigned freeSlots = __ballot_sync(F, lane < 8 && !packed_used(spk)) & 0xFFu;
-            int id;
-            if (freeSlots) {
-                id = __ffs(freeSlots) - 1;
-            } else {
-                uint32_t key = 0xFFFFFFFFu;
-                if (lane < 8) {
-                    const uint32_t n = packed_nleaves(spk);
-                    const uint32_t cls = n > 2 ? 0u : (n == 2 ? 1u : 2u);
-                    key = (cls << 20) | (((spk >> 16) & 0x7FFu) << 3) | (uint32_t)lane;
-                }
-                id = (int)(__reduce_min_sync(F, key) & 7u);
+            uint32_t key = 0xFFFFFFFFu;
+            if (lane < 8) {
+                const uint32_t n = packed_nleaves(spk);
+                const uint32_t cls = n > 2 ? 0u : (n == 2 ? 1u : 2u);
+                key = (cls << 20) | (((spk >> 16) & 0x7FFu) << 3) | (uint32_t)lane;
             }
+            const uint32_t lowest = __reduce_min_sync(F, key);
+            const int id = freeSlots ? __ffs(freeSlots) - 1 : (int)(lowest & 7u);
             if (lane == id) spk &= ~(1u << 30);
             if (!m.ok) continue;
             const int xl[4] = {m.x0, m.x1, m.x2, m.x3};
@@ -354,7 +353,7 @@ __device__ __forceinline__ void enum_node_warp(const EnumArgs &A, int64_t q, int
         A.cutA[q * 8 + lane] = make_int2((int)sa0, (int)sa1);
         __threadfence();
     }
-    __syncwarp();
+    __syncwarp();  // also: every lane is done reading sc before the next node overwrites it
     if (lane == 0) st_release(&A.done[q], 1);
 }
 
@@ -496,6 +495,7 @@ __device__ __forceinline__ void enum_node_thread(const EnumArgs &A, int64_t q, b
 // time is the time of its slowest node).  Warps claim chunks in level
 // order, so every fanin of a claimed node lies in an earlier, claimed chunk.
 __global__ void __launch_bounds__(kEnumBlock, 3) k_enumerate(EnumArgs A) {
+    __shared__ int4 s_cand[kEnumBlock / 32][64][4];
     const unsigned F = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int total = A.chunkStart[A.maxLevel + 1];
@@ -519,7 +519,7 @@ __global__ void __launch_bounds__(kEnumBlock, 3) k_enumerate(EnumArgs A) {
             const int64_t q = base + k * 32 + lane;
             enum_node_thread(A, q, q < base + w);
         } else {
-            enum_node_warp(A, base + k, lane);
+            enum_node_warp(A, base + k, lane, s_cand[threadIdx.x >> 5]);
         }
     }
 }
