@@ -494,7 +494,7 @@ __device__ __forceinline__ void enum_node_thread(const EnumArgs &A, int64_t q, b
 // one-node chunks, each node on a whole warp (latency: a narrow level's
 // time is the time of its slowest node).  Warps claim chunks in level
 // order, so every fanin of a claimed node lies in an earlier, claimed chunk.
-__global__ void __launch_bounds__(kEnumBlock, 3) k_enumerate(EnumArgs A) {
+__global__ void __launch_bounds__(kEnumBlock, 4) k_enumerate(EnumArgs A) {
     __shared__ int4 s_cand[kEnumBlock / 32][64][4];
     const unsigned F = 0xffffffffu;
     const int lane = threadIdx.x & 31;
