@@ -299,6 +299,10 @@ __global__ void k_fill_i32(int *d, int v, int64_t n) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
         d[i] = v;
 }
+__global__ void k_fill_i4(int4 *d, int4 v, int64_t n) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        d[i] = v;
+}
 __global__ void k_iota_i32(int *d, int start, int64_t n) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
         d[i] = start + (int)i;
@@ -314,6 +318,11 @@ static unsigned grid_for(int64_t n) {
 cudaError_t fill_i32(int *dst, int v, int64_t n, cudaStream_t s) {
     if (n <= 0) return cudaSuccess;
     k_fill_i32<<<grid_for(n), 256, 0, s>>>(dst, v, n);
+    return cudaGetLastError();
+}
+cudaError_t fill_i4(int4 *dst, int4 v, int64_t n, cudaStream_t s) {
+    if (n <= 0) return cudaSuccess;
+    k_fill_i4<<<grid_for(n), 256, 0, s>>>(dst, v, n);
     return cudaGetLastError();
 }
 cudaError_t iota_i32(int *dst, int start, int64_t n, cudaStream_t s) {

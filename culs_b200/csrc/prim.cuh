@@ -60,6 +60,7 @@ cudaError_t radix_sort_pairs(uint32_t *keys, int *vals, uint32_t *keysOut, int *
 
 // Fills dst[0..n) with v.
 cudaError_t fill_i32(int *dst, int v, int64_t n, cudaStream_t s);
+cudaError_t fill_i4(int4 *dst, int4 v, int64_t n, cudaStream_t s);
 // dst[i] = i + start
 cudaError_t iota_i32(int *dst, int start, int64_t n, cudaStream_t s);
 

@@ -10,6 +10,9 @@
 #pragma once
 
 #include "common.cuh"
+#ifdef __CUDACC__
+#include "prim.cuh"
+#endif
 
 namespace culs {
 
@@ -341,18 +344,34 @@ CULS_HD unsigned long long and_key(int in0, int in1, int c0, int c1) {
            ((unsigned long long)c0 << 1) | (unsigned long long)c1;
 }
 
+// A slot holds its key and value in one 16-byte word, so that an insertion's
+// CAS and min, and a lookup's key and value, touch one 32-byte sector.
+// Empty: key kEmptyKey, value kEmptyVal.
+struct alignas(16) AndSlot {
+    unsigned long long key;
+    int val;
+    int pad;
+};
+constexpr int kEmptyVal = 0x7F7F7F7F;
+
 struct AndTable {
-    unsigned long long *keys;
-    int *vals;
+    AndSlot *slots;
     uint32_t mask;  // capacity - 1 (capacity is a power of two)
 };
+
+#ifdef __CUDACC__
+// Empties n slots on stream s.
+inline cudaError_t and_table_clear(AndSlot *slots, int64_t n, cudaStream_t s) {
+    return fill_i4(reinterpret_cast<int4 *>(slots), make_int4(-1, -1, kEmptyVal, 0), n, s);
+}
+#endif
 
 CULS_HD int table_insert(const AndTable &t, unsigned long long key, int val, int *status) {
     uint32_t h = (uint32_t)mix64(key) & t.mask;
     for (uint32_t probe = 0; probe <= t.mask; probe++) {
-        unsigned long long prev = at_cas(&t.keys[h], kEmptyKey, key);
+        unsigned long long prev = at_cas(&t.slots[h].key, kEmptyKey, key);
         if (prev == kEmptyKey || prev == key) {
-            at_min(&t.vals[h], val);
+            at_min(&t.slots[h].val, val);
             return (int)h;
         }
         h = (h + 1) & t.mask;
@@ -365,8 +384,8 @@ CULS_HD int table_insert(const AndTable &t, unsigned long long key, int val, int
 CULS_HD int table_find(const AndTable &t, unsigned long long key, int *status) {
     uint32_t h = (uint32_t)mix64(key) & t.mask;
     for (uint32_t probe = 0; probe <= t.mask; probe++) {
-        unsigned long long k = t.keys[h];
-        if (k == key) return t.vals[h];
+        unsigned long long k = t.slots[h].key;
+        if (k == key) return t.slots[h].val;
         if (k == kEmptyKey) return -1;
         h = (h + 1) & t.mask;
     }

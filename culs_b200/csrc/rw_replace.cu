@@ -209,7 +209,7 @@ __global__ void k_rep_canon(int d, MergeArgs A) {
     for (int64_t T = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; T < A.K; T += stride) {
         if (A.depth[T] != d) continue;
         int sl = A.slot[T];
-        A.canon[T] = sl >= 0 ? A.tab.vals[sl] : (int)T;
+        A.canon[T] = sl >= 0 ? A.tab.slots[sl].val : (int)T;
     }
 }
 
@@ -386,10 +386,9 @@ int rw_replace(ExecCtx &X, Batch &b, RwWork &w) {
         *kpo = ar.get<int>(nCand + 1);
     uint32_t cap = 1024;
     while ((int64_t)cap < 2 * K) cap <<= 1;
-    unsigned long long *tk = ar.get<unsigned long long>(cap);
-    int *tv = ar.get<int>(cap);
+    AndSlot *ts = ar.get<AndSlot>(cap);
     if (!recCand || !r0 || !r1 || !depth || !rc0 || !rc1 || !canon || !f0 || !f1 || !slot || !nph || !c0 || !c1 ||
-        !owner || !newPos || !kp || !kpo || !tk || !tv)
+        !owner || !newPos || !kp || !kpo || !ts)
         return X.fail(CULS_E_OOM, "rw: arena exhausted (replace)");
     A.recCand = recCand;
     A.r0 = r0;
@@ -404,9 +403,8 @@ int rw_replace(ExecCtx &X, Batch &b, RwWork &w) {
     if ((rc = X.sync())) return rc;
     if ((rc = X.status_check("rw replace match"))) return rc;
     const int maxDepth = X.hostSmall[17];
-    if ((rc = X.check(cudaMemsetAsync(tk, 0xFF, sizeof(unsigned long long) * cap, s), "memset"))) return rc;
-    if ((rc = X.check(cudaMemsetAsync(tv, 0x7F, sizeof(int) * cap, s), "memset"))) return rc;
-    MergeArgs Mg{N, K, r0, r1, depth, rc0, rc1, w.wph, canon, nph, f0, f1, c0, c1, slot, AndTable{tk, tv, cap - 1},
+    if ((rc = X.check(and_table_clear(ts, cap, s), "fill"))) return rc;
+    MergeArgs Mg{N, K, r0, r1, depth, rc0, rc1, w.wph, canon, nph, f0, f1, c0, c1, slot, AndTable{ts, cap - 1},
                  X.status};
     for (int d = 1; d <= maxDepth; d++) {
         k_rep_insert<<<X.grid(K), kBlock, 0, s>>>(d, Mg);

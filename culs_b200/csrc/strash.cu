@@ -357,7 +357,7 @@ constexpr int kDedupChunk = kBlock;
 __device__ __forceinline__ int resolve_map(const DedupArgs &A, int u) {
     int e = __ldcg(&A.mapEnc[u]);
     if (e >= 0) return e;
-    int r = __ldcg(&A.tab.vals[-e - 1]);
+    int r = __ldcg(&A.tab.slots[-e - 1].val);
     return 2 * A.posOfRank[r];
 }
 
@@ -563,19 +563,19 @@ __global__ void k_round_resolve(RoundArgs A) {
         const int slot = A.slotT[t];
         if (slot < 0) continue;
         const int v = A.srt[t];
-        const int m = 2 * A.posOfRank[A.tab.vals[slot]];
+        const int m = 2 * A.posOfRank[A.tab.slots[slot].val];
         A.nxt[v] = m;
         if (m != A.cur[v]) *A.changed = 1;
     }
 }
 
-__global__ void k_winner_flags(int64_t n, const int *srt, const int *rankOf, const int *mapEnc, const int *vals,
+__global__ void k_winner_flags(int64_t n, const int *srt, const int *rankOf, const int *mapEnc, const AndSlot *slots,
                                uint8_t *flags) {
     int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += stride) {
         int v = srt[t];
         int e = mapEnc[v];
-        flags[t] = (e < 0 && vals[-e - 1] == rankOf[v]) ? 1 : 0;
+        flags[t] = (e < 0 && slots[-e - 1].val == rankOf[v]) ? 1 : 0;
     }
 }
 
@@ -606,7 +606,9 @@ __global__ void k_winner_local(int64_t n, const int *wlByG, const int *srt, cons
 }
 
 struct OutArgs {
-    const int *srt, *posOfRank, *tOf, *gid, *lidIn, *L0, *kl0, *kl1, *newLocalT, *mapEnc, *vals, *po;
+    const int *srt, *posOfRank, *tOf, *gid, *lidIn, *L0, *kl0, *kl1, *newLocalT, *mapEnc;
+    const AndSlot *slots;
+    const int *po;
     const DevGraph *dgNew;
     int *F0, *F1, *PO;
     int64_t nPO;
@@ -638,7 +640,7 @@ __global__ void k_strash_out(int64_t nW, const int *wl, OutArgs A) {
         int m = lit;
         if (A.L0[u] >= 0) {
             int e = A.mapEnc[u];
-            int base = e >= 0 ? e : 2 * A.posOfRank[A.vals[-e - 1]];
+            int base = e >= 0 ? e : 2 * A.posOfRank[A.slots[-e - 1].val];
             m = base ^ (lit & 1);
         }
         A.PO[k] = local_lit(A, m);
@@ -843,13 +845,12 @@ int Engine::strash_core(Batch &b, int64_t M, const int *L0, const int *L1, const
             cap = std::min(cap, c);
         }
     }
-    unsigned long long *tk = ar_.get<unsigned long long>(cap);
-    int *tv = ar_.get<int>(cap);
+    AndSlot *ts = ar_.get<AndSlot>(cap);
     int *mapEnc = ar_.get<int>(M + 1);
     int *kl0 = ar_.get<int>(nLive + 1), *kl1 = ar_.get<int>(nLive + 1);
     uint8_t *wflags = ar_.get<uint8_t>(nLive + 1);
     int *wl = ar_.get<int>(nLive + 1);
-    if (!tk || !tv || !mapEnc || !kl0 || !kl1 || !wflags || !wl) return fail(CULS_E_OOM, "strash: arena exhausted");
+    if (!ts || !mapEnc || !kl0 || !kl1 || !wflags || !wl) return fail(CULS_E_OOM, "strash: arena exhausted");
     check(cudaMemsetAsync(qc + 5, 0, sizeof(int), s), "memset");
     // Rounds (k_round_*) for batches whose table stays in L2, where they
     // replace one wait latency per level by a few full passes; the level
@@ -872,10 +873,9 @@ int Engine::strash_core(Batch &b, int64_t M, const int *L0, const int *L1, const
         k_round_init<<<gl, kBlock, 0, s>>>(nLive, srt, cur);
         launches_ += 1;
         for (int r = 0; r < kMaxRounds; r++) {
-            check(cudaMemsetAsync(tk, 0xFF, sizeof(unsigned long long) * cap, s), "memset");
-            check(cudaMemsetAsync(tv, 0x7F, sizeof(int) * cap, s), "memset");
+            check(and_table_clear(ts, cap, s), "fill");
             check(cudaMemsetAsync(qc + 16, 0, sizeof(int), s), "memset");
-            RoundArgs R{nLive,  srt,   rankOf, idOrder ? liveIdx : srt, L0, L1, gidA, b.dg, AndTable{tk, tv, cap - 1},
+            RoundArgs R{nLive,  srt,   rankOf, idOrder ? liveIdx : srt, L0, L1, gidA, b.dg, AndTable{ts, cap - 1},
                         cur,    nxt,   slotT,  mapEnc, kl0, kl1, foldTrivial ? 1 : 0, unique ? 1 : 0, qc + 16, status_};
             k_round_insert<<<gl, kBlock, 0, s>>>(R);
             k_round_resolve<<<gl, kBlock, 0, s>>>(R);
@@ -892,12 +892,11 @@ int Engine::strash_core(Batch &b, int64_t M, const int *L0, const int *L1, const
         if (prof_) this->mark(kMkDedupK1);
     }
     if (nLive > 0 && !settled) {
-        check(cudaMemsetAsync(tk, 0xFF, sizeof(unsigned long long) * cap, s), "memset");
-        check(cudaMemsetAsync(tv, 0x7F, sizeof(int) * cap, s), "memset");
+        check(and_table_clear(ts, cap, s), "fill");
         DedupArgs A{nLive,      srt,      rankOf,  idOrder ? liveIdx : srt,
                     L0,         L1,       level,   lvlCnt,
                     lvlStart,   chunkStart, maxLevel, lvlDone,
-                    gidA,       b.dg,     AndTable{tk, tv, cap - 1}, mapEnc,
+                    gidA,       b.dg,     AndTable{ts, cap - 1}, mapEnc,
                     kl0,        kl1,      foldTrivial ? 1 : 0, unique ? 1 : 0,
                     qc + 5,     status_};
         if (prof_) this->mark(kMkDedupK0);
@@ -906,7 +905,7 @@ int Engine::strash_core(Batch &b, int64_t M, const int *L0, const int *L1, const
         launches_ += 1;
     }
     if (nLive > 0) {
-        k_winner_flags<<<grid_1d(nLive, kBlock, sms_ * 16), kBlock, 0, s>>>(nLive, srt, rankOf, mapEnc, tv, wflags);
+        k_winner_flags<<<grid_1d(nLive, kBlock, sms_ * 16), kBlock, 0, s>>>(nLive, srt, rankOf, mapEnc, ts, wflags);
         launches_ += 1;
     }
     check(compact_flags(wflags, nLive, wl, qc + 6, ar_, s), "compact");
@@ -978,7 +977,7 @@ int Engine::strash_core(Batch &b, int64_t M, const int *L0, const int *L1, const
         k_winner_local<<<gw, kBlock, 0, s>>>(nW, wlByG, srt, gidA, gStart, b.dg, newLocalT);
         launches_ += 1;
     }
-    OutArgs O{srt, idOrder ? liveIdx : srt, tOf, gidA, lidIn, L0, kl0, kl1, newLocalT, mapEnc, tv, po, dgNew, F0n, F1n, POn, nPO, G};
+    OutArgs O{srt, idOrder ? liveIdx : srt, tOf, gidA, lidIn, L0, kl0, kl1, newLocalT, mapEnc, ts, po, dgNew, F0n, F1n, POn, nPO, G};
     k_strash_out<<<grid_1d(std::max<int64_t>(std::max<int64_t>(nW, nPO), 1), kBlock, sms_ * 16), kBlock, 0, s>>>(nW, wl,
                                                                                                              O);
     launches_ += 1;
