@@ -1,7 +1,8 @@
 """Proves `rw; st` and `b` equivalence-preserving on the single-graph
 configurations with the z3 SAT-sweeping CEC (oracle/cec.py, the substitute
 for ABC `cec`, which cannot be built here), and records the outcome in
-tests/golden/cec.json.  Runs on the CPU (minutes):
+tests/golden/cec.json.  Runs on the CPU, one process per check (about an
+hour, set by the 64x64 multiplier):
 
     python tests/golden/run_cec.py
 
@@ -35,16 +36,26 @@ def run(g, ops):
     return o.graph()
 
 
+FLOWS = {"rw;st": [lambda o: o.rw(), lambda o: o.st()], "b": [lambda o: o.b()]}
+
+
+def check(job):
+    name, flow = job
+    g = CASES[name]()
+    r = run(g, FLOWS[flow])
+    res = cec(to_oracle(g), r, words=32)
+    res.update({"and_in": g.nAnds, "and_out": r.nAnds, "level_out": r.nLevels})
+    print(name, flow, res, flush=True)
+    return f"{name} {flow}", res
+
+
 def main():
-    out = {}
-    for name, make in CASES.items():
-        g = make()
-        for flow, ops in [("rw;st", [lambda o: o.rw(), lambda o: o.st()]), ("b", [lambda o: o.b()])]:
-            r = run(g, ops)
-            res = cec(to_oracle(g), r, words=32)
-            res.update({"and_in": g.nAnds, "and_out": r.nAnds, "level_out": r.nLevels})
-            out[f"{name} {flow}"] = res
-            print(name, flow, res, flush=True)
+    import multiprocessing as mp
+    jobs = [(name, flow) for name in CASES for flow in FLOWS]
+    # one z3 process per check (the multiplier's take the better part of an hour)
+    with mp.get_context("spawn").Pool(len(jobs)) as pool:
+        out = dict(pool.map(check, jobs))
+    out = {f"{n} {f}": out[f"{n} {f}"] for n, f in jobs}
     (Path(__file__).resolve().parent / "cec.json").write_text(json.dumps(out, indent=1) + "\n")
 
 
