@@ -37,7 +37,7 @@ SERVE_BYTES_PER_OBJ = 720  # device bytes the served mode's admission charges pe
 ST_CPU = 1
 B_NO_STRASH = 1
 STAT_NAMES = ["replaced", "replaced_pos", "replaced_zero", "reverted", "compromised", "pre_eval", "small_cut",
-              "new_idx", "expected", "new_nodes", "candidates", "enum_warp_pairs"]
+              "new_idx", "expected", "new_nodes", "candidates", "enum_warp_pairs", "hash_rounds"]
 DUMPS = ["reorder_f0", "reorder_f1", "reorder_out", "cuts", "selected", "replace", "new_f0", "new_f1", "choice"]
 
 

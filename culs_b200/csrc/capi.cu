@@ -451,9 +451,10 @@ int culs_rw_stats(culs_ctx *ctx, int64_t *out, int n) {
     return culs::guard_call(ctx ? &ctx->err : &g_err, [&]() -> int {
         if (!ctx || !out) return CULS_E_INVALID;
         const culs::RwStats &s = ctx->last;
-        int64_t v[12] = {s.replaced, s.replacedPos, s.replacedZero, s.reverted, s.compromised, s.preEval,
-                         s.smallCut, s.newIdx,      s.expected,     s.newNodes, s.candidates, s.warpPairs};
-        for (int i = 0; i < n && i < 12; i++) out[i] = v[i];
+        int64_t v[13] = {s.replaced, s.replacedPos, s.replacedZero, s.reverted,   s.compromised,
+                         s.preEval,  s.smallCut,    s.newIdx,       s.expected,   s.newNodes,
+                         s.candidates, s.warpPairs, s.hashRounds};
+        for (int i = 0; i < n && i < 13; i++) out[i] = v[i];
         return CULS_OK;
     });
 }

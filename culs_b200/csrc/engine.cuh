@@ -47,6 +47,7 @@ struct RwStats {
     long long replaced, replacedPos, replacedZero, reverted, compromised, preEval, smallCut, newIdx, expected,
         newNodes, candidates;
     long long warpPairs;  // fanin-cut pairs the one-node-per-warp enumeration replayed
+    long long hashRounds; // rounds of the deduplication's hashing (0: the level dataflow)
 };
 
 // Device blocks freed by batches, kept for the next batch of a context (a
@@ -253,6 +254,10 @@ class Engine {
                     const int *procInv = nullptr, const int *procPos = nullptr);
     // strash_core over b's own graph-major arrays (the body of st).
     int strash_batch(Batch &b, bool idOrder, bool removeDangling, bool foldTrivial);
+    // rounds the last strash_core's hashing took to settle; 0 when it ran
+    // as the level dataflow (by size, by CULS_DEDUP_MODE, or because the
+    // rounds did not settle)
+    int hashRounds_ = 0;
 
     std::string err_;
     cudaStream_t s_ = nullptr;

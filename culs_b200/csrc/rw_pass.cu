@@ -199,6 +199,7 @@ int Engine::rw(Batch &b, bool useZeros, bool gpuDedup, RwStats *stats, RwDump *d
         // updateFromRewriteManager(2): GPU strash, which also ends the
         // rewrite manager's state (src/aig_manager.cu:523-546)
         rc = strash_core(b, M, o0, o1, w.gidAll, w.wl, opo, false, true, true, false, false, procInv, procPos);
+        if (stats) stats->hashRounds = hashRounds_;
         b.keep = false;
     } else {
         // updateFromRewriteManager(1): the manager's graph (every node, in
@@ -208,6 +209,7 @@ int Engine::rw(Batch &b, bool useZeros, bool gpuDedup, RwStats *stats, RwDump *d
         if (!rc) rc = check(b.keep_current(s_), "keep");
         if (!rc) {
             rc = strash_batch(b, false, false, false);
+            if (stats) stats->hashRounds = hashRounds_;
             b.keep = rc == 0;
         }
     }

@@ -865,6 +865,7 @@ int Engine::strash_core(Batch &b, int64_t M, const int *L0, const int *L1, const
         if (!strcmp(env, "rounds")) useRounds = nLive > 0;
     }
     bool settled = false;
+    hashRounds_ = 0;
     if (useRounds) {
         int *cur = ar_.get<int>(M + 1), *nxt = ar_.get<int>(M + 1), *slotT = ar_.get<int>(nLive + 1);
         if (!cur || !nxt || !slotT) return fail(CULS_E_OOM, "strash: arena exhausted");
@@ -886,6 +887,7 @@ int Engine::strash_core(Batch &b, int64_t M, const int *L0, const int *L1, const
             std::swap(cur, nxt);
             if (hostSmall_[16] == 0) {
                 settled = true;
+                hashRounds_ = r + 1;
                 break;
             }
         }

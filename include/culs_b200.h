@@ -248,7 +248,8 @@ int culs_autotune(culs_ctx *ctx, const culs_graph *sample, int rounds);
  * gain, replaced with zero gain, reverted, compromised, without a cut, small
  * cut, without a replacement, real reduction, new nodes built, candidates;
  * then (no reference counterpart) the fanin-cut pairs the one-node-per-warp
- * cut enumeration replayed. */
+ * cut enumeration replayed, and the rounds the deduplication's hashing took
+ * to settle (0 when it ran level by level). */
 int culs_rw_stats(culs_ctx *ctx, int64_t *out, int n);
 
 /* Per-node intermediate results of the last culs_rw run with CULS_RW_DUMP,

@@ -67,12 +67,22 @@ def test_hashing_rounds_equal_level_dataflow(gpu_dedup, monkeypatch):
     gs = graphs()
     ctx = C.Context()
     try:
-        got = {}
+        got, rounds = {}, {}
         for mode in ["rounds", "levels"]:
             monkeypatch.setenv("CULS_DEDUP_MODE", mode)
-            got[mode] = run(ctx, gs, gpu_dedup, True)
+            d = ctx.upload_batch(gs)
+            rounds[mode] = []
+            for _ in range(2):
+                ctx.rw(d, gpu_dedup=gpu_dedup)
+                rounds[mode].append(ctx.rw_stats()["hash_rounds"])
+            ctx.st(d)
+            got[mode] = d.download_all()
+            d.free()
     finally:
         ctx.close()
+    # the rounds settled by themselves (the level dataflow did not step in)
+    assert all(1 <= r <= 8 for r in rounds["rounds"]), rounds
+    assert rounds["levels"] == [0, 0], rounds
     for i, g in enumerate(gs):
         assert same_graph(got["rounds"][i], got["levels"][i]), i
         assert same_graph(got["rounds"][i], oracle(g, gpu_dedup, True)), i
