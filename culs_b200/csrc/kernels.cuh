@@ -157,6 +157,29 @@ __device__ __forceinline__ bool queue_round_end(bool fin, bool progressed, int64
     return false;
 }
 
+// Per-block histogram of small keys in shared memory (a few hundred levels
+// for millions of nodes: global counters would serialise in L2).  Usage, by
+// every thread of the block: hist_begin, hist_add per key, hist_end.  With
+// nBins > kHistBins the keys go straight to the global counters.
+constexpr int kHistBins = 4096;
+__device__ __forceinline__ void hist_begin(int *h, int nBins) {
+    if (nBins <= kHistBins)
+        for (int i = threadIdx.x; i < nBins; i += blockDim.x) h[i] = 0;
+    __syncthreads();
+}
+__device__ __forceinline__ void hist_add(int *h, int nBins, int *global, int key) {
+    if (nBins <= kHistBins)
+        atomicAdd(&h[key], 1);
+    else
+        agg_add(global, key, 1);
+}
+__device__ __forceinline__ void hist_end(const int *h, int nBins, int *global) {
+    __syncthreads();
+    if (nBins <= kHistBins)
+        for (int i = threadIdx.x; i < nBins; i += blockDim.x)
+            if (h[i]) atomicAdd(&global[i], h[i]);
+}
+
 // Blocks for a persistent dataflow kernel over a batch `width` nodes wide
 // (Batch::flow_width): enough for about sixteen levels' worth of nodes in
 // flight at itemsPerBlock nodes per block, at least minBlocks (one per SM:

@@ -524,10 +524,14 @@ __global__ void __launch_bounds__(kEnumBlock, 4) k_enumerate(EnumArgs A) {
     }
 }
 
-__global__ void k_level_count(int64_t nL0, int64_t N, const int *wlev, int *lvlCnt) {
+// lvlCnt has nBins counters (levels 0 .. nBins - 1)
+__global__ void k_level_count(int64_t nL0, int64_t N, const int *wlev, int *lvlCnt, int nBins) {
+    __shared__ int h[kHistBins];
+    hist_begin(h, nBins);
     int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t q = nL0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < N; q += stride)
-        agg_add(lvlCnt, wlev[q], 1);
+        hist_add(h, nBins, lvlCnt, wlev[q]);
+    hist_end(h, nBins, lvlCnt);
 }
 
 __global__ void k_level_chunks(int n, const int *lvlCnt, int wideMin, int *cc) {
@@ -560,7 +564,7 @@ int rw_enumerate(ExecCtx &X, RwWork &w) {
         *chunkStart = X.ar->get<int>(L);
     if (!lvlCnt || !lvlStart || !cc || !chunkStart) return X.fail(CULS_E_OOM, "rw: scratch arena exhausted (levels)");
     if ((rc = X.check(cudaMemsetAsync(lvlCnt, 0, sizeof(int) * L, s), "memset"))) return rc;
-    k_level_count<<<X.grid(N - w.nL0), kBlock, 0, s>>>(w.nL0, N, w.wlev, lvlCnt);
+    k_level_count<<<X.grid(N - w.nL0), kBlock, 0, s>>>(w.nL0, N, w.wlev, lvlCnt, w.maxLevel + 1);
     k_level_chunks<<<grid_1d(L, kBlock, X.sms * 16), kBlock, 0, s>>>(L - 1, lvlCnt, X.tune->enumWideMin, cc);
     if ((rc = X.check(scan_exclusive(lvlCnt, lvlStart, L - 1, nullptr, *X.ar, s), "scan"))) return rc;
     if ((rc = X.check(scan_exclusive(cc, chunkStart, L - 1, chunkStart + L - 1, *X.ar, s), "scan"))) return rc;

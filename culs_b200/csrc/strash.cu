@@ -315,13 +315,17 @@ __global__ void k_unresolved_next(int64_t n, const int *idx, const int *list, in
     }
 }
 
-__global__ void k_gather_levels(int64_t n, const int *idx, const int *level, uint32_t *keys, int *lvlCnt) {
+// lvlCnt has nBins counters (levels 0 .. nBins - 1)
+__global__ void k_gather_levels(int64_t n, const int *idx, const int *level, uint32_t *keys, int *lvlCnt, int nBins) {
+    __shared__ int h[kHistBins];
+    hist_begin(h, nBins);
     int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
         int l = level[idx[i]];
         keys[i] = (uint32_t)l;
-        agg_add(lvlCnt, l, 1);
+        hist_add(h, nBins, lvlCnt, l);
     }
+    hist_end(h, nBins, lvlCnt);
 }
 
 __global__ void k_inverse(int64_t n, const int *srt, int *tOf) {
@@ -346,6 +350,7 @@ struct DedupArgs {
     AndTable tab;
     int *mapEnc;  // per position: mapped literal (>= 0) or -(slot+1)
     int *kl0, *kl1;
+    int *slotT;   // per processing index: table slot, -1 when folded
     int foldTrivial;
     int unique;  // key each node by its position: nothing merges
     int *counter;
@@ -450,6 +455,7 @@ __global__ void __launch_bounds__(kDedupChunk) k_dedup(DedupArgs A) {
             }
             if (triv >= 0) {
                 A.mapEnc[v] = triv;
+                A.slotT[t] = -1;
             } else {
                 // literals are non-negative, so a key with the top bit set
                 // is never a real one
@@ -459,6 +465,7 @@ __global__ void __launch_bounds__(kDedupChunk) k_dedup(DedupArgs A) {
                 A.kl0[t] = l0;
                 A.kl1[t] = l1;
                 A.mapEnc[v] = slot >= 0 ? -(slot + 1) : 0;
+                A.slotT[t] = slot;
             }
         }
         __threadfence();
@@ -569,13 +576,15 @@ __global__ void k_round_resolve(RoundArgs A) {
     }
 }
 
-__global__ void k_winner_flags(int64_t n, const int *srt, const int *rankOf, const int *mapEnc, const AndSlot *slots,
-                               uint8_t *flags) {
+// A node wins when its key's lowest rank is its own: its rank is its
+// processing index, or (id order) rankOf of its position.
+__global__ void k_winner_flags(int64_t n, const int *srt, const int *rankOf, bool idOrder, const int *slotT,
+                               const AndSlot *slots, uint8_t *flags) {
     int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += stride) {
-        int v = srt[t];
-        int e = mapEnc[v];
-        flags[t] = (e < 0 && slots[-e - 1].val == rankOf[v]) ? 1 : 0;
+        const int slot = slotT[t];
+        const int rank = idOrder ? rankOf[srt[t]] : (int)t;
+        flags[t] = (slot >= 0 && slots[slot].val == rank) ? 1 : 0;
     }
 }
 
@@ -817,7 +826,7 @@ int Engine::strash_core(Batch &b, int64_t M, const int *L0, const int *L1, const
     check(cudaMemsetAsync(lvlDone, 0, sizeof(int) * (maxLevel + 2), s), "memset");
     if (nLive > 0) {
         unsigned gl = grid_1d(nLive, kBlock, sms_ * 16);
-        k_gather_levels<<<gl, kBlock, 0, s>>>(nLive, liveIdx, level, keys, lvlCnt);
+        k_gather_levels<<<gl, kBlock, 0, s>>>(nLive, liveIdx, level, keys, lvlCnt, maxLevel + 1);
         int bits = 1;
         while ((1ll << bits) <= maxLevel) bits++;
         check(cudaMemcpyAsync(vals2, liveIdx, sizeof(int) * nLive, cudaMemcpyDeviceToDevice, s), "copy");
@@ -866,9 +875,11 @@ int Engine::strash_core(Batch &b, int64_t M, const int *L0, const int *L1, const
     }
     bool settled = false;
     hashRounds_ = 0;
+    int *slotT = ar_.get<int>(nLive + 1);
+    if (!slotT) return fail(CULS_E_OOM, "strash: arena exhausted");
     if (useRounds) {
-        int *cur = ar_.get<int>(M + 1), *nxt = ar_.get<int>(M + 1), *slotT = ar_.get<int>(nLive + 1);
-        if (!cur || !nxt || !slotT) return fail(CULS_E_OOM, "strash: arena exhausted");
+        int *cur = ar_.get<int>(M + 1), *nxt = ar_.get<int>(M + 1);
+        if (!cur || !nxt) return fail(CULS_E_OOM, "strash: arena exhausted");
         const unsigned gl = grid_1d(nLive, kBlock, sms_ * 16);
         if (prof_) this->mark(kMkDedupK0);
         k_round_init<<<gl, kBlock, 0, s>>>(nLive, srt, cur);
@@ -899,7 +910,7 @@ int Engine::strash_core(Batch &b, int64_t M, const int *L0, const int *L1, const
                     L0,         L1,       level,   lvlCnt,
                     lvlStart,   chunkStart, maxLevel, lvlDone,
                     gidA,       b.dg,     AndTable{ts, cap - 1}, mapEnc,
-                    kl0,        kl1,      foldTrivial ? 1 : 0, unique ? 1 : 0,
+                    kl0,        kl1,      slotT,   foldTrivial ? 1 : 0, unique ? 1 : 0,
                     qc + 5,     status_};
         if (prof_) this->mark(kMkDedupK0);
         k_dedup<<<gridQ, kBlock, 0, s>>>(A);
@@ -907,7 +918,7 @@ int Engine::strash_core(Batch &b, int64_t M, const int *L0, const int *L1, const
         launches_ += 1;
     }
     if (nLive > 0) {
-        k_winner_flags<<<grid_1d(nLive, kBlock, sms_ * 16), kBlock, 0, s>>>(nLive, srt, rankOf, mapEnc, ts, wflags);
+        k_winner_flags<<<grid_1d(nLive, kBlock, sms_ * 16), kBlock, 0, s>>>(nLive, srt, rankOf, idOrder, slotT, ts, wflags);
         launches_ += 1;
     }
     check(compact_flags(wflags, nLive, wl, qc + 6, ar_, s), "compact");
