@@ -43,6 +43,7 @@ CULS_HD int lit_c(int lit) { return lit & 1; }
 CULS_DEV int at_add(int *p, int v) { return atomicAdd(p, v); }
 CULS_DEV unsigned long long at_add(unsigned long long *p, unsigned long long v) { return atomicAdd(p, v); }
 CULS_DEV int at_min(int *p, int v) { return atomicMin(p, v); }
+CULS_DEV unsigned long long at_min(unsigned long long *p, unsigned long long v) { return atomicMin(p, v); }
 CULS_DEV int at_cas(int *p, int cmp, int v) { return atomicCAS(p, cmp, v); }
 CULS_DEV unsigned long long at_cas(unsigned long long *p, unsigned long long cmp, unsigned long long v) {
     return atomicCAS(p, cmp, v);
@@ -82,6 +83,11 @@ inline unsigned long long at_add(unsigned long long *p, unsigned long long v) {
 }
 inline int at_min(int *p, int v) {
     int o = *p;
+    if (v < o) *p = v;
+    return o;
+}
+inline unsigned long long at_min(unsigned long long *p, unsigned long long v) {
+    unsigned long long o = *p;
     if (v < o) *p = v;
     return o;
 }

@@ -344,15 +344,18 @@ CULS_HD unsigned long long and_key(int in0, int in1, int c0, int c1) {
            ((unsigned long long)c0 << 1) | (unsigned long long)c1;
 }
 
-// A slot holds its key and value in one 16-byte word, so that an insertion's
-// CAS and min, and a lookup's key and value, touch one 32-byte sector.
-// Empty: key kEmptyKey, value kEmptyVal.
+// A slot holds its key and, in one 64-bit word, the lowest rank inserted
+// with it and that insertion's position (rank << 32 | position), so that an
+// insertion's CAS and min touch one 32-byte sector and a lookup finds the
+// winner's position without a rank-to-position table.  Empty: key
+// kEmptyKey, rank and position kEmptyRp.
 struct alignas(16) AndSlot {
     unsigned long long key;
-    int val;
-    int pad;
+    unsigned long long rp;
 };
-constexpr int kEmptyVal = 0x7F7F7F7F;
+constexpr unsigned long long kEmptyRp = 0x7F7F7F7F7F7F7F7Full;
+CULS_HD int slot_rank(unsigned long long rp) { return (int)(rp >> 32); }
+CULS_HD int slot_pos(unsigned long long rp) { return (int)(uint32_t)rp; }
 
 struct AndTable {
     AndSlot *slots;
@@ -362,16 +365,19 @@ struct AndTable {
 #ifdef __CUDACC__
 // Empties n slots on stream s.
 inline cudaError_t and_table_clear(AndSlot *slots, int64_t n, cudaStream_t s) {
-    return fill_i4(reinterpret_cast<int4 *>(slots), make_int4(-1, -1, kEmptyVal, 0), n, s);
+    return fill_i4(reinterpret_cast<int4 *>(slots), make_int4(-1, -1, 0x7F7F7F7F, 0x7F7F7F7F), n, s);
 }
 #endif
 
-CULS_HD int table_insert(const AndTable &t, unsigned long long key, int val, int *status) {
+// Inserts key with (rank, pos): the slot keeps the lowest rank and its
+// position.  Returns the slot, or -1 (and kDevTableFull) when the probe
+// sequence runs out.
+CULS_HD int table_insert(const AndTable &t, unsigned long long key, int rank, int pos, int *status) {
     uint32_t h = (uint32_t)mix64(key) & t.mask;
     for (uint32_t probe = 0; probe <= t.mask; probe++) {
         unsigned long long prev = at_cas(&t.slots[h].key, kEmptyKey, key);
         if (prev == kEmptyKey || prev == key) {
-            at_min(&t.slots[h].val, val);
+            at_min(&t.slots[h].rp, ((unsigned long long)(uint32_t)rank << 32) | (uint32_t)pos);
             return (int)h;
         }
         h = (h + 1) & t.mask;
@@ -380,12 +386,12 @@ CULS_HD int table_insert(const AndTable &t, unsigned long long key, int val, int
     return -1;
 }
 
-// Returns the value stored for key, or -1 when absent.
+// Returns the lowest rank stored for key, or -1 when absent.
 CULS_HD int table_find(const AndTable &t, unsigned long long key, int *status) {
     uint32_t h = (uint32_t)mix64(key) & t.mask;
     for (uint32_t probe = 0; probe <= t.mask; probe++) {
         unsigned long long k = t.slots[h].key;
-        if (k == key) return t.slots[h].val;
+        if (k == key) return slot_rank(t.slots[h].rp);
         if (k == kEmptyKey) return -1;
         h = (h + 1) & t.mask;
     }

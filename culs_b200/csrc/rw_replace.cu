@@ -200,7 +200,7 @@ __global__ void k_rep_insert(int d, MergeArgs A) {
         A.f1[T] = f1;
         A.c0[T] = (uint8_t)c0;
         A.c1[T] = (uint8_t)c1;
-        A.slot[T] = table_insert(A.tab, and_key(f0, f1, c0, c1), (int)T, A.status);
+        A.slot[T] = table_insert(A.tab, and_key(f0, f1, c0, c1), (int)T, (int)T, A.status);
     }
 }
 
@@ -209,7 +209,7 @@ __global__ void k_rep_canon(int d, MergeArgs A) {
     for (int64_t T = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; T < A.K; T += stride) {
         if (A.depth[T] != d) continue;
         int sl = A.slot[T];
-        A.canon[T] = sl >= 0 ? A.tab.slots[sl].val : (int)T;
+        A.canon[T] = sl >= 0 ? slot_rank(A.tab.slots[sl].rp) : (int)T;
     }
 }
 

@@ -337,7 +337,6 @@ struct DedupArgs {
     int64_t nLive;
     const int *srt;        // live AND positions in processing order
     const int *rankOf;     // per position: tentative rank (min wins)
-    const int *posOfRank;  // rank -> position
     const int *L0, *L1;
     const int *level;
     const int *lvlCnt;     // live AND nodes per level
@@ -362,8 +361,7 @@ constexpr int kDedupChunk = kBlock;
 __device__ __forceinline__ int resolve_map(const DedupArgs &A, int u) {
     int e = __ldcg(&A.mapEnc[u]);
     if (e >= 0) return e;
-    int r = __ldcg(&A.tab.slots[-e - 1].val);
-    return 2 * A.posOfRank[r];
+    return 2 * slot_pos(__ldcg(&A.tab.slots[-e - 1].rp));
 }
 
 // chunks per level, for the level-aligned claim order of k_dedup
@@ -461,7 +459,7 @@ __global__ void __launch_bounds__(kDedupChunk) k_dedup(DedupArgs A) {
                 // is never a real one
                 const unsigned long long key = A.unique ? (1ull << 63) | (unsigned long long)(uint32_t)v
                                                         : ((unsigned long long)(uint32_t)l0 << 32) | (uint32_t)l1;
-                int slot = table_insert(A.tab, key, A.rankOf[v], A.status);
+                int slot = table_insert(A.tab, key, A.rankOf[v], v, A.status);
                 A.kl0[t] = l0;
                 A.kl1[t] = l1;
                 A.mapEnc[v] = slot >= 0 ? -(slot + 1) : 0;
@@ -492,7 +490,7 @@ __global__ void __launch_bounds__(kDedupChunk) k_dedup(DedupArgs A) {
 
 struct RoundArgs {
     int64_t nLive;
-    const int *srt, *rankOf, *posOfRank;
+    const int *srt, *rankOf;
     const int *L0, *L1;
     const int *gid;
     const DevGraph *dg;
@@ -554,7 +552,7 @@ __global__ void k_round_insert(RoundArgs A) {
         } else {
             const unsigned long long key = A.unique ? (1ull << 63) | (unsigned long long)(uint32_t)v
                                                     : ((unsigned long long)(uint32_t)l0 << 32) | (uint32_t)l1;
-            const int slot = table_insert(A.tab, key, A.rankOf[v], A.status);
+            const int slot = table_insert(A.tab, key, A.rankOf[v], v, A.status);
             A.kl0[t] = l0;
             A.kl1[t] = l1;
             A.mapEnc[v] = slot >= 0 ? -(slot + 1) : 0;
@@ -570,7 +568,7 @@ __global__ void k_round_resolve(RoundArgs A) {
         const int slot = A.slotT[t];
         if (slot < 0) continue;
         const int v = A.srt[t];
-        const int m = 2 * A.posOfRank[A.tab.slots[slot].val];
+        const int m = 2 * slot_pos(A.tab.slots[slot].rp);
         A.nxt[v] = m;
         if (m != A.cur[v]) *A.changed = 1;
     }
@@ -584,7 +582,7 @@ __global__ void k_winner_flags(int64_t n, const int *srt, const int *rankOf, boo
     for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += stride) {
         const int slot = slotT[t];
         const int rank = idOrder ? rankOf[srt[t]] : (int)t;
-        flags[t] = (slot >= 0 && slots[slot].val == rank) ? 1 : 0;
+        flags[t] = (slot >= 0 && slot_rank(slots[slot].rp) == rank) ? 1 : 0;
     }
 }
 
@@ -615,7 +613,7 @@ __global__ void k_winner_local(int64_t n, const int *wlByG, const int *srt, cons
 }
 
 struct OutArgs {
-    const int *srt, *posOfRank, *tOf, *gid, *lidIn, *L0, *kl0, *kl1, *newLocalT, *mapEnc;
+    const int *srt, *tOf, *gid, *lidIn, *L0, *kl0, *kl1, *newLocalT, *mapEnc;
     const AndSlot *slots;
     const int *po;
     const DevGraph *dgNew;
@@ -649,7 +647,7 @@ __global__ void k_strash_out(int64_t nW, const int *wl, OutArgs A) {
         int m = lit;
         if (A.L0[u] >= 0) {
             int e = A.mapEnc[u];
-            int base = e >= 0 ? e : 2 * A.posOfRank[A.slots[-e - 1].val];
+            int base = e >= 0 ? e : 2 * slot_pos(A.slots[-e - 1].rp);
             m = base ^ (lit & 1);
         }
         A.PO[k] = local_lit(A, m);
@@ -887,7 +885,7 @@ int Engine::strash_core(Batch &b, int64_t M, const int *L0, const int *L1, const
         for (int r = 0; r < kMaxRounds; r++) {
             check(and_table_clear(ts, cap, s), "fill");
             check(cudaMemsetAsync(qc + 16, 0, sizeof(int), s), "memset");
-            RoundArgs R{nLive,  srt,   rankOf, idOrder ? liveIdx : srt, L0, L1, gidA, b.dg, AndTable{ts, cap - 1},
+            RoundArgs R{nLive,  srt,   rankOf, L0, L1, gidA, b.dg, AndTable{ts, cap - 1},
                         cur,    nxt,   slotT,  mapEnc, kl0, kl1, foldTrivial ? 1 : 0, unique ? 1 : 0, qc + 16, status_};
             k_round_insert<<<gl, kBlock, 0, s>>>(R);
             k_round_resolve<<<gl, kBlock, 0, s>>>(R);
@@ -906,7 +904,7 @@ int Engine::strash_core(Batch &b, int64_t M, const int *L0, const int *L1, const
     }
     if (nLive > 0 && !settled) {
         check(and_table_clear(ts, cap, s), "fill");
-        DedupArgs A{nLive,      srt,      rankOf,  idOrder ? liveIdx : srt,
+        DedupArgs A{nLive,      srt,      rankOf,
                     L0,         L1,       level,   lvlCnt,
                     lvlStart,   chunkStart, maxLevel, lvlDone,
                     gidA,       b.dg,     AndTable{ts, cap - 1}, mapEnc,
@@ -990,7 +988,7 @@ int Engine::strash_core(Batch &b, int64_t M, const int *L0, const int *L1, const
         k_winner_local<<<gw, kBlock, 0, s>>>(nW, wlByG, srt, gidA, gStart, b.dg, newLocalT);
         launches_ += 1;
     }
-    OutArgs O{srt, idOrder ? liveIdx : srt, tOf, gidA, lidIn, L0, kl0, kl1, newLocalT, mapEnc, ts, po, dgNew, F0n, F1n, POn, nPO, G};
+    OutArgs O{srt, tOf, gidA, lidIn, L0, kl0, kl1, newLocalT, mapEnc, ts, po, dgNew, F0n, F1n, POn, nPO, G};
     k_strash_out<<<grid_1d(std::max<int64_t>(std::max<int64_t>(nW, nPO), 1), kBlock, sms_ * 16), kBlock, 0, s>>>(nW, wl,
                                                                                                              O);
     launches_ += 1;
