@@ -279,7 +279,7 @@ class Context:
                                         ST_CPU if cpu_st else 0), "rw;st batch")
 
     # ---- tuning (speed only; results never change)
-    PARAMS = {"enum_wide_min": 1, "enum_blocks_per_sm": 2, "sm_share": 4, "high_priority": 5}
+    PARAMS = {"enum_wide_min": 1, "enum_blocks_per_sm": 2, "sm_share": 4, "high_priority": 5, "eval_group_mslots": 6}
 
     def set_param(self, name, value):
         self._err(_lib.culs_set_param(self.h, self.PARAMS[name], value), f"set_param {name}")

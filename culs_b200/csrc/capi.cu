@@ -418,6 +418,10 @@ int culs_set_param(culs_ctx *ctx, int which, int64_t value) {
             case CULS_PARAM_HIGH_PRIORITY:
                 if (value != 0 && value != 1) return CULS_E_INVALID;
                 return set_err(ctx, ctx->eng.set_high_priority(value != 0));
+            case CULS_PARAM_EVAL_GROUP_MSLOTS:
+                if (value < 1 || value > 1024) return CULS_E_INVALID;
+                t.evalGroupMSlots = (int)value;
+                return CULS_OK;
             default:
                 return CULS_E_INVALID;
         }
@@ -434,6 +438,7 @@ int culs_get_param(culs_ctx *ctx, int which, int64_t *value) {
             case CULS_PARAM_ENUM_BLOCKS_PER_SM: *value = t.enumBlocksPerSm; return CULS_OK;
             case CULS_PARAM_SM_SHARE: *value = ctx->eng.sm_share(); return CULS_OK;
             case CULS_PARAM_HIGH_PRIORITY: *value = ctx->eng.high_priority() ? 1 : 0; return CULS_OK;
+            case CULS_PARAM_EVAL_GROUP_MSLOTS: *value = t.evalGroupMSlots; return CULS_OK;
             default: return CULS_E_INVALID;
         }
     });

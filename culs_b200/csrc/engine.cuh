@@ -32,6 +32,7 @@ struct ExecCtx;
 struct Tune {
     int enumWideMin = 16384;   // levels this wide run one node per thread, narrower one per warp
     int enumBlocksPerSm = 8;   // persistent enumeration blocks per SM
+    int evalGroupMSlots = 16;  // existence-table slots (millions) of a group of graphs built and evaluated together
 };
 
 struct DevGraph {
@@ -186,11 +187,11 @@ class Engine {
     // that `share` engines running at once (the served workers) overlap on
     // the GPU instead of queueing behind one another's persistent kernels.
     // Persistent kernels get one resident wave of blocks on that share (the
-    // enumeration's blocks fit 3 to an SM).
+    // enumeration's blocks fit 4 to an SM).
     void set_sm_share(int share) {
         share_ = std::max(1, share);
         sms_ = std::max(8, num_sms() / share_);
-        if (share_ > 1) tune_.enumBlocksPerSm = std::min(tune_.enumBlocksPerSm, 3);
+        if (share_ > 1) tune_.enumBlocksPerSm = std::min(tune_.enumBlocksPerSm, 4);
     }
     int sm_share() const { return share_; }
     // Recreates the engine's stream at the device's highest stream priority

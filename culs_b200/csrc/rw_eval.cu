@@ -292,11 +292,12 @@ int rw_evaluate(ExecCtx &X, RwWork &w, const Batch &b) {
     if (nAnd > 0) {
         k_table_clear<<<X.grid(nSlots), kBlock, 0, s>>>(nSlots, slots);
         X.mark(kMkEvalK0);
-        // Graphs in groups of at most kGroupSlots table slots (256 MB of
-        // regions), each group's regions built right before its nodes are
-        // evaluated, so the probes find them in L2 instead of DRAM (a single
-        // larger graph is a group of its own).
-        constexpr int64_t kGroupSlots = 16ll << 20;
+        // Graphs in groups of at most kGroupSlots table slots (16M by
+        // default: 256 MB of regions; a tuned parameter), each group's
+        // regions built right before its nodes are evaluated, so the probes
+        // find them in L2 instead of DRAM (a single larger graph is a group
+        // of its own).
+        const int64_t kGroupSlots = (int64_t)X.tune->evalGroupMSlots << 20;
         const bool lev16 = w.maxLevel + 64 < 0xFFFF;  // see the launch below
         int g0 = 0;
         while (g0 < w.G) {

@@ -6,7 +6,9 @@
 // workload's level widths and depths, so it is chosen by timing rw's cut
 // enumeration (device events around the kernel) on clones of a sample of
 // the workload: first the width threshold at the default grid, then the
-// grid at the chosen threshold.
+// grid at the chosen threshold.  Then the evaluation's group size (how many
+// graphs' existence tables are built and probed together, which decides
+// whether they stay in L2), timed on the evaluation's marks.
 #include <cfloat>
 
 #include "engine.cuh"
@@ -19,6 +21,8 @@ int Engine::autotune(const Batch &sample, int rounds) {
     const bool prof = prof_;
     prof_ = true;
     Batch work;
+    // rw's time between marks m0 and m1, the best of `rounds` runs
+    int m0 = kMkEnumK0, m1 = kMkEnumK1;
     auto measure = [&](const Tune &t, float &ms) -> int {
         tune_ = t;
         ms = FLT_MAX;
@@ -27,7 +31,7 @@ int Engine::autotune(const Batch &sample, int rounds) {
             RwStats st{};
             if (rc == CULS_OK) rc = rw(work, false, true, &st, nullptr);
             if (rc != CULS_OK) return rc;
-            const float e = elapsed(kMkEnumK0, kMkEnumK1);
+            const float e = elapsed(m0, m1);
             if (e >= 0.f && e < ms) ms = e;
         }
         return CULS_OK;
@@ -59,6 +63,25 @@ int Engine::autotune(const Batch &sample, int rounds) {
         if (rc) break;
         Tune t = best;
         t.enumBlocksPerSm = b;
+        float ms;
+        if ((rc = measure(t, ms))) break;
+        if (ms < bestMs) {
+            bestMs = ms;
+            best = t;
+        }
+    }
+    // the evaluation's group size, at the chosen enumeration schedule
+    m0 = kMkEvalK0, m1 = kMkEvalK1;
+    if (!rc) {
+        float ms;
+        rc = measure(best, ms);
+        bestMs = ms;
+    }
+    const int groups[] = {4, 8, 32, 64};
+    for (int gm : groups) {
+        if (rc) break;
+        Tune t = best;
+        t.evalGroupMSlots = gm;
         float ms;
         if ((rc = measure(t, ms))) break;
         if (ms < bestMs) {

@@ -229,16 +229,20 @@ int culs_fetch_aiger(culs_ctx *ctx, int64_t job, uint8_t *buf, size_t cap, size_
  * blocks per SM (default 8).  CULS_PARAM_SM_SHARE: size every grid of the
  * context for 1/value of the device's SMs (default 1), for contexts that run
  * at once on one GPU (the served workers use their share); setting it also
- * caps the enumeration blocks per SM at 3, one resident wave.
+ * caps the enumeration blocks per SM at 4, one resident wave.
  * CULS_PARAM_HIGH_PRIORITY: 1 runs the context's work on a stream of the
  * device's highest priority, 0 (default) on a default-priority stream.
- * culs_autotune times rw's enumeration on
- * clones of `sample` (left unchanged) for candidate values, `rounds` times
- * each, and keeps the fastest in the context.  No reference counterpart. */
+ * CULS_PARAM_EVAL_GROUP_MSLOTS: the evaluation builds and probes the
+ * existence tables of groups of graphs whose tables hold at most this many
+ * million slots (default 16), so that a group's tables stay in L2.
+ * culs_autotune times rw's enumeration, then its evaluation, on clones of
+ * `sample` (left unchanged) for candidate values, `rounds` times each, and
+ * keeps the fastest in the context.  No reference counterpart. */
 #define CULS_PARAM_ENUM_WIDE_MIN 1
 #define CULS_PARAM_ENUM_BLOCKS_PER_SM 2
 #define CULS_PARAM_SM_SHARE 4
 #define CULS_PARAM_HIGH_PRIORITY 5
+#define CULS_PARAM_EVAL_GROUP_MSLOTS 6
 int culs_set_param(culs_ctx *ctx, int which, int64_t value);
 int culs_get_param(culs_ctx *ctx, int which, int64_t *value);
 int culs_autotune(culs_ctx *ctx, const culs_graph *sample, int rounds);

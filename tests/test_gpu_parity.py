@@ -423,8 +423,27 @@ def test_autotune_keeps_results():
         chosen = c.autotune(sample)
         assert chosen["enum_wide_min"] in (2048, 4096, 8192, 16384, 32768, 65536, 1 << 30)
         assert chosen["enum_blocks_per_sm"] in (4, 6, 8, 12, 16)
+        assert chosen["eval_group_mslots"] in (4, 8, 16, 32, 64)
         c.rw_st(sample)  # the sample itself is left unchanged by the tuner
         for i, g in enumerate(gs):
             assert same_graph(sample.download(i), oracle_rw_st(g).graph()), i
+    finally:
+        c.close()
+
+
+def test_evaluation_groups_do_not_change_results():
+    """The evaluation builds and probes the existence tables of a group of
+    graphs at a time (a speed parameter): groups of at most 1M table slots
+    split this 36-graph batch (3.3M slots) into four, with the oracle's
+    graphs as the result."""
+    c = C.Context()
+    try:
+        c.set_param("eval_group_mslots", 1)
+        assert c.get_param("eval_group_mslots") == 1
+        gs = C.gen_batch(4, 500, 36, 5000, 60000, 16, 512, threads=8)
+        db = c.upload_batch(gs)
+        c.rw_st(db)
+        for i, g in enumerate(gs):
+            assert same_graph(db.download(i), oracle_rw_st(g).graph()), i
     finally:
         c.close()
