@@ -298,14 +298,10 @@ __device__ __forceinline__ void enum_node_warp(const EnumArgs &A, int64_t q, int
             }
         }
         __syncwarp();
-        for (int k = 0; k < nPairs; k++) {
+        int k = 0;
+        for (; k < nPairs; k++) {
             Cand m;
             get_cand(sc[k], m);
-            // Count the pair.  Besides the statistic, this atomic is
-            // measured to make this loop run 3.4x faster on B200 (64x64
-            // multiplier: 37.7 -> 11 ms; the instruction count drops 2.9x);
-            // a plain store or a compiler barrier in its place does not.
-            if (lane == 0) atomicAdd(A.warpPairs, 1ull);
             // FindCut (rewrite.cu:84-109): the first free slot, else the
             // lowest (class, value, index); both computed, one kept
             const unsigned freeSlots = __ballot_sync(F, lane < 8 && !packed_used(spk)) & 0xFFu;
@@ -344,8 +340,12 @@ __device__ __forceinline__ void enum_node_warp(const EnumArgs &A, int64_t q, int
             pc.value = m.yval;
             pc.used = keep ? 1u : 0u;
             if (lane == id) spk = cut_pack(pc);
-            if (m.yn < 2) break;  // enumeration of this node stops (rewrite.cu:291)
+            if (m.yn < 2) {  // enumeration of this node stops (rewrite.cu:291)
+                k++;
+                break;
+            }
         }
+        if (lane == 0 && k > 0) atomicAdd(A.warpPairs, (unsigned long long)k);  // pairs replayed
     }
     if (lane < 8) {
         A.cutL[q * 8 + lane] = make_int4(sl[0], sl[1], sl[2], sl[3]);
