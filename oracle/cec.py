@@ -1,9 +1,9 @@
 """Combinational equivalence check of two AIGs by SAT sweeping with z3.
 
-TEST INFRASTRUCTURE.  ABC's `cec` (which BASELINE.json's north_star names)
-cannot be built here: the reference's ABC submodule is empty.  This is the
-substitute the survey planned, reported under its own name ("z3 SAT-sweeping
-CEC"), not as ABC:
+TEST INFRASTRUCTURE.  ABC's `cec`, the check the reference's users run,
+cannot be built here: the reference's ABC submodule is empty.  This is a
+substitute, reported under its own name ("z3 SAT-sweeping CEC"), not as
+ABC:
 
 1. both AIGs (AIGMan convention: literal 0 = TRUE) share their PIs and are
    simulated on random 64-bit patterns, every node of both;

@@ -34,9 +34,9 @@ HARNESS = ROOT / "oracle" / "_ref" / "rw_harness"
 FULL_LIMIT = 6000  # objects: store full per-node arrays up to this size
 
 CASES = {
-    # 64 PIs, 32 POs, 5,000 ANDs in 40 layers, window 4 + PIs
+    # the 5,000-AND layered graph: 64 PIs, 32 POs, 5,000 ANDs in 40 layers, window 4 + PIs
     "c1_layered5k": lambda: C.gen_layered(1, 64, 32, 5000, 40, 4, 0.0, True),
-    # 64x64 array multiplier
+    # the 64x64 array multiplier
     "c2_mult64": lambda: C.gen_multiplier(64),
     "mult8": lambda: C.gen_multiplier(8),
     "mult16": lambda: C.gen_multiplier(16),

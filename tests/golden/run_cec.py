@@ -23,8 +23,8 @@ from oracle.oracle import Oracle  # noqa: E402
 from util import to_oracle  # noqa: E402
 
 CASES = {
-    "c1_layered5k (configs[0])": lambda: C.gen_layered(1, 64, 32, 5000, 40, 4, 0.0, True),
-    "c2_mult64 (configs[1])": lambda: C.gen_multiplier(64),
+    "c1_layered5k": lambda: C.gen_layered(1, 64, 32, 5000, 40, 4, 0.0, True),
+    "c2_mult64x64": lambda: C.gen_multiplier(64),
 }
 
 
