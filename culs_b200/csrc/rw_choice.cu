@@ -223,40 +223,54 @@ __device__ __forceinline__ void fd_open(const Mem &m, int l0, int l1, int &v0, i
     v0 = c0 == c1 ? v1 : o0 - 1;  // one node twice: both decrements precede the first check
 }
 
-// FastDelete, rewrite.h:208-220; r0, r1 = L0, L1 of root
+// FastDelete, rewrite.h:208-220; r0, r1 = L0, L1 of root.  The recursion
+// replayed with an explicit stack: a node is opened (both fanins'
+// decrements), then its fanin 0 entered if its count fell to zero, then --
+// with fanin 1's count read again, since fanin 0's subtree may have changed
+// it -- its fanin 1, then it is marked deleted and its count handed to its
+// parent.  A pushed frame is {node, count << 2 | where to resume (1: at
+// fanin 1, 2: at the end), fanin0 literal, fanin1 literal}.
 template <class Mem>
 __device__ int ch_fast_delete(const GraphCtx<Mem> &C, int root, int r0, int r1) {
     const Mem &m = C.m;
     if (root < C.nL0) return 0;
     int v0, a0, b0, v1, a1, b1;
-    fd_open(m, r0, r1, v0, a0, b0, v1, a1, b1);
-    int4 f = make_int4(root, 1 | ((1 - ch_red(C, root, r0, r1)) << 2), r0, r1);
-    int sp = 0;
+    int x = root, l0 = r0, l1 = r1, sp = 0;
+    fd_open(m, l0, l1, v0, a0, b0, v1, a1, b1);
+    int cnt = 1 - ch_red(C, x, l0, l1);
     while (true) {
-        const int step = f.y & 3;
-        if (step < 3) {
-            const int child = (step == 1 ? f.z : f.w) >> 1;
-            const int r = step == 1 ? v0 : v1, c0 = step == 1 ? a0 : a1, c1 = step == 1 ? b0 : b1;
-            f.y++;
-            if (r == 0 && child >= C.nL0) {
+        // x is open: enter fanin 0 when its count fell to zero
+        if (v0 == 0 && (l0 >> 1) >= C.nL0) {
+            if (sp + 1 >= C.stackCap) {
+                set_status(C.status, kDevStackOverflow);
+                return 0;
+            }
+            C.push(sp++, make_int4(x, (cnt << 2) | 1, l0, l1));
+            x = l0 >> 1, l0 = a0, l1 = b0;
+            fd_open(m, l0, l1, v0, a0, b0, v1, a1, b1);
+            cnt = 1 - ch_red(C, x, l0, l1);
+            continue;
+        }
+        int resume = 1;  // 1: at fanin 1 of x, 2: x is finished
+        while (true) {
+            if (resume == 1 && v1 == 0 && (l1 >> 1) >= C.nL0) {
                 if (sp + 1 >= C.stackCap) {
                     set_status(C.status, kDevStackOverflow);
                     return 0;
                 }
-                fd_open(m, c0, c1, v0, a0, b0, v1, a1, b1);
-                C.push(sp++, f);
-                f = make_int4(child, 1 | ((1 - ch_red(C, child, c0, c1)) << 2), c0, c1);
+                C.push(sp++, make_int4(x, (cnt << 2) | 2, l0, l1));
+                x = l1 >> 1, l0 = a1, l1 = b1;
+                fd_open(m, l0, l1, v0, a0, b0, v1, a1, b1);
+                cnt = 1 - ch_red(C, x, l0, l1);
+                break;  // the new node is open
             }
-            continue;
-        }
-        m.set_del(f.x, 1);
-        const int cnt = f.y >> 2;
-        if (sp == 0) return cnt;
-        f = C.pop(--sp);
-        f.y += cnt << 2;
-        if ((f.y & 3) == 2) {  // resumes at fanin 1 after fanin 0's subtree
-            const int c = f.w >> 1;
-            m.rab(c, v1, a1, b1);
+            m.set_del(x, 1);
+            if (sp == 0) return cnt;
+            const int4 f = C.pop(--sp);
+            x = f.x, l0 = f.z, l1 = f.w;
+            cnt += f.y >> 2;
+            resume = f.y & 3;
+            if (resume == 1) m.rab(l1 >> 1, v1, a1, b1);
         }
     }
 }
