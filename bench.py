@@ -618,6 +618,11 @@ def our_arm(args, group):
                        "tuned": tuned,
                        "parallelism": f"graph-sharded x{group.world}" if group.world > 1 else "single GPU"},
             "roofline": roof,
+            # the whole step against the same roof: 1,036 algorithmic bytes
+            # per input AND node over every stage (enumerate 584, evaluate
+            # 328, levels 20, two strash passes 2 x 52)
+            "roofline_step": {"algorithmic_bytes_per_and": B_ALG_STEP, "achieved": value * B_ALG_STEP / 1e9,
+                              "peak": peak, "unit": "GB/s", "frac": value * B_ALG_STEP / 1e9 / peak},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": in_bytes,
                     "d2h_bytes_per_step": out_bytes, "steps": e2e_steps},
             "e2e_aiger": e2e_aiger,
@@ -659,6 +664,9 @@ def our_arm(args, group):
                 del pool
         print(json.dumps(line), flush=True)
     return 1 if bad else 0
+
+
+B_ALG_STEP = 1036  # algorithmic bytes per input AND node of one rw; st step
 
 
 def once(args):
