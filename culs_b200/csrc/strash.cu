@@ -838,7 +838,7 @@ int Engine::strash_core(Batch &b, int64_t M, const int *L0, const int *L1, const
         check(scan_exclusive(lvlCnt, lvlStart, maxLevel + 1, nullptr, ar_, s), "scan");
         check(scan_exclusive(chunkCnt, chunkStart, maxLevel + 1, chunkStart + maxLevel + 1, ar_, s), "scan");
     }
-    // 4. hash in dataflow order
+    // 4. hash: fixed-point rounds or the level dataflow (below)
     uint32_t cap = 1024;
     while (cap < (uint32_t)std::min<int64_t>(nLive * 2, 1ll << 31)) cap <<= 1;
     // CULS_STRASH_TABLE_CAP lowers the capacity (rounded up to a power of
