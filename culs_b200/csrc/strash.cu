@@ -20,8 +20,8 @@
 // B200 design: no per-frontier host loop.  Liveness is a reverse Kahn
 // worklist, levels an in-order dataflow (a forward Kahn worklist over a
 // fanout CSR as the fallback), and hashing either a few full-width rounds
-// that iterate the mapping to its fixed point (batches whose table fits in
-// L2) or a single in-order dataflow pass whose dependency waits are
+// that iterate the mapping to its fixed point (batches of up to 16M live
+// nodes) or a single in-order dataflow pass whose dependency waits are
 // per-level completion counters (bounded spins).
 #include <algorithm>
 #include <cstdlib>
@@ -859,12 +859,14 @@ int Engine::strash_core(Batch &b, int64_t M, const int *L0, const int *L1, const
     int *wl = ar_.get<int>(nLive + 1);
     if (!ts || !mapEnc || !kl0 || !kl1 || !wflags || !wl) return fail(CULS_E_OOM, "strash: arena exhausted");
     check(cudaMemsetAsync(qc + 5, 0, sizeof(int), s), "memset");
-    // Rounds (k_round_*) for batches whose table stays in L2, where they
-    // replace one wait latency per level by a few full passes; the level
-    // dataflow (k_dedup) for larger ones, and whenever the rounds do not
-    // settle within kMaxRounds.  CULS_DEDUP_MODE=levels|rounds forces either
+    // Rounds (k_round_*) for batches of up to 16M live nodes, where a few
+    // full passes cost less than one wait latency per level (the 10M-AND
+    // single graph: each strash 22 -> 6 ms); the level dataflow (k_dedup)
+    // for larger ones, whose rounds each move gigabytes and whose merges
+    // can cascade for many rounds, and whenever the rounds do not settle
+    // within kMaxRounds.  CULS_DEDUP_MODE=levels|rounds forces either
     // (the tests run both on the same graphs).
-    constexpr int64_t kRoundsMaxLive = 4ll << 20;
+    constexpr int64_t kRoundsMaxLive = 16ll << 20;
     constexpr int kMaxRounds = 24;
     bool useRounds = nLive > 0 && nLive <= kRoundsMaxLive;
     if (const char *env = getenv("CULS_DEDUP_MODE")) {
